@@ -1,0 +1,243 @@
+#!/usr/bin/env python3
+"""Benchmark: paths/s of PATH_TRACING on the 2.1M-triangle heightfield scene.
+
+Workload (one step): a 1920x1080 film at 64 samples per pixel, maximum
+bounce 8, Russian roulette from bounce 5, over a seeded 1024x1024-cell fractal
+heightfield (2,097,152 triangles) with 2,000 spheres of log-uniform radius
+0.1-2 (matte/plastic/metal/glass, roughness U(0.05, 0.6)) under a Perez sky
+(turbidity 2.5, sun elevation 35 degrees).  Synthetic, generated from a fixed
+seed; no dataset is read.
+
+`value` is device-timed throughput with the scene resident in HBM; `e2e` runs
+the whole job through the public API from host arrays each step (scene upload
+and acceleration-structure build, render, RGBA8 read-back).  The scene and
+the wavefront buffers (several hundred MB) exceed the 126 MB L2 between steps.
+
+Multi-GPU: the passes are independent, so N ranks render N independent
+replicas of the job (weak scaling, no collective on the data path).
+
+``--impl reference`` times the CPU restatement of the reference CPURenderer
+(the oracle) on all host threads on a bounded row sample of the same job.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "paths/s"
+CONFIG = {"workload": "terrain_2.1M_tris+2000_spheres_perez_1920x1080_pt64spp_bounce8", "resolution": [1920, 1080],
+          "spp": 64, "max_bounce": 8, "min_rr": 5, "triangles": 2097152, "spheres": 2000,
+          "l2": "inputs larger than L2 (scene + wavefront > 126 MB)"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=1024)
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def build_scene(cells):
+    from dayflower_b200.scene import generators as G
+    from dayflower_b200.scene.compiler import compile_scene
+    return compile_scene(G.terrain_spheres(cells=cells, n_spheres=2000, resolution=(1920, 1080), seed=2), layout_version=2)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q, "--format=csv,noheader,nounits"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 4 + k and "Active" in s[4 + k] and "Not" not in s[4 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(compiled, spp_sample=1, rows=12, threads=None):
+    """Times the oracle (CPU restatement of CPURenderer) on a bounded row sample."""
+    from oracle import dfo
+    threads = threads or os.cpu_count() or 1
+    o = dfo.OracleScene(compiled)
+    H = o.height
+    r0 = H // 2 - rows // 2
+    t0 = time.perf_counter()
+    res = o.render(2, spp=spp_sample, max_bounce=CONFIG["max_bounce"], min_rr=CONFIG["min_rr"], rows=(r0, r0 + rows), threads=threads)
+    dt = time.perf_counter() - t0
+    paths = o.width * rows * spp_sample
+    return {"value": paths / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": "%d rows x %d px x %d spp of the same job (%d paths, %.1f s, %d rays)" % (rows, o.width, spp_sample, paths, dt, res["rays"])}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    compiled = build_scene(args.cells)
+    res = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(compiled, rows=8)
+        if i >= args.warmup:
+            res.append(r)
+    v = statistics.median(x["value"] for x in res)
+    line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * CONFIG["resolution"][0] * CONFIG["resolution"][1] * args.spp / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": res[0]["cores"], "kind": "port", "sample": res[0]["sample"]},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from dayflower_b200 import GPURenderer, RenderingAlgorithm
+
+    compiled = build_scene(args.cells)
+    W, H = CONFIG["resolution"]
+    r = GPURenderer(device=local)
+    r.setScene(compiled)
+    r.setRenderingAlgorithm(RenderingAlgorithm.PATH_TRACING)
+    r.setMaximumBounce(CONFIG["max_bounce"])
+    r.setMinimumBounceRussianRoulette(CONFIG["min_rr"])
+    r.setSeed(0x5EED0000 + rank)
+    r.setup()
+
+    def step():
+        r.clear()
+        assert r.render(args.spp)
+        return r.lastRenderMillis()
+
+    for _ in range(args.warmup):
+        step()
+    c0 = r.getCounters()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = []
+    rays = 0
+    launches = 0
+    for _ in range(args.steps):
+        ms.append(step())
+        c = r.getCounters()
+        rays += c["rays"]
+        launches += c["launches"]
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = sum(ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    paths_per_step = W * H * args.spp
+    value = world * paths_per_step * args.steps / (total_ms / 1000.0)
+
+    # end to end through the public API from host arrays
+    e2e = None
+    if not args.no_e2e:
+        import numpy as np
+        h2d = compiled.nbytes()
+        t0 = time.perf_counter()
+        e_steps = 1
+        for _ in range(e_steps):
+            q = GPURenderer(device=local)
+            q.setScene(compiled)
+            q.setRenderingAlgorithm(RenderingAlgorithm.PATH_TRACING)
+            q.setMaximumBounce(CONFIG["max_bounce"])
+            q.setMinimumBounceRussianRoulette(CONFIG["min_rr"])
+            q.setup()
+            q.render(args.spp)
+            img = q.getImage()
+            q.dispose()
+        dt = time.perf_counter() - t0
+        e2e = {"value": paths_per_step * e_steps / dt, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(img.nbytes),
+               "note": "per step: scene upload + acceleration build + render(%d) + RGBA8 read-back" % args.spp}
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        # Dominant stage: traversal; algorithmic bytes per traced ray = ray record in (32 B) + hit out (16 B).
+        rays_per_step = rays / args.steps
+        achieved = rays_per_step * 48 / (total_ms / args.steps / 1000.0) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp),
+            "rays_per_s": world * rays / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "k_trace (whole pass, ray+hit records only)", "peak_kind": peak_kind},
+            "clocks": clk,
+            "e2e": e2e,
+        }
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(compiled)
+        print(json.dumps(line), flush=True)
+    r.dispose()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,74 @@
+"""ctypes loading of the in-tree native libraries.
+
+The render path has no fallback: if ``libdayflower_cuda.so`` cannot be built
+or loaded, :func:`load_renderer` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+from . import build as _build
+
+_lock = threading.Lock()
+_cuda = None
+_scene = None
+
+_c_int, _c_i64, _c_f, _c_p, _c_u32 = ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_void_p, ctypes.c_uint32
+
+# (name, restype, argtypes) for every entry point in include/dayflower_cuda.h
+SIGNATURES = [
+    ("dfc_create", _c_int, [_c_int, ctypes.POINTER(_c_p)]),
+    ("dfc_destroy", _c_int, [_c_p]),
+    ("dfc_last_error", ctypes.c_char_p, [_c_p]),
+    ("dfc_scene_put", _c_int, [_c_p, ctypes.c_char_p, _c_p, _c_i64, _c_int]),
+    ("dfc_scene_commit", _c_int, [_c_p, _c_int]),
+    ("dfc_set_image", _c_int, [_c_p, _c_int, _c_int]),
+    ("dfc_set_maximum_bounce", _c_int, [_c_p, _c_int]),
+    ("dfc_set_minimum_bounce_russian_roulette", _c_int, [_c_p, _c_int]),
+    ("dfc_set_rendering_algorithm", _c_int, [_c_p, _c_int]),
+    ("dfc_set_samples", _c_int, [_c_p, _c_int]),
+    ("dfc_set_maximum_distance", _c_int, [_c_p, _c_f]),
+    ("dfc_set_tone_mapper", _c_int, [_c_p, _c_int]),
+    ("dfc_set_preview_mode", _c_int, [_c_p, _c_int]),
+    ("dfc_set_seed", _c_int, [_c_p, _c_u32]),
+    ("dfc_setup", _c_int, [_c_p]),
+    ("dfc_render", _c_int, [_c_p, _c_int, ctypes.POINTER(_c_int)]),
+    ("dfc_render_shutdown", _c_int, [_c_p]),
+    ("dfc_clear", _c_int, [_c_p]),
+    ("dfc_update_camera", _c_int, [_c_p, _c_p]),
+    ("dfc_update_matrices", _c_int, [_c_p, _c_p, _c_i64]),
+    ("dfc_read_image_rgba8", _c_int, [_c_p, _c_p, _c_i64]),
+    ("dfc_read_film", _c_int, [_c_p, _c_p, _c_i64]),
+    ("dfc_read_primary_hits", _c_int, [_c_p, _c_p, _c_p, _c_i64]),
+    ("dfc_read_counters", _c_int, [_c_p, _c_p]),
+    ("dfc_read_stage_times", _c_int, [_c_p, _c_p]),
+]
+
+
+def load_renderer(build: bool = True) -> ctypes.CDLL:
+    """Loads libdayflower_cuda.so (building it first if sources changed)."""
+    global _cuda
+    with _lock:
+        if _cuda is None:
+            path = _build.build_cuda() if build else _build.cuda_lib_path()
+            lib = ctypes.CDLL(path)
+            for name, res, args in SIGNATURES:
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _cuda = lib
+        return _cuda
+
+
+def load_scene_compiler() -> ctypes.CDLL:
+    """Loads the scene-compiler host helper (libdayflower_scene.so)."""
+    global _scene
+    with _lock:
+        if _scene is None:
+            lib = ctypes.CDLL(_build.build_scene())
+            lib.dfc_sc_build_mesh_bvh.restype = ctypes.c_longlong
+            lib.dfc_sc_build_mesh_bvh.argtypes = [_c_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _c_p, _c_p,
+                                                  ctypes.c_longlong]
+            _scene = lib
+        return _scene

@@ -1,0 +1,94 @@
+"""Builds the native libraries in-tree (no JIT cache):
+
+* ``dayflower_b200/_lib/libdayflower_cuda.so``  - the render path (nvcc, sm_100a)
+* ``dayflower_b200/_lib/libdayflower_scene.so`` - the scene-compiler host helper (g++)
+
+Each library is rebuilt only when one of its sources is newer than it.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "_lib")
+ROOT = os.path.dirname(HERE)
+
+CUDA_SOURCES = ["dfc_api.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp"]
+CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h"]
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s" % (" ".join(cmd), r.stdout))
+    return r.stdout
+
+
+def cuda_lib_path() -> str:
+    return os.path.join(LIB, "libdayflower_cuda.so")
+
+
+def scene_lib_path() -> str:
+    return os.path.join(LIB, "libdayflower_scene.so")
+
+
+def build_cuda(force: bool = False, verbose: bool = False, extra=()) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    out = cuda_lib_path()
+    deps = [os.path.join(CSRC, s) for s in CUDA_SOURCES + CUDA_HEADERS] + [os.path.join(ROOT, "include", "dayflower_cuda.h")]
+    if not force and not _stale(out, deps):
+        return out
+    obj_dir = os.path.join(LIB, "_obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    objs = []
+    for s in CUDA_SOURCES:
+        o = os.path.join(obj_dir, s + ".o")
+        # -fmad=false: every float operation is rounded on its own, as in the
+        # reference (Java float arithmetic has no contraction); the traversal's
+        # box tests use explicit fmaf where the rounding does not matter.
+        cmd = [_nvcc(), "-c", os.path.join(CSRC, s), "-o", o, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+               "-Xptxas", "-O3", "--expt-relaxed-constexpr", "-fmad=false"] + GENCODE + list(extra)
+        if verbose and s.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"]
+        log = _run(cmd)
+        if verbose:
+            sys.stdout.write(log)
+        objs.append(o)
+    _run([_nvcc(), "-shared", "-o", out] + objs + GENCODE + ["-cudart", "static"])
+    return out
+
+
+def build_scene(force: bool = False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    out = scene_lib_path()
+    src = os.path.join(CSRC, "scene_compiler.cpp")
+    if force or _stale(out, [src]):
+        _run([shutil.which("g++") or "g++", "-O2", "-std=c++17", "-fPIC", "-shared", src, "-o", out])
+    return out
+
+
+def build_all(force: bool = False, verbose: bool = False):
+    return build_scene(force), build_cuda(force, verbose)
+
+
+if __name__ == "__main__":
+    print(build_all(force="--force" in sys.argv, verbose="-v" in sys.argv))

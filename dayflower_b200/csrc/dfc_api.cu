@@ -1,0 +1,576 @@
+// C-ABI of libdayflower_cuda: the handle that stands in for Dayflower's
+// GPURenderer (renderer/gpu/GPURenderer.java, AbstractGPURenderer.java).
+//
+// A handle owns one CUDA stream, the device scene, the film and the
+// wavefront buffers.  dfc_render() runs render passes of one sample per pixel
+// (AbstractGPURenderer.java:231-297); each pass is the kernel sequence in
+// dfc_kernels.cu enqueued on the handle's stream, with no host synchronisation
+// between the bounce steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dayflower_cuda.h"
+#include "dfc_ingest.h"
+#include "dfc_kernels.h"
+
+using namespace dfc;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { release(); }
+  void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, n ? n : 16);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct dfc_renderer {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::mutex mu;
+  std::atomic<bool> stop{false};
+  std::string err;
+  // settings (AbstractGPURenderer.java:148-158)
+  int width = 800, height = 800;
+  int image_from_camera = 0;
+  int algorithm = DFC_PATH_TRACING;
+  int max_bounce = 20, min_rr = 5, ao_samples = 10, tone_mapper = DFC_TONE_MAPPER_NONE, preview = 0;
+  float max_distance = 20.0f;
+  uint32_t seed = 0x5eed1234u;
+  // scene
+  Staged staged;
+  bool have_scene = false;
+  HostScene host;
+  DevBuf d_prims, d_mats, d_lights, d_nodes, d_tlas_items, d_unbounded, d_tri_pos, d_tri_attr, d_rects, d_perez, d_camera;
+  SceneView view{};
+  // film and wavefront
+  bool set_up = false;
+  unsigned pixels = 0, paths = 0;
+  int steps = 0;
+  DevBuf d_film_sum, d_film_sq, d_primary_prim, d_primary_t, d_rgba;
+  DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
+  DevBuf d_ray_list[2], d_work_list[2], d_counts, d_overflow, d_ray_total;
+  DevBuf d_ao_o, d_ao_d, d_ao_v;
+  int64_t pass = 0, total_paths = 0, launches = 0;
+  float last_ms[5] = {0, 0, 0, 0, 0};
+  int sm_count = 148;
+};
+
+namespace {
+
+int fail(dfc_renderer* r, int code, const std::string& msg) {
+  if (r) r->err = msg;
+  return code;
+}
+int cuda_fail(dfc_renderer* r, cudaError_t e, const char* what) {
+  int code = (e == cudaErrorMemoryAllocation) ? DFC_E_OOM : DFC_E_CUDA;
+  return fail(r, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define DFC_CK(expr, what)                             \
+  do {                                                 \
+    cudaError_t e_ = (expr);                           \
+    if (e_ != cudaSuccess) return cuda_fail(r, e_, what); \
+  } while (0)
+
+template <typename T>
+cudaError_t upload(dfc_renderer* r, DevBuf& b, const std::vector<T>& v) {
+  cudaError_t e = b.ensure(v.size() * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, r->stream);
+}
+
+__global__ void k_sum_counts(const unsigned* counts, int steps, unsigned long long* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int i = 0; i < steps; ++i) s += counts[2 * i];
+    *total += s;
+  }
+}
+
+int alloc_wavefront(dfc_renderer* r) {
+  const unsigned W = (unsigned)r->width, H = (unsigned)r->height;
+  r->pixels = W * H;
+  r->paths = r->pixels;
+  const size_t P = r->paths;
+  DFC_CK(r->d_film_sum.ensure(P * 16), "film");
+  DFC_CK(r->d_film_sq.ensure(P * 16), "film");
+  DFC_CK(r->d_primary_prim.ensure(P * 4), "primary hits");
+  DFC_CK(r->d_primary_t.ensure(P * 4), "primary hits");
+  DFC_CK(r->d_rgba.ensure(P * 4), "image");
+  DFC_CK(r->d_beta.ensure(P * 16), "path state");
+  DFC_CK(r->d_rad.ensure(P * 16), "path state");
+  DFC_CK(r->d_meta.ensure(P * 16), "path state");
+  DFC_CK(r->d_ray_o.ensure(3 * P * 16), "rays");
+  DFC_CK(r->d_ray_d.ensure(3 * P * 16), "rays");
+  DFC_CK(r->d_hits.ensure(3 * P * 16), "hits");
+  DFC_CK(r->d_pend_s.ensure(P * 16), "pending");
+  DFC_CK(r->d_pend_m.ensure(P * 16), "pending");
+  for (int k = 0; k < 2; ++k) {
+    DFC_CK(r->d_ray_list[k].ensure(3 * P * 4), "ray list");
+    DFC_CK(r->d_work_list[k].ensure(P * 4), "work list");
+  }
+  DFC_CK(r->d_overflow.ensure(16), "counters");
+  DFC_CK(r->d_ray_total.ensure(16), "counters");
+  return DFC_OK;
+}
+
+int clear_film(dfc_renderer* r) {
+  const size_t P = r->pixels;
+  DFC_CK(cudaMemsetAsync(r->d_film_sum.p, 0, P * 16, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_film_sq.p, 0, P * 16, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_primary_prim.p, 0xff, P * 4, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_primary_t.p, 0, P * 4, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_overflow.p, 0, 16, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_ray_total.p, 0, 16, r->stream), "clear");
+  r->pass = 0;
+  r->total_paths = 0;
+  r->launches = 0;
+  return DFC_OK;
+}
+
+ShadeArgs shade_args(dfc_renderer* r, int step) {
+  ShadeArgs a{};
+  a.scene = r->view;
+  a.paths = r->paths;
+  a.pixels = r->pixels;
+  a.max_bounce = r->max_bounce;
+  a.min_rr = r->min_rr;
+  a.preview = r->preview;
+  a.last_step = 0;
+  a.record_primary = r->pass == 0;
+  a.ao_samples = r->ao_samples;
+  unsigned* counts = r->d_counts.as<unsigned>();
+  a.work_list = r->d_work_list[step & 1].as<unsigned>();
+  a.work_count = counts + 2 * step + 1;
+  a.next_work_list = r->d_work_list[(step + 1) & 1].as<unsigned>();
+  a.next_work_count = counts + 2 * (step + 1) + 1;
+  a.next_ray_list = r->d_ray_list[(step + 1) & 1].as<unsigned>();
+  a.next_ray_count = counts + 2 * (step + 1);
+  a.beta = r->d_beta.as<float4>();
+  a.radiance = r->d_rad.as<float4>();
+  a.meta = r->d_meta.as<uint4>();
+  a.ray_o = r->d_ray_o.as<float4>();
+  a.ray_d = r->d_ray_d.as<float4>();
+  a.hits = r->d_hits.as<float4>();
+  a.pend_shadow = r->d_pend_s.as<float4>();
+  a.pend_mis = r->d_pend_m.as<float4>();
+  a.film_sum = r->d_film_sum.as<float4>();
+  a.film_sq = r->d_film_sq.as<float4>();
+  a.primary_prim = r->d_primary_prim.as<int>();
+  a.primary_t = r->d_primary_t.as<float>();
+  a.ao_o = r->d_ao_o.as<float4>();
+  a.ao_d = r->d_ao_d.as<float4>();
+  return a;
+}
+
+TraceArgs trace_args(dfc_renderer* r, int step) {
+  TraceArgs t{};
+  t.scene = r->view;
+  unsigned* counts = r->d_counts.as<unsigned>();
+  t.ray_list = r->d_ray_list[step & 1].as<unsigned>();
+  t.ray_count = counts + 2 * step;
+  t.ray_o = r->d_ray_o.as<float4>();
+  t.ray_d = r->d_ray_d.as<float4>();
+  t.hits = r->d_hits.as<float4>();
+  t.paths = r->paths;
+  t.overflow = r->d_overflow.as<unsigned>();
+  return t;
+}
+
+// Enqueues one render pass (one sample per pixel) on the handle's stream.
+int enqueue_pass(dfc_renderer* r) {
+  const int algo = r->algorithm;
+  const int steps = algo == DFC_PATH_TRACING ? r->max_bounce + 4 : 1;
+  const size_t counts_bytes = (size_t)(steps + 2) * 2 * sizeof(unsigned);
+  DFC_CK(r->d_counts.ensure(counts_bytes), "counters");
+  DFC_CK(cudaMemsetAsync(r->d_counts.p, 0, counts_bytes, r->stream), "counters");
+  unsigned* counts = r->d_counts.as<unsigned>();
+  RaygenArgs g{};
+  g.scene = r->view;
+  g.paths = r->paths;
+  g.pixels = r->pixels;
+  g.width = (unsigned)r->width;
+  g.sample_base = (unsigned)r->pass;
+  g.seed = r->seed;
+  g.beta = r->d_beta.as<float4>();
+  g.radiance = r->d_rad.as<float4>();
+  g.meta = r->d_meta.as<uint4>();
+  g.ray_o = r->d_ray_o.as<float4>();
+  g.ray_d = r->d_ray_d.as<float4>();
+  g.ray_list = r->d_ray_list[0].as<unsigned>();
+  g.ray_count = counts;
+  g.work_list = r->d_work_list[0].as<unsigned>();
+  g.work_count = counts + 1;
+  k_raygen<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(g);
+  r->launches++;
+  const int trace_grid = r->sm_count * 6;
+  const int shade_grid = r->sm_count * 8;
+  if (algo == DFC_PATH_TRACING) {
+    for (int s = 0; s < steps; ++s) {
+      k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, s));
+      ShadeArgs a = shade_args(r, s);
+      a.last_step = s == steps - 1;
+      k_shade_path<<<shade_grid, 256, 0, r->stream>>>(a);
+      r->launches += 2;
+    }
+  } else {
+    k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, 0));
+    ShadeArgs a = shade_args(r, 0);
+    const int kind = algo == DFC_AMBIENT_OCCLUSION ? DFC_ALGO_AO : (algo == DFC_DEPTH_CAMERA ? DFC_ALGO_DEPTH : DFC_ALGO_RAY_CASTING);
+    k_shade_primary<<<shade_grid, 256, 0, r->stream>>>(a, kind);
+    r->launches += 2;
+    if (kind == DFC_ALGO_AO) {
+      AoArgs o{};
+      o.scene = r->view;
+      o.paths = r->paths;
+      o.samples = r->ao_samples;
+      o.max_distance = r->max_distance;
+      o.radiance = r->d_rad.as<float4>();
+      o.ao_o = r->d_ao_o.as<float4>();
+      o.ao_d = r->d_ao_d.as<float4>();
+      o.ao_value = r->d_ao_v.as<float>();
+      o.overflow = r->d_overflow.as<unsigned>();
+      k_trace_ao<<<trace_grid, kTraceThreads, 0, r->stream>>>(o);
+      k_ao_resolve<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(a, r->d_ao_v.as<float>(), r->ao_samples);
+      r->launches += 2;
+    }
+  }
+  k_sum_counts<<<1, 1, 0, r->stream>>>(counts, algo == DFC_PATH_TRACING ? steps : 1, r->d_ray_total.as<unsigned long long>());
+  DFC_CK(cudaGetLastError(), "kernel launch");
+  r->pass++;
+  r->total_paths += r->paths;
+  return DFC_OK;
+}
+
+bool valid(const dfc_renderer* r) { return r != nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int dfc_create(int device, dfc_renderer** out) {
+  if (!out) return DFC_E_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess) return DFC_E_CUDA;
+  if (device < 0 || device >= count) return DFC_E_INVALID_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return DFC_E_CUDA;
+  dfc_renderer* r = new dfc_renderer();
+  r->device = device;
+  cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
+    delete r;
+    return DFC_E_CUDA;
+  }
+  *out = r;
+  return DFC_OK;
+}
+
+int dfc_destroy(dfc_renderer* r) {
+  if (!r) return DFC_E_INVALID_ARG;
+  {
+    std::lock_guard<std::mutex> lk(r->mu);
+    cudaSetDevice(r->device);
+    cudaStreamSynchronize(r->stream);
+  }
+  cudaEventDestroy(r->ev0);
+  cudaEventDestroy(r->ev1);
+  cudaStream_t s = r->stream;
+  delete r;  // DevBuf destructors free device memory
+  cudaStreamDestroy(s);
+  return DFC_OK;
+}
+
+const char* dfc_last_error(const dfc_renderer* r) { return r ? r->err.c_str() : "null handle"; }
+
+int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t count, int type) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!name) return fail(r, DFC_E_INVALID_ARG, "name == null");
+  if (count < 0 || (count > 0 && !data)) return fail(r, DFC_E_INVALID_ARG, "data == null or negative count");
+  if (type == DFC_F32) {
+    const float* f = static_cast<const float*>(data);
+    r->staged.f32[name].assign(f, f + count);
+  } else if (type == DFC_I32) {
+    const int32_t* q = static_cast<const int32_t*>(data);
+    r->staged.i32[name].assign(q, q + count);
+  } else {
+    return fail(r, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
+  }
+  return DFC_OK;
+}
+
+int dfc_scene_commit(dfc_renderer* r, int layout_version) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  cudaSetDevice(r->device);
+  HostScene hs;
+  std::string err;
+  int rc = ingest_scene(r->staged, layout_version, &hs, &err);
+  if (rc != DFC_OK) return fail(r, rc, err);
+  DFC_CK(cudaStreamSynchronize(r->stream), "sync");
+  DFC_CK(upload(r, r->d_prims, hs.prims), "scene upload");
+  DFC_CK(upload(r, r->d_mats, hs.materials), "scene upload");
+  DFC_CK(upload(r, r->d_lights, hs.lights), "scene upload");
+  DFC_CK(upload(r, r->d_nodes, hs.nodes), "scene upload");
+  DFC_CK(upload(r, r->d_tlas_items, hs.tlas_items), "scene upload");
+  DFC_CK(upload(r, r->d_unbounded, hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded), "scene upload");
+  DFC_CK(upload(r, r->d_tri_pos, hs.tri_pos), "scene upload");
+  DFC_CK(upload(r, r->d_tri_attr, hs.tri_attr), "scene upload");
+  DFC_CK(upload(r, r->d_rects, hs.rects), "scene upload");
+  DFC_CK(upload(r, r->d_perez, hs.perez), "scene upload");
+  std::vector<float> cam(hs.camera, hs.camera + 19);
+  DFC_CK(upload(r, r->d_camera, cam), "scene upload");
+  DFC_CK(cudaStreamSynchronize(r->stream), "sync");
+  SceneView& v = r->view;
+  v.prims = r->d_prims.as<DPrim>();
+  v.prim_count = (int)hs.prims.size();
+  v.materials = r->d_mats.as<DMaterial>();
+  v.lights = r->d_lights.as<DLight>();
+  v.light_count = hs.lights_storage_pad ? 0 : (int)hs.lights.size();
+  v.nodes = r->d_nodes.as<BVH4Node>();
+  v.tlas_root = hs.tlas_root;
+  v.tlas_items = r->d_tlas_items.as<int>();
+  v.unbounded = r->d_unbounded.as<int>();
+  v.unbounded_count = (int)hs.unbounded.size();
+  v.tri_pos = r->d_tri_pos.as<F4>();
+  v.tri_attr = r->d_tri_attr.as<float>();
+  v.rects = r->d_rects.as<float>();
+  v.perez = r->d_perez.as<float>();
+  v.camera = r->d_camera.as<float>();
+  r->host = std::move(hs);
+  r->have_scene = true;
+  r->staged = Staged();
+  if (r->image_from_camera) {
+    r->width = (int)r->host.camera[17];
+    r->height = (int)r->host.camera[18];
+  }
+  r->set_up = false;
+  return DFC_OK;
+}
+
+int dfc_set_image(dfc_renderer* r, int width, int height) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (width == 0 && height == 0) {
+    r->image_from_camera = 1;
+    if (r->have_scene) { r->width = (int)r->host.camera[17]; r->height = (int)r->host.camera[18]; }
+  } else {
+    if (width < 1 || height < 1 || (int64_t)width * height > (1LL << 27)) return fail(r, DFC_E_INVALID_ARG, "resolution out of range");
+    r->image_from_camera = 0;
+    r->width = width;
+    r->height = height;
+  }
+  r->set_up = false;
+  return DFC_OK;
+}
+
+#define DFC_SETTER(fn, field, lo, hi, msg)                                            \
+  int fn(dfc_renderer* r, int v) {                                                    \
+    if (!valid(r)) return DFC_E_INVALID_ARG;                                          \
+    std::lock_guard<std::mutex> lk(r->mu);                                            \
+    if (v < (lo) || v > (hi)) return fail(r, DFC_E_INVALID_ARG, msg);                 \
+    r->field = v;                                                                     \
+    return DFC_OK;                                                                    \
+  }
+DFC_SETTER(dfc_set_maximum_bounce, max_bounce, 0, 4096, "maximumBounce out of range")
+DFC_SETTER(dfc_set_minimum_bounce_russian_roulette, min_rr, 0, 1 << 30, "minimumBounceRussianRoulette out of range")
+DFC_SETTER(dfc_set_rendering_algorithm, algorithm, 0, 4, "unknown rendering algorithm")
+DFC_SETTER(dfc_set_samples, ao_samples, 1, 4096, "samples out of range")
+DFC_SETTER(dfc_set_tone_mapper, tone_mapper, 0, 5, "unknown tone mapper")
+DFC_SETTER(dfc_set_preview_mode, preview, 0, 1, "preview mode is 0 or 1")
+
+int dfc_set_maximum_distance(dfc_renderer* r, float v) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!std::isfinite(v)) return fail(r, DFC_E_INVALID_ARG, "maximumDistance must be finite");
+  r->max_distance = v;
+  return DFC_OK;
+}
+
+int dfc_set_seed(dfc_renderer* r, uint32_t seed) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  r->seed = seed;
+  return DFC_OK;
+}
+
+int dfc_setup(dfc_renderer* r) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->have_scene) return fail(r, DFC_E_STATE, "setup() before setScene()");
+  cudaSetDevice(r->device);
+  int rc = alloc_wavefront(r);
+  if (rc) return rc;
+  rc = clear_film(r);
+  if (rc) return rc;
+  r->set_up = true;
+  return DFC_OK;
+}
+
+int dfc_render(dfc_renderer* r, int passes, int* completed) {
+  if (completed) *completed = 0;
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (passes < 1) return fail(r, DFC_E_INVALID_ARG, "renderPasses < 1");  // AbstractGPURenderer.java:323
+  if (!r->set_up) return fail(r, DFC_E_STATE, "render() before setup()");
+  if (r->algorithm == DFC_RAY_TRACING) return fail(r, DFC_E_UNSUPPORTED, "RAY_TRACING is not implemented by this renderer");
+  cudaSetDevice(r->device);
+  if (r->algorithm == DFC_AMBIENT_OCCLUSION) {
+    const size_t n = (size_t)r->paths * r->ao_samples;
+    DFC_CK(r->d_ao_o.ensure(n * 16), "AO rays");
+    DFC_CK(r->d_ao_d.ensure(n * 16), "AO rays");
+    DFC_CK(r->d_ao_v.ensure(n * 4), "AO rays");
+  }
+  r->stop.store(false);
+  DFC_CK(cudaEventRecord(r->ev0, r->stream), "event");
+  int done = 0;
+  for (int k = 0; k < passes; ++k) {
+    if (r->stop.load()) break;
+    int rc = enqueue_pass(r);
+    if (rc) return rc;
+    ++done;
+  }
+  DFC_CK(cudaEventRecord(r->ev1, r->stream), "event");
+  DFC_CK(cudaEventSynchronize(r->ev1), "render");
+  DFC_CK(cudaGetLastError(), "render");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+  r->last_ms[0] = ms;
+  unsigned ov = 0;
+  DFC_CK(cudaMemcpy(&ov, r->d_overflow.p, 4, cudaMemcpyDeviceToHost), "readback");
+  if (completed) *completed = done;
+  if (ov) return fail(r, DFC_E_TIMEOUT, "traversal stack bound exceeded on " + std::to_string(ov) + " node visits");
+  if (done < passes) return fail(r, DFC_E_STOPPED, "render stopped");
+  return DFC_OK;
+}
+
+int dfc_render_shutdown(dfc_renderer* r) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  r->stop.store(true);
+  return DFC_OK;
+}
+
+int dfc_clear(dfc_renderer* r) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->set_up) return DFC_OK;
+  cudaSetDevice(r->device);
+  return clear_film(r);
+}
+
+int dfc_update_camera(dfc_renderer* r, const float* camera19) {
+  if (!valid(r) || !camera19) return fail(r, DFC_E_INVALID_ARG, "camera == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->have_scene) return fail(r, DFC_E_STATE, "updateCamera() before setScene()");
+  std::memcpy(r->host.camera, camera19, 19 * sizeof(float));
+  DFC_CK(cudaMemcpyAsync(r->d_camera.p, camera19, 19 * sizeof(float), cudaMemcpyHostToDevice, r->stream), "camera");
+  DFC_CK(cudaStreamSynchronize(r->stream), "camera");
+  return DFC_OK;
+}
+
+int dfc_update_matrices(dfc_renderer* r, const float* m, int64_t n) {
+  if (!valid(r) || !m) return fail(r, DFC_E_INVALID_ARG, "matrices == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->have_scene) return fail(r, DFC_E_STATE, "updateMatrix44Fs() before setScene()");
+  if (n != (int64_t)r->host.prims.size()) return fail(r, DFC_E_INVALID_ARG, "matrix count differs from the primitive count");
+  // The top level is built over compiled bounding volumes; moving primitives
+  // requires a new setScene so that the hierarchy sees their new boxes.
+  for (int64_t p = 0; p < n; ++p) {
+    DPrim& pr = r->host.prims[p];
+    const float* q = m + p * 32;
+    std::memcpy(pr.o2w, q, 12 * sizeof(float));
+    std::memcpy(pr.w2o, q + 16, 12 * sizeof(float));
+    bool id = true;
+    for (int k = 0; k < 16; ++k) id = id && q[k] == ((k % 5) == 0 ? 1.0f : 0.0f) && q[16 + k] == ((k % 5) == 0 ? 1.0f : 0.0f);
+    pr.identity = id;
+  }
+  DFC_CK(upload(r, r->d_prims, r->host.prims), "matrices");
+  DFC_CK(cudaStreamSynchronize(r->stream), "matrices");
+  r->view.prims = r->d_prims.as<DPrim>();
+  return DFC_OK;
+}
+
+int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t cap) {
+  if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
+  if (cap < (int64_t)r->pixels * 4) return fail(r, DFC_E_INVALID_ARG, "destination too small");
+  k_resolve_rgba8<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->d_film_sum.as<float4>(), (int)r->pixels, r->tone_mapper, 1.0f, r->d_rgba.as<uchar4>());
+  DFC_CK(cudaMemcpyAsync(dst, r->d_rgba.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+  DFC_CK(cudaStreamSynchronize(r->stream), "readback");
+  return DFC_OK;
+}
+
+int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
+  if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
+  const size_t P = r->pixels;
+  if (cap < (int64_t)P * 7) return fail(r, DFC_E_INVALID_ARG, "destination too small");
+  std::vector<float> s(P * 4), q(P * 4);
+  DFC_CK(cudaMemcpyAsync(s.data(), r->d_film_sum.p, P * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+  DFC_CK(cudaMemcpyAsync(q.data(), r->d_film_sq.p, P * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+  DFC_CK(cudaStreamSynchronize(r->stream), "readback");
+  for (size_t i = 0; i < P; ++i) {
+    dst[i * 7 + 0] = s[i * 4 + 0]; dst[i * 7 + 1] = s[i * 4 + 1]; dst[i * 7 + 2] = s[i * 4 + 2];
+    dst[i * 7 + 3] = q[i * 4 + 0]; dst[i * 7 + 4] = q[i * 4 + 1]; dst[i * 7 + 5] = q[i * 4 + 2];
+    dst[i * 7 + 6] = s[i * 4 + 3];
+  }
+  return DFC_OK;
+}
+
+int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t cap) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
+  if (cap < (int64_t)r->pixels) return fail(r, DFC_E_INVALID_ARG, "destination too small");
+  if (prim) DFC_CK(cudaMemcpyAsync(prim, r->d_primary_prim.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+  if (t) DFC_CK(cudaMemcpyAsync(t, r->d_primary_t.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+  DFC_CK(cudaStreamSynchronize(r->stream), "readback");
+  return DFC_OK;
+}
+
+int dfc_read_counters(dfc_renderer* r, int64_t* out4) {
+  if (!valid(r) || !out4) return fail(r, DFC_E_INVALID_ARG, "out == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  unsigned long long rays = 0;
+  if (r->set_up) {
+    DFC_CK(cudaMemcpyAsync(&rays, r->d_ray_total.p, 8, cudaMemcpyDeviceToHost, r->stream), "readback");
+    DFC_CK(cudaStreamSynchronize(r->stream), "readback");
+  }
+  out4[0] = r->pass;
+  out4[1] = r->total_paths;
+  out4[2] = (int64_t)rays;
+  out4[3] = r->launches;
+  return DFC_OK;
+}
+
+int dfc_read_stage_times(dfc_renderer* r, float* out5) {
+  if (!valid(r) || !out5) return fail(r, DFC_E_INVALID_ARG, "out == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  std::memcpy(out5, r->last_ms, sizeof r->last_ms);
+  return DFC_OK;
+}
+
+}  // extern "C"

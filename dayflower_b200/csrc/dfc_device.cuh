@@ -1,0 +1,845 @@
+// Device math, sampling, intersection and shading routines of the render path.
+// Each routine names the reference code whose semantics it implements (paths
+// relative to src/main/java/org/dayflower/); the CPU renderer (CPURenderer)
+// is the behaviour followed where it differs from the Aparapi kernel.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dfc_scene.h"
+
+namespace dfc {
+
+#define DFC_D __device__ __forceinline__
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTMin = 0.001f;  // scene/Scene.java:70
+constexpr float kFltMax = 3.402823466e+38f;
+
+// ---------------------------------------------------------------- vectors --
+struct V3 { float x, y, z; };
+DFC_D V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+DFC_D V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+DFC_D V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+DFC_D V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+DFC_D V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+DFC_D V3 mul(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+DFC_D float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+DFC_D V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+DFC_D float len(V3 a) { return sqrtf(dot(a, a)); }
+DFC_D bool is_black(V3 c) { return c.x == 0.0f && c.y == 0.0f && c.z == 0.0f; }
+DFC_D V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+// geometry/Vector3F.java:1000: lengths within [nextDown^3(1), nextUp(1)] are kept.
+DFC_D V3 normalize(V3 v) {
+  const float l = len(v);
+  if (l >= 0.99999982f && l <= 1.00000012f) return v;
+  return V3{v.x / l, v.y / l, v.z / l};
+}
+DFC_D float clampf(float v, float a, float b) { return v < a ? a : (v > b ? b : v); }
+DFC_D float luminance(V3 c) { return c.x * 0.212671f + c.y * 0.715160f + c.z * 0.072169f; }
+
+// 3x4 row-major affine transforms (the top three rows of Matrix44F).
+DFC_D V3 xf_point(const float* m, V3 p) {
+  return {m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7], m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]};
+}
+DFC_D V3 xf_vec(const float* m, V3 v) {
+  return {m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z, m[8] * v.x + m[9] * v.y + m[10] * v.z};
+}
+DFC_D V3 xf_vec_t(const float* m, V3 v) {  // transpose of the 3x3 part
+  return {m[0] * v.x + m[4] * v.y + m[8] * v.z, m[1] * v.x + m[5] * v.y + m[9] * v.z, m[2] * v.x + m[6] * v.y + m[10] * v.z};
+}
+
+struct ONB { V3 u, v, w; };
+DFC_D V3 compute_v(V3 w) {  // geometry/Vector3F.java:527
+  V3 n = normalize(w);
+  float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+  if (ax < ay && ax < az) return normalize(V3{0.0f, n.z, -n.y});
+  if (ay < az) return normalize(V3{n.z, 0.0f, -n.x});
+  return normalize(V3{n.y, -n.x, 0.0f});
+}
+DFC_D ONB onb_w(V3 w) { ONB o; o.w = normalize(w); o.v = compute_v(w); o.u = cross(o.v, o.w); return o; }  // OrthonormalBasis33F.java:88
+DFC_D ONB onb_wv(V3 w, V3 v) {  // OrthonormalBasis33F.java:110
+  ONB o; o.w = normalize(w); o.u = normalize(cross(normalize(v), o.w)); o.v = cross(o.w, o.u); return o;
+}
+DFC_D V3 to_local(V3 a, const ONB& b) { return {dot(a, b.u), dot(a, b.v), dot(a, b.w)}; }
+DFC_D V3 to_world(V3 a, const ONB& b) { return b.u * a.x + b.v * a.y + b.w * a.z; }
+
+// ------------------------------------------------------------ random numbers
+// Counter-based: every draw is keyed by (seed, pixel, sample, dimension), so a
+// sample gets the same numbers alone or batched with other work.
+DFC_D uint32_t rng_hash(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16; return x;
+}
+DFC_D uint32_t rng_path_key(uint32_t seed, uint32_t pixel, uint32_t sample) {
+  return rng_hash(seed ^ rng_hash(pixel ^ rng_hash(sample + 0x632be5abu)));
+}
+DFC_D float rng_uniform(uint32_t key, uint32_t dim) {
+  return (float)(rng_hash(key + dim * 0x9e3779b9u) >> 8) * (1.0f / 16777216.0f);
+}
+enum : uint32_t {
+  kDimPixelX = 0, kDimPixelY = 1, kDimLensU = 2, kDimLensV = 3, kDimBounceBase = 8, kDimBounceStride = 16,
+  kDimLightPick = 0, kDimLightSampleU = 1, kDimLightSampleV = 2, kDimMisSampleU = 3, kDimMisSampleV = 4,
+  kDimSunPick = 5, kDimBsdfU = 6, kDimBsdfV = 7, kDimRoulette = 8,
+};
+DFC_D uint32_t bounce_dim(int b, uint32_t w) { return kDimBounceBase + (uint32_t)b * kDimBounceStride + w; }
+
+// -------------------------------------------------------------- sampling --
+DFC_D void concentric(float u, float v, float* x, float* y) {  // geometry/SampleGeneratorF.java:129
+  if (u == 0.0f && v == 0.0f) { *x = 0.0f; *y = 0.0f; return; }
+  float a = u * 2.0f - 1.0f, b = v * 2.0f - 1.0f;
+  float r, phi;
+  if (a * a > b * b) { r = a; phi = (kPi / 4.0f) * (b / a); }
+  else { r = b; phi = (kPi / 2.0f) - (kPi / 4.0f) * (a / b); }
+  float s, c;
+  sincosf(phi, &s, &c);
+  *x = r * c; *y = r * s;
+}
+DFC_D V3 cosine_hemisphere(float u, float v) {
+  float x, y;
+  concentric(u, v, &x, &y);
+  return {x, y, sqrtf(fmaxf(0.0f, 1.0f - x * x - y * y))};
+}
+DFC_D V3 uniform_hemisphere(float u, float v) {
+  float st = sqrtf(fmaxf(0.0f, 1.0f - u * u)), s, c;
+  sincosf(2.0f * kPi * v, &s, &c);
+  return {st * c, st * s, u};
+}
+
+// ------------------------------------------------------------------ camera
+// scene/Camera.java:243 createPrimaryRay over the 19-float compiled camera.
+DFC_D bool camera_ray(const float* c, float ix, float iy, float px, float py, float lu, float lv, V3* o, V3* d) {
+  const float cx = 2.0f * ((ix + px) / (c[17] - 1.0f)) - 1.0f;
+  const float cy = 2.0f * ((iy + py) / (c[18] - 1.0f)) - 1.0f;
+  float wf = 1.0f;
+  if ((int)c[2] == 0) {  // Lens.FISHEYE
+    float dp = cx * cx + cy * cy;
+    if (dp > 1.0f) return false;
+    wf = sqrtf(1.0f - dp);
+  }
+  V3 U = ld3(c + 3), Vv = ld3(c + 6), W = ld3(c + 9), eye = ld3(c + 12);
+  V3 pp = (U * (c[0] * cx) + Vv * (c[1] * cy)) + (eye + W * wf);
+  V3 pip = eye + normalize(pp - eye) * c[16];
+  V3 org = eye;
+  if (c[15] > 0.00001f) {
+    float dx, dy;
+    concentric(lu, lv, &dx, &dy);
+    org = eye + (U * (dx * c[15]) + Vv * (dy * c[15]));
+  }
+  *o = org;
+  *d = normalize(normalize(pip - org));
+  return true;
+}
+
+// ---------------------------------------------------------- intersection --
+DFC_D float gamma_n(int n) { const float e = 5.9604645e-8f; return (n * e) / (1.0f - n * e); }
+
+// geometry/shape/Triangle3F.java:505 watertight test; returns -1 on a miss.
+DFC_D float tri_t(V3 a, V3 b, V3 c, V3 o, V3 d, float tmin, float tmax) {
+  V3 p0 = a - o, p1 = b - o, p2 = c - o;
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  // permutation (kx, ky, kz) = (kz+1, kz+2, kz) mod 3
+  float dX, dY, dZ, x0, y0, z0, x1, y1, z1, x2, y2, z2;
+  if (kz == 0) { dX = d.y; dY = d.z; dZ = d.x; x0 = p0.y; y0 = p0.z; z0 = p0.x; x1 = p1.y; y1 = p1.z; z1 = p1.x; x2 = p2.y; y2 = p2.z; z2 = p2.x; }
+  else if (kz == 1) { dX = d.z; dY = d.x; dZ = d.y; x0 = p0.z; y0 = p0.x; z0 = p0.y; x1 = p1.z; y1 = p1.x; z1 = p1.y; x2 = p2.z; y2 = p2.x; z2 = p2.y; }
+  else { dX = d.x; dY = d.y; dZ = d.z; x0 = p0.x; y0 = p0.y; z0 = p0.z; x1 = p1.x; y1 = p1.y; z1 = p1.z; x2 = p2.x; y2 = p2.y; z2 = p2.z; }
+  const float sx = -dX / dZ, sy = -dY / dZ, sz = 1.0f / dZ;
+  x0 = x0 + sx * z0; y0 = y0 + sy * z0;
+  x1 = x1 + sx * z1; y1 = y1 + sy * z1;
+  x2 = x2 + sx * z2; y2 = y2 + sy * z2;
+  float e0 = x1 * y2 - y1 * x2;
+  float e1 = x2 * y0 - y2 * x0;
+  float e2 = x0 * y1 - y0 * x1;
+  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) {
+    e0 = (float)((double)y2 * (double)x1 - (double)x2 * (double)y1);
+    e1 = (float)((double)y0 * (double)x2 - (double)x0 * (double)y2);
+    e2 = (float)((double)y1 * (double)x0 - (double)x1 * (double)y0);
+  }
+  if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
+  const float det = e0 + e1 + e2;
+  if (det == 0.0f) return -1.0f;
+  z0 *= sz; z1 *= sz; z2 *= sz;
+  const float ts = e0 * z0 + e1 * z1 + e2 * z2;
+  if (det < 0.0f && (ts >= tmin || ts < tmax * det)) return -1.0f;
+  if (det > 0.0f && (ts <= tmin || ts > tmax * det)) return -1.0f;
+  const float inv = 1.0f / det;
+  const float t = ts * inv;
+  const float mz = fmaxf(fabsf(z0), fmaxf(fabsf(z1), fabsf(z2)));
+  const float mx = fmaxf(fabsf(x0), fmaxf(fabsf(x1), fabsf(x2)));
+  const float my = fmaxf(fabsf(y0), fmaxf(fabsf(y1), fabsf(y2)));
+  const float dz = gamma_n(3) * mz;
+  const float ddx = gamma_n(5) * (mx + mz);
+  const float ddy = gamma_n(5) * (my + mz);
+  const float de = 2.0f * (gamma_n(2) * mx * my + ddy * mx + ddx * my);
+  const float me = fmaxf(fabsf(e0), fmaxf(fabsf(e1), fabsf(e2)));
+  const float dt = 3.0f * (gamma_n(3) * me * mz + de * mz + dz * me) * fabsf(inv);
+  if (t <= dt) return -1.0f;
+  return t;
+}
+
+// utility/EFloat.java: running float interval for the sphere test.
+struct EF { float v, lo, hi; };
+DFC_D EF ef(float v) { return {v, v, v}; }
+DFC_D float nup(float v) { return nextafterf(v, __int_as_float(0x7f800000)); }
+DFC_D float ndn(float v) { return nextafterf(v, -__int_as_float(0x7f800000)); }
+DFC_D EF ef_add(EF a, EF b) { return {a.v + b.v, ndn(a.lo + b.lo), nup(a.hi + b.hi)}; }
+DFC_D EF ef_sub(EF a, EF b) { return {a.v - b.v, ndn(a.lo - b.hi), nup(a.hi - b.lo)}; }
+DFC_D EF ef_mul(EF a, EF b) {
+  float p0 = a.lo * b.lo, p1 = a.hi * b.lo, p2 = a.lo * b.hi, p3 = a.hi * b.hi;
+  return {a.v * b.v, ndn(fminf(fminf(p0, p1), fminf(p2, p3))), nup(fmaxf(fmaxf(p0, p1), fmaxf(p2, p3)))};
+}
+DFC_D EF ef_div(EF a, EF b) {
+  float v = a.v / b.v;
+  if (b.lo < 0.0f && b.hi > 0.0f) return {v, -__int_as_float(0x7f800000), __int_as_float(0x7f800000)};
+  float d0 = a.lo / b.lo, d1 = a.hi / b.lo, d2 = a.lo / b.hi, d3 = a.hi / b.hi;
+  return {v, ndn(fminf(fminf(d0, d1), fminf(d2, d3))), nup(fmaxf(fmaxf(d0, d1), fmaxf(d2, d3)))};
+}
+// geometry/shape/Sphere3F.java:507, unit sphere; returns -1 on a miss.
+DFC_D float sphere_t(V3 o, V3 d, float tmin, float tmax) {
+  EF ox = ef(o.x), oy = ef(o.y), oz = ef(o.z), dx = ef(d.x), dy = ef(d.y), dz = ef(d.z);
+  EF a = ef_add(ef_add(ef_mul(dx, dx), ef_mul(dy, dy)), ef_mul(dz, dz));
+  EF b = ef_mul(ef(2.0f), ef_add(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_mul(dz, oz)));
+  EF c = ef_sub(ef_add(ef_add(ef_mul(ox, ox), ef_mul(oy, oy)), ef_mul(oz, oz)), ef(1.0f));
+  double disc = (double)b.v * (double)b.v - 4.0 * (double)a.v * (double)c.v;
+  if (disc < 0.0) return -1.0f;
+  double root = sqrt(disc);
+  float fr = (float)root;
+  EF r = {fr, ndn(fr - 5.9604645e-8f * fr), nup(fr + 5.9604645e-8f * fr)};
+  if (fr == 0.0f) r = ef(0.0f);
+  EF q = b.v < 0.0f ? ef_mul(ef(-0.5f), ef_sub(b, r)) : ef_mul(ef(-0.5f), ef_add(b, r));
+  EF t0 = ef_div(q, a), t1 = ef_div(c, q);
+  if (t0.v > t1.v) { EF s = t0; t0 = t1; t1 = s; }
+  if (t0.hi > tmax || t1.lo <= tmin) return -1.0f;
+  EF th = t0;
+  if (th.lo <= 0.0f) { th = t1; if (th.hi > tmax) return -1.0f; }
+  return th.v;
+}
+
+// geometry/shape/Rectangle3F.java:368 over the compiled record (position, side A, side B, normal).
+DFC_D float rect_t(const float* q, V3 o, V3 d, float tmin, float tmax) {
+  V3 n = ld3(q + 9);
+  float dp = dot(n, d);
+  if (dp == 0.0f) return -1.0f;
+  V3 a = ld3(q), sa = ld3(q + 3), sb = ld3(q + 6);
+  float t = dot(a - o, n) / dp;
+  if (t <= tmin || t >= tmax) return -1.0f;
+  V3 ap = (o + d * t) - a;
+  float x = dot(ap, normalize(sa)), y = dot(ap, normalize(sb));
+  if (x >= 0.0f && x <= len(sa) && y >= 0.0f && y <= len(sb)) return t;
+  return -1.0f;
+}
+
+// geometry/shape/Plane3F.java (z = 0 in object space)
+DFC_D float plane_t(V3 o, V3 d, float tmin, float tmax) {
+  if (d.z == 0.0f) return -1.0f;
+  float t = -o.z / d.z;
+  return (t > tmin && t < tmax) ? t : -1.0f;
+}
+
+// ------------------------------------------------------------- surfaces --
+struct Surface { ONB g, s; V3 p; float tu, tv; };
+
+// geometry/shape/Triangle3F.java:1070-1160 surface at object-space distance t.
+DFC_D Surface triangle_surface(const float* q, V3 o, V3 d, float t) {
+  V3 A = ld3(q), B = ld3(q + 3), C = ld3(q + 6);
+  V3 eab = B - A, eca = A - C;
+  V3 d1 = cross(eab, eca);
+  float inv = 1.0f / dot(d, d1);
+  V3 d3 = cross(A - o, d);
+  float bu = dot(d3, eca) * inv, bv = dot(d3, eab) * inv, bw = 1.0f - bu - bv;
+  Surface s;
+  s.p = o + d * t;
+  s.tu = q[9] * bw + q[11] * bu + q[13] * bv;
+  s.tv = q[10] * bw + q[12] * bu + q[14] * bv;
+  s.g = onb_w(normalize(cross(normalize(B - A), normalize(C - A))));
+  V3 w = normalize(ld3(q + 15) * bw + ld3(q + 18) * bu + ld3(q + 21) * bv);
+  float ca0 = q[9] - q[13], ca1 = q[10] - q[14], cb0 = q[11] - q[13], cb1 = q[12] - q[14];
+  float det = ca0 * cb1 - ca1 * cb0;
+  if (det == 0.0f) {
+    s.s = onb_w(w);
+  } else {
+    float rd = 1.0f / det;
+    V3 ec = A - C, eb = B - C;
+    s.s = onb_wv(w, V3{(-cb0 * ec.x + ca0 * eb.x) * rd, (-cb0 * ec.y + ca0 * eb.y) * rd, (-cb0 * ec.z + ca0 * eb.z) * rd});
+  }
+  return s;
+}
+
+// geometry/shape/Sphere3F.java:243 surface (unit sphere, full).
+DFC_D Surface sphere_surface(V3 o, V3 d, float t) {
+  V3 p = o + d * t;
+  float sc = 1.0f / len(p);
+  p = p * sc;
+  if (p.x == 0.0f && p.y == 0.0f) p.x = 1.0e-5f;
+  float phi = atan2f(p.y, p.x);
+  if (phi < 0.0f) phi += 2.0f * kPi;
+  const float phiMax = 2.0f * kPi;
+  float theta = acosf(clampf(p.z, -1.0f, 1.0f));
+  float zr = sqrtf(p.x * p.x + p.y * p.y), zri = 1.0f / zr;
+  float cphi = p.x * zri, sphi = p.y * zri;
+  V3 dpdu = {-phiMax * p.y, phiMax * p.x, 0.0f};
+  V3 dpdv = V3{p.z * cphi, p.z * sphi, -sinf(theta)} * (-kPi);
+  Surface s;
+  s.g.w = normalize(cross(dpdu, dpdv)); s.g.v = dpdv; s.g.u = dpdu;  // stored unnormalized as the reference does
+  s.s = s.g;
+  s.p = p; s.tu = phi / phiMax; s.tv = (theta - kPi) / (0.0f - kPi);
+  return s;
+}
+
+DFC_D Surface rect_surface(const float* q, V3 o, V3 d, float t) {
+  Surface s;
+  V3 n = ld3(q + 9), a = ld3(q), b = a + ld3(q + 3), dd = a + ld3(q + 6);
+  s.p = o + d * t;
+  s.g = onb_w(n); s.s = s.g;
+  V3 na = {fabsf(n.x), fabsf(n.y), fabsf(n.z)};
+  bool isX = na.x > na.y && na.x > na.z, isY = na.y > na.z;
+  auto pr0 = [&](V3 p) { return isX ? p.y : (isY ? p.z : p.x); };
+  auto pr1 = [&](V3 p) { return isX ? p.z : (isY ? p.x : p.y); };
+  float vA0 = pr0(a), vA1 = pr1(a), vB0 = pr0(dd), vB1 = pr1(dd), vC0 = pr0(b), vC1 = pr1(b);
+  float ab0 = vB0 - vA0, ab1 = vB1 - vA1, ac0 = vC0 - vA0, ac1 = vC1 - vA1;
+  float di = 1.0f / (ab0 * ac1 - ab1 * ac0);
+  float h0 = pr0(s.p), h1 = pr1(s.p);
+  s.tu = h0 * (-ab1 * di) + h1 * (ab0 * di) + (vA0 * ab1 - vA1 * ab0) * di;
+  s.tv = h0 * (ac1 * di) + h1 * (-ac0 * di) + (ac0 * vA1 - ac1 * vA0) * di;
+  return s;
+}
+
+DFC_D Surface plane_surface(V3 o, V3 d, float t) {
+  Surface s;
+  s.p = o + d * t;
+  s.g.w = {0, 0, 1}; s.g.v = {0, 1, 0}; s.g.u = {1, 0, 0};
+  s.s = s.g;
+  s.tu = s.p.x; s.tv = s.p.y;
+  return s;
+}
+
+// geometry/SurfaceIntersection3F.java:372 object -> world for one primitive.
+DFC_D void surface_to_world(const DPrim& pr, Surface& s) {
+  if (pr.identity) {
+    s.g.u = normalize(s.g.u); s.g.v = normalize(s.g.v); s.g.w = normalize(s.g.w);
+    s.s.u = normalize(s.s.u); s.s.v = normalize(s.s.v); s.s.w = normalize(s.s.w);
+  } else {
+    s.g.u = normalize(xf_vec_t(pr.w2o, s.g.u)); s.g.v = normalize(xf_vec_t(pr.w2o, s.g.v)); s.g.w = normalize(xf_vec_t(pr.w2o, s.g.w));
+    s.s.u = normalize(xf_vec_t(pr.w2o, s.s.u)); s.s.v = normalize(xf_vec_t(pr.w2o, s.s.v)); s.s.w = normalize(xf_vec_t(pr.w2o, s.s.w));
+    s.p = xf_point(pr.o2w, s.p);
+  }
+  if (dot(s.s.w, s.g.w) < 0.0f) s.s.w = -s.s.w;  // OrthonormalBasis33F.flipW
+}
+
+// ---------------------------------------------------------------- BSDFs --
+enum { kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossy = 8, kSpecular = 16, kAll = 31, kAllButSpecular = 15 };
+enum : int { kLambert = 0, kOrenNayar = 1, kSpecBRDF = 2, kFresnelSpec = 3, kSpecBTDF = 4, kTSBRDF = 5, kTSBTDF = 6 };
+enum : int { kFresConst = 0, kFresDielectric = 1, kFresConductor = 2 };
+
+struct Lobe {
+  int kind, type, fresnel;
+  V3 scale, scale2;          // scale2: FresnelSpecular transmittance
+  float a, b;                // Oren-Nayar
+  float etaI, etaT;          // dielectric Fresnel
+  V3 cEta, cK;               // conductor Fresnel (etaI = 1)
+  float ax, ay;
+  float etaA, etaB;
+};
+struct Bsdf {
+  int n;
+  Lobe l[2];
+  float eta;
+  ONB s;
+  V3 ng, wo_w, wo;
+};
+
+DFC_D float fr_dielectric(float cosi, float etaI, float etaT) {  // scene/fresnel/DielectricFresnel.java
+  float c = clampf(cosi, -1.0f, 1.0f);
+  bool ent = c > 0.0f;
+  float ci = ent ? c : fabsf(c);
+  float ei = ent ? etaI : etaT, et = ent ? etaT : etaI;
+  float si = sqrtf(fmaxf(0.0f, 1.0f - ci * ci));
+  float st = ei / et * si;
+  if (st >= 1.0f) return 1.0f;
+  float ct = sqrtf(fmaxf(0.0f, 1.0f - st * st));
+  float rpa = ((et * ci) - (ei * ct)) / ((et * ci) + (ei * ct));
+  float rpe = ((ei * ci) - (et * ct)) / ((ei * ci) + (et * ct));
+  return (rpa * rpa + rpe * rpe) / 2.0f;
+}
+DFC_D float fr_conductor1(float c, float eta, float k) {  // scene/fresnel/ConductorFresnel.java, etaI = 1
+  c = clampf(c, -1.0f, 1.0f);
+  float c2 = c * c, s2 = 1.0f - c2, s4 = s2 * s2, eta2 = eta * eta, k2 = k * k;
+  float t0 = eta2 - k2 - s2;
+  float ab = sqrtf(t0 * t0 + eta2 * k2 * 4.0f);
+  float t1 = ab + c2, t2 = sqrtf((ab + t0) * 0.5f) * (c * 2.0f), t3 = ab * c2 + s4, t4 = t2 * s2;
+  float rs = (t1 - t2) / (t1 + t2);
+  float rp = rs * (t3 - t4) / (t3 + t4);
+  return (rp + rs) * 0.5f;
+}
+DFC_D V3 fresnel(const Lobe& L, float cosi) {
+  if (L.fresnel == kFresDielectric) { float f = fr_dielectric(cosi, L.etaI, L.etaT); return {f, f, f}; }
+  if (L.fresnel == kFresConductor) {
+    float c = fabsf(cosi);
+    return {fr_conductor1(c, L.cEta.x, L.cK.x), fr_conductor1(c, L.cEta.y, L.cK.y), fr_conductor1(c, L.cEta.z, L.cK.z)};
+  }
+  return {1, 1, 1};
+}
+
+DFC_D float sin2t(V3 v) { return fmaxf(0.0f, 1.0f - v.z * v.z); }
+DFC_D float sint(V3 v) { return sqrtf(sin2t(v)); }
+DFC_D float cosphi(V3 v) { float s = sint(v); return s == 0.0f ? 1.0f : clampf(v.x / s, -1.0f, 1.0f); }
+DFC_D float sinphi(V3 v) { float s = sint(v); return s == 0.0f ? 0.0f : clampf(v.y / s, -1.0f, 1.0f); }
+DFC_D bool same_hemi(V3 a, V3 b) { return a.z * b.z > 0.0f; }
+
+// scene/microfacet/TrowbridgeReitzMicrofacetDistribution.java
+DFC_D float tr_D(const Lobe& L, V3 h) {
+  float t2 = sin2t(h) / (h.z * h.z);
+  if (isinf(t2)) return 0.0f;
+  float cp = cosphi(h), sp = sinphi(h);
+  float c4 = (h.z * h.z) * (h.z * h.z);
+  float e = (cp * cp / (L.ax * L.ax) + sp * sp / (L.ay * L.ay)) * t2;
+  return 1.0f / (kPi * L.ax * L.ay * c4 * (1.0f + e) * (1.0f + e));
+}
+DFC_D float tr_lambda(const Lobe& L, V3 w) {
+  float ta = fabsf(sint(w) / w.z);
+  if (isinf(ta)) return 0.0f;
+  float cp = cosphi(w), sp = sinphi(w);
+  float al = sqrtf(cp * cp * L.ax * L.ax + sp * sp * L.ay * L.ay);
+  float x = (al * ta) * (al * ta);
+  return (-1.0f + sqrtf(1.0f + x)) / 2.0f;
+}
+DFC_D float tr_G(const Lobe& L, V3 wo, V3 wi) { return 1.0f / (1.0f + tr_lambda(L, wo) + tr_lambda(L, wi)); }
+DFC_D float tr_pdf(const Lobe& L, V3 wo, V3 h) {
+  return tr_D(L, h) * (1.0f / (1.0f + tr_lambda(L, wo))) * fabsf(dot(wo, h)) / fabsf(wo.z);
+}
+DFC_D V3 tr_visible(V3 w, float ax, float ay, float u, float v) {
+  V3 ws = normalize(V3{w.x * ax, w.y * ay, w.z});
+  float ct = ws.z, sx, sy;
+  if (ct > 0.9999f) {
+    float r = sqrtf(u / (1.0f - u)), s, c;
+    sincosf(2.0f * kPi * v, &s, &c);
+    sx = r * c; sy = r * s;
+  } else {
+    float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), tt = st / ct;
+    float a = 2.0f / (1.0f + sqrtf(1.0f + 1.0f / ((1.0f / tt) * (1.0f / tt))));
+    float b = 2.0f * u / a - 1.0f;
+    float c = fminf(1.0f / (b * b - 1.0f), 1.0e10f);
+    float e = sqrtf(fmaxf(tt * tt * c * c - (b * b - tt * tt) * c, 0.0f));
+    float f = tt * c - e, g = tt * c + e;
+    float hs = v > 0.5f ? 1.0f : -1.0f;
+    float i = v > 0.5f ? 2.0f * (v - 0.5f) : 2.0f * (0.5f - v);
+    float j = (i * (i * (i * 0.27385f - 0.73369f) + 0.46341f)) / (i * (i * (i * 0.093073f + 0.309420f) - 1.0f) + 0.597999f);
+    sx = (b < 0.0f || g > 1.0f / tt) ? f : g;
+    sy = hs * j * sqrtf(1.0f + sx * sx);
+  }
+  float cp = cosphi(ws), sp = sinphi(ws);
+  return normalize(V3{-((cp * sx - sp * sy) * ax), -((sp * sx + cp * sy) * ay), 1.0f});
+}
+DFC_D V3 tr_sample_h(const Lobe& L, V3 wo, float u, float v) {
+  return wo.z >= 0.0f ? tr_visible(wo, L.ax, L.ay, u, v) : -tr_visible(-wo, L.ax, L.ay, u, v);
+}
+DFC_D bool refract(V3 d, V3 n, float eta, V3* out) {  // geometry/Vector3F.java:454
+  float ci = dot(d, n);
+  float st2 = eta * eta * fmaxf(0.0f, 1.0f - ci * ci);
+  if (st2 >= 1.0f) return false;
+  *out = (-d) * eta + n * (eta * ci - sqrtf(1.0f - st2));
+  return true;
+}
+
+DFC_D V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
+  switch (L.kind) {
+    case kLambert: return L.scale * (1.0f / kPi);
+    case kOrenNayar: {
+      float ci = fabsf(wi.z), co = fabsf(wo.z), si = sint(wi), so = sint(wo);
+      float mc = (si > 1.0e-4f && so > 1.0e-4f) ? fmaxf(0.0f, cosphi(wi) * cosphi(wo) + sinphi(wi) * sinphi(wo)) : 0.0f;
+      float sa = ci > co ? so : si, tb = ci > co ? si / ci : so / co;
+      return L.scale * (1.0f / kPi) * (L.a + L.b * mc * sa * tb);
+    }
+    case kTSBRDF: {
+      float co = fabsf(wo.z), ci = fabsf(wi.z);
+      if (co == 0.0f || ci == 0.0f) return {0, 0, 0};
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      V3 hf = h.z < 0.0f ? -h : h;
+      V3 F = fresnel(L, dot(wi, hf));
+      return mul(L.scale * (tr_D(L, h) * tr_G(L, wo, wi)), F) * (1.0f / (4.0f * ci * co));
+    }
+    case kTSBTDF: {
+      if (same_hemi(wo, wi)) return {0, 0, 0};
+      if (wi.z == 0.0f || wo.z == 0.0f) return {0, 0, 0};
+      float eta = wo.z > 0.0f ? L.etaB / L.etaA : L.etaA / L.etaB;
+      V3 h = normalize(wi * eta + wo);
+      if (h.z < 0.0f) h = -h;
+      float oh = dot(wo, h), ih = dot(wi, h);
+      if (oh * ih > 0.0f) return {0, 0, 0};
+      float F = fr_dielectric(oh, L.etaA, L.etaB);
+      float a = oh + eta * ih, b = 1.0f / eta;
+      float k = fabsf(tr_D(L, h) * tr_G(L, wo, wi) * eta * eta * fabsf(ih) * fabsf(oh) * b * b / (wi.z * wo.z * a * a));
+      return L.scale * ((1.0f - F) * k);
+    }
+    default: return {0, 0, 0};
+  }
+}
+DFC_D float lobe_pdf(const Lobe& L, V3 wo, V3 wi) {
+  switch (L.kind) {
+    case kLambert: case kOrenNayar: return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
+    case kTSBRDF: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      V3 h = normalize(wo + wi);
+      return tr_pdf(L, wo, h) / (4.0f * dot(wo, h));
+    }
+    case kTSBTDF: {
+      if (same_hemi(wo, wi)) return 0.0f;
+      float eta = wo.z > 0.0f ? L.etaB / L.etaA : L.etaA / L.etaB;
+      V3 h = normalize(wi * eta + wo);
+      float oh = dot(wo, h), ih = dot(wi, h);
+      if (oh * ih > 0.0f) return 0.0f;
+      float a = oh + eta * ih;
+      return tr_pdf(L, wo, h) * fabsf((eta * eta * ih) / (a * a));
+    }
+    default: return 0.0f;
+  }
+}
+struct LSample { V3 f, wi; float pdf; int type; };
+DFC_D bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LSample* s) {
+  s->type = L.type;
+  switch (L.kind) {
+    case kLambert: case kOrenNayar: {
+      V3 wi = cosine_hemisphere(u, v);
+      if (wo.z < 0.0f) wi.z = -wi.z;
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+    }
+    case kSpecBRDF: {
+      V3 wi = {-wo.x, -wo.y, wo.z};
+      s->wi = wi; s->f = mul(fresnel(L, wi.z), L.scale) * (1.0f / fabsf(wi.z)); s->pdf = 1.0f; return true;
+    }
+    case kSpecBTDF: case kFresnelSpec: {
+      float F = L.kind == kFresnelSpec ? fr_dielectric(wo.z, L.etaA, L.etaB) : 0.0f;
+      if (L.kind == kFresnelSpec && u < F) {
+        V3 wi = {-wo.x, -wo.y, wo.z};
+        s->type = kSpecular | kRefl; s->wi = wi; s->f = L.scale * (F / fabsf(wi.z)); s->pdf = F; return true;
+      }
+      bool ent = wo.z > 0.0f;
+      float ei = ent ? L.etaA : L.etaB, et = ent ? L.etaB : L.etaA;
+      V3 n = wo.z < 0.0f ? V3{0, 0, -1} : V3{0, 0, 1};
+      V3 wi;
+      if (!refract(wo, n, ei / et, &wi)) return false;
+      if (L.kind == kSpecBTDF) {
+        float Ft = fr_dielectric(wi.z, L.etaA, L.etaB);
+        s->wi = wi; s->f = L.scale * ((1.0f - Ft) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f; return true;
+      }
+      s->type = kSpecular | kTrans; s->wi = wi;
+      s->f = L.scale2 * ((1.0f - F) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f - F; return true;
+    }
+    case kTSBRDF: {
+      if (wo.z == 0.0f) return false;
+      V3 h = tr_sample_h(L, wo, u, v);
+      if (dot(wo, h) < 0.0f) return false;
+      V3 wi = h * (dot(wo, h) * 2.0f) - wo;
+      if (!same_hemi(wo, wi)) return false;
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = tr_pdf(L, wo, h) / (4.0f * dot(wo, h)); return true;
+    }
+    case kTSBTDF: {
+      if (wo.z == 0.0f) return false;
+      V3 h = tr_sample_h(L, wo, u, v);
+      if (dot(wo, h) < 0.0f) return false;
+      float eta = wo.z > 0.0f ? L.etaA / L.etaB : L.etaB / L.etaA;
+      V3 wi;
+      if (!refract(wo, h, eta, &wi)) return false;
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+    }
+  }
+  return false;
+}
+DFC_D bool type_match(int t, int flags) { return (t & flags) == t; }
+DFC_D bool is_spec(int t) { return (t & kSpecular) != 0; }
+
+DFC_D Lobe tr_lobe(int kind, int type, V3 scale, float ax, float ay) {
+  Lobe L = {};
+  L.kind = kind; L.type = type; L.scale = scale; L.ax = fmaxf(ax, 0.001f); L.ay = fmaxf(ay, 0.001f);
+  return L;
+}
+
+// Material.computeScatteringFunctions(intersection, RADIANCE, isAllowingMultipleLobes = true)
+// for the resolved kinds (scene/material/{Matte,Mirror,Glass,Metal,Plastic}Material.java).
+DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, Bsdf* B) {
+  B->n = 0; B->eta = 1.0f;
+  switch (m.kind) {
+    case kMatLambert: case kMatOrenNayar: {
+      Lobe L = {};
+      L.kind = m.kind == kMatLambert ? kLambert : kOrenNayar; L.type = kRefl | kDiffuse; L.scale = ld3(m.c0); L.a = m.on_a; L.b = m.on_b;
+      B->l[B->n++] = L; break;
+    }
+    case kMatMirror: {
+      Lobe L = {}; L.kind = kSpecBRDF; L.type = kRefl | kSpecular; L.scale = ld3(m.c0); L.fresnel = kFresConst;
+      B->l[B->n++] = L; break;
+    }
+    case kMatGlassSpec: {
+      Lobe L = {}; L.kind = kFresnelSpec; L.type = kRefl | kTrans | kSpecular; L.scale = ld3(m.c0); L.scale2 = ld3(m.c1);
+      L.etaA = 1.0f; L.etaB = m.eta;
+      B->l[B->n++] = L; B->eta = m.eta; break;
+    }
+    case kMatGlassRough: {
+      if (m.has_kr) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay); L.fresnel = kFresDielectric; L.etaI = 1.0f; L.etaT = m.eta; B->l[B->n++] = L; }
+      if (m.has_kt) { Lobe L = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c1), m.ax, m.ay); L.etaA = 1.0f; L.etaB = m.eta; B->l[B->n++] = L; }
+      B->eta = m.eta; break;
+    }
+    case kMatMetal: {
+      Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, V3{1, 1, 1}, m.ax, m.ay);
+      L.fresnel = kFresConductor; L.cEta = ld3(m.c1); L.cK = ld3(m.c2);
+      B->l[B->n++] = L; break;
+    }
+    case kMatPlastic: {
+      if (m.has_kr) { Lobe L = {}; L.kind = kLambert; L.type = kRefl | kDiffuse; L.scale = ld3(m.c0); B->l[B->n++] = L; }
+      if (m.has_kt) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; L.etaI = 1.5f; L.etaT = 1.0f; B->l[B->n++] = L; }
+      break;
+    }
+    default: return false;
+  }
+  B->s = sf.s;
+  B->ng = sf.g.w;
+  B->wo_w = -ray_d;
+  B->wo = normalize(to_local(B->wo_w, B->s));
+  return B->n > 0;
+}
+DFC_D V3 bsdf_f(const Bsdf& B, int flags, V3 wi_w) {
+  V3 wi = normalize(to_local(wi_w, B.s));
+  bool refl = dot(wi_w, B.ng) * dot(B.wo_w, B.ng) > 0.0f;
+  V3 r = {0, 0, 0};
+  for (int k = 0; k < B.n; ++k) {
+    const Lobe& L = B.l[k];
+    if (type_match(L.type, flags) && ((refl && (L.type & kRefl)) || (!refl && (L.type & kTrans)))) r = r + lobe_f(L, B.wo, wi);
+  }
+  return r;
+}
+DFC_D float bsdf_pdf(const Bsdf& B, int flags, V3 wi_w) {
+  if (B.n == 0 || B.wo.z == 0.0f) return 0.0f;
+  V3 wi = normalize(to_local(wi_w, B.s));
+  float p = 0.0f;
+  int m = 0;
+  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) { ++m; p += lobe_pdf(B.l[k], B.wo, wi); }
+  return m > 1 ? p / m : p;
+}
+struct BSample { V3 f, wi; float pdf; int type; };
+// scene/BSDF.java:323 sampleDistributionFunction
+DFC_D bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BSample* out) {
+  if (B.wo.z == 0.0f) return false;
+  int idx[2], m = 0;
+  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) idx[m++] = k;
+  if (m == 0) return false;
+  int match = min((int)floorf(u * m), m - 1);
+  const Lobe& L = B.l[idx[match]];
+  LSample s;
+  if (!lobe_sample(L, B.wo, fminf(u * m - match, 0.99999994f), v, &s)) return false;
+  V3 wiw = normalize(to_world(s.wi, B.s));
+  V3 f = s.f;
+  float pdf = s.pdf;
+  if (!is_spec(L.type)) {
+    bool refl = dot(wiw, B.ng) * dot(B.wo_w, B.ng) > 0.0f;
+    f = {0, 0, 0};
+    for (int k = 0; k < m; ++k) {
+      const Lobe& O = B.l[idx[k]];
+      if (k != match) pdf += lobe_pdf(O, B.wo, s.wi);
+      if ((refl && (O.type & kRefl)) || (!refl && (O.type & kTrans))) f = f + lobe_f(O, B.wo, s.wi);
+    }
+  }
+  if (m > 1) pdf /= m;
+  out->f = f; out->wi = wiw; out->pdf = pdf; out->type = s.type;
+  return true;
+}
+DFC_D int bsdf_nonspec(const Bsdf& B) { int c = 0; for (int k = 0; k < B.n; ++k) c += is_spec(B.l[k].type) ? 0 : 1; return c; }
+
+// ---------------------------------------------------------------- lights --
+// sampler/Distribution1F.java + Distribution2F.java over the packed array form.
+DFC_D int d1_index(const float* a, int off, float value) {
+  int lenc = (int)a[off + 1], mn = 0, cl = lenc;
+  while (cl > 0) {
+    int half = cl >> 1, mid = mn + half;
+    if (a[off + 4 + mid] <= value) { mn = mid + 1; cl -= half + 1; } else { cl = half; }
+  }
+  int r = mn - 1;
+  return r < 0 ? 0 : (r > lenc - 2 ? lenc - 2 : r);
+}
+DFC_D float d1_remap(const float* a, int off, float value, int i) {
+  float n = a[off + 2], c0 = a[off + 4 + i], c1 = a[off + 4 + i + 1];
+  if (c1 - c0 > 0.0f) return (i + ((value - c0) / (c1 - c0))) / n;
+  return (i + (value - c0)) / n;
+}
+DFC_D void d2_remap(const float* a, float su, float sv, float* ou, float* ov) {
+  bool uv = (int)a[0] != 0;
+  float m = uv ? su : sv, c = uv ? sv : su;
+  int offM = (int)a[2];
+  int iM = d1_index(a, offM, m);
+  int offC = (int)a[3 + iM];
+  int iC = d1_index(a, offC, c);
+  float mr = d1_remap(a, offM, m, iM), cr = d1_remap(a, offC, c, iC);
+  *ou = uv ? mr : cr; *ov = uv ? cr : mr;
+}
+DFC_D float d2_pdf(const float* a, float su, float sv) {
+  bool uv = (int)a[0] != 0;
+  float m = uv ? su : sv, c = uv ? sv : su;
+  int offM = (int)a[2];
+  int nM = (int)a[offM + 2];
+  int iM = max(0, min((int)(m * nM), nM - 1));
+  int offC = (int)a[3 + iM];
+  int nC = (int)a[offC + 2];
+  int iC = max(0, min((int)(c * nC), nC - 1));
+  return a[offC + 4 + iC + (int)a[offC + 1]] / a[offM + 3];
+}
+
+// scene/light/PerezLight.java doRadianceSky (renderer/gpu/AbstractLightKernel.java:1615 form).
+DFC_D V3 perez_sky(const float* q, V3 dir) {
+  if (dir.z < 0.0f) return {0, 0, 0};
+  V3 ds = normalize(V3{dir.x, dir.y, fmaxf(dir.z, 0.001f)});
+  const float T = q[41];
+  const float theta = acosf(clampf(ds.z, -1.0f, 1.0f));
+  const float gamma = acosf(clampf(dot(ds, ld3(q + 35)), -1.0f, 1.0f));
+  const float thS = q[46], cs = cosf(thS), cs2 = cs * cs, cg = cosf(gamma), cg2 = cg * cg, ict = 1.0f / cosf(theta);
+  auto perez = [&](float l0, float l1, float l2, float l3, float l4, float z) {
+    return z * ((1.0f + l0 * expf(l1 * ict)) * (1.0f + l2 * expf(l3 * gamma) + l4 * cg2)) / ((1.0f + l0 * expf(l1)) * (1.0f + l2 * expf(l3 * thS) + l4 * cs2));
+  };
+  float Y = perez(0.17872f * T - 1.46303f, -0.35540f * T + 0.42749f, -0.02266f * T + 5.32505f, 0.12064f * T - 2.57705f, -0.06696f * T + 0.37027f, q[42]) * 0.0001f;
+  float x = perez(-0.01925f * T - 0.25922f, -0.06651f * T + 0.00081f, -0.00041f * T + 0.21247f, -0.06409f * T - 0.89887f, -0.00325f * T + 0.04517f, q[43]);
+  float y = perez(-0.01669f * T - 0.26078f, -0.09495f * T + 0.00921f, -0.00792f * T + 0.21023f, -0.04405f * T - 1.65369f, -0.01092f * T + 0.05291f, q[44]);
+  float den = 0.0241f + 0.2562f * x - 0.7341f * y;
+  float m1 = (-1.3515f - 1.7703f * x + 5.9114f * y) / den;
+  float m2 = (0.03f - 31.4424f * x + 30.0717f * y) / den;
+  float X = 95.6824722290f + m1 * 1.7548348904f + m2 * 1.9917192459f;
+  float Yc = 99.7036819458f + m1 * 1.8025954962f + m2 * 0.7136800885f;
+  float Z = 115.5248031616f + m1 * 32.5218048096f + m2 * -2.1984319687f;
+  float cx = X * Y / Yc, cy = Y, cz = Z * Y / Yc;
+  // sRGB XYZ -> RGB (color/ColorSpaceF.java:85), matrix derived from the sRGB primaries
+  return {3.2404542f * cx - 1.5371385f * cy - 0.4985314f * cz, -0.9692660f * cx + 1.8760108f * cy + 0.0415560f * cz,
+          0.0556434f * cx - 0.2040259f * cy + 1.0572252f * cz};
+}
+DFC_D V3 sat0(V3 c) { return {fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f)}; }
+
+struct LightS { V3 L, p, wi; float pdf; };
+
+// Light.sampleRadianceIncoming for each supported light type.
+DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf, float u, float v, float sun_pick, LightS* o) {
+  const V3 p = sf.p;
+  switch (lt.type) {
+    case kLightDiffuseArea: {
+      V3 ref = xf_point(lt.w2o, p);
+      V3 sp, sn;
+      float pdf;
+      if (lt.shape == kShapeTriangle) {
+        // Triangle3F.sample(Point2F) + Shape3F.sample(sample, ref): the solid-angle
+        // pdf there is dist^2/|cos| (the area density of the point is not applied).
+        const float* q = S.tri_attr + (size_t)lt.shape_data * 24;
+        float su = sqrtf(u), b0 = 1.0f - su, b1 = v * su, b2 = 1.0f - b0 - b1;
+        V3 A = ld3(q), B = ld3(q + 3), C = ld3(q + 6);
+        sp = {A.x * b0 + B.x * b1 + C.x * b2, A.y * b0 + B.y * b1 + C.y * b2, A.z * b0 + B.z * b1 + C.z * b2};
+        sn = normalize(ld3(q + 15) * b0 + ld3(q + 18) * b1 + ld3(q + 21) * b2);
+        V3 inc = sp - ref;
+        if (dot(inc, inc) == 0.0f) return false;
+        V3 incn = normalize(inc);
+        pdf = dot(inc, inc) / fabsf(dot(sn, -incn));
+        if (isinf(pdf) || isnan(pdf)) return false;
+      } else if (lt.shape == kShapeSphere) {
+        if (dot(ref, ref) <= 1.0f) {
+          float ct = 1.0f - 2.0f * u, st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), s, c;
+          sincosf(v * 2.0f * kPi, &s, &c);
+          sp = {st * c, st * s, ct};
+          sn = normalize(sp);
+          V3 inc = sp - ref;
+          if (dot(inc, inc) == 0.0f) return false;
+          pdf = dot(inc, inc) / fabsf(dot(sn, -normalize(inc)));
+          if (isinf(pdf) || isnan(pdf)) return false;
+        } else {
+          float dist = len(ref), dr = 1.0f / dist;
+          V3 dc = (-ref) * dr;
+          ONB b = onb_w(dc);
+          float stm2 = dr * dr, stmr = dist;
+          float ctm = sqrtf(fmaxf(0.0f, 1.0f - stm2));
+          float ct = stm2 < 0.00068523f ? sqrtf(1.0f - stm2 * u) : (ctm - 1.0f) * u + 1.0f;
+          float st2 = stm2 < 0.00068523f ? stm2 * u : 1.0f - ct * ct;
+          float ca = st2 * stmr + ct * sqrtf(fmaxf(0.0f, 1.0f - st2 * stmr * stmr));
+          float sa = sqrtf(fmaxf(0.0f, 1.0f - ca * ca)), s, c;
+          sincosf(v * 2.0f * kPi, &s, &c);
+          V3 sd = (-b.u) * (sa * c) + (-b.v) * (sa * s) + (-b.w) * ca;
+          sp = sd; sn = normalize(sd); pdf = 1.0f / (2.0f * kPi * (1.0f - ctm));
+        }
+      } else {
+        return false;  // Shape3F.sample default: no sample for other shapes
+      }
+      V3 pw = xf_point(lt.o2w, sp);
+      V3 nw = normalize(xf_vec_t(lt.w2o, sn));
+      V3 wi = normalize(pw - p);
+      if (pdf > 0.0f && (lt.two_sided || dot(nw, -wi) > 0.0f)) { *o = LightS{ld3(lt.radiance), pw, wi, pdf}; return true; }
+      return false;
+    }
+    case kLightPoint: {
+      V3 pos = ld3(lt.pos);
+      V3 d = pos - p;
+      *o = LightS{ld3(lt.radiance) * (1.0f / dot(d, d)), pos, normalize(d), 1.0f};
+      return true;
+    }
+    case kLightSpot: {
+      V3 pos = ld3(lt.pos);
+      V3 d = pos - p;
+      V3 wi = normalize(d);
+      V3 dobj = normalize(xf_vec(lt.w2o, -wi));
+      float ct = dobj.z, fall;
+      if (ct < lt.cos_cone) fall = 0.0f;
+      else if (ct >= lt.cos_cone_delta) fall = 1.0f;
+      else { float t = (ct - lt.cos_cone) / (lt.cos_cone_delta - lt.cos_cone); fall = (t * t) * (t * t); }
+      *o = LightS{ld3(lt.radiance) * (fall / dot(d, d)), pos, wi, 1.0f};
+      return true;
+    }
+    case kLightDirectional: {
+      V3 d = ld3(lt.dir);
+      *o = LightS{ld3(lt.radiance), p + d * (2.0f * lt.radius), d, 1.0f};
+      return true;
+    }
+    case kLightPerez: {
+      const float* q = S.perez + lt.perez;
+      const float* dist = q + 48;
+      V3 sunW = ld3(q + 38), sunO = ld3(q + 35);
+      if (dot(sunW, sf.g.w) > sun_pick && dot(sunW, sf.s.w) > sun_pick) {
+        float st = sint(sunO);
+        if (st != 0.0f) {
+          float phi = atan2f(sunO.y, sunO.x);
+          if (phi < 0.0f) phi += 2.0f * kPi;
+          float pdf = d2_pdf(dist, phi * (1.0f / (2.0f * kPi)), acosf(clampf(sunO.z, -1.0f, 1.0f)) * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
+          if (pdf != 0.0f) { *o = LightS{ld3(q + 32), p + sunW * (2.0f * q[45]), sunW, pdf}; return true; }
+        }
+      }
+      float ru, rv;
+      d2_remap(dist, u, v, &ru, &rv);
+      float pr = d2_pdf(dist, ru, rv);
+      if (pr == 0.0f) return false;
+      float sth, cth, sph, cph;
+      sincosf(rv * kPi, &sth, &cth);
+      sincosf(ru * 2.0f * kPi, &sph, &cph);
+      V3 dobj = {sth * cph, sth * sph, cth};
+      V3 dw = normalize(xf_vec(q, dobj));
+      float st = sint(dobj);
+      if (st == 0.0f) return false;
+      *o = LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
+      return true;
+    }
+  }
+  return false;
+}
+
+DFC_D bool light_is_delta(int type) { return type == kLightPoint || type == kLightSpot || type == kLightDirectional; }
+
+// Light.evaluateRadianceEmitted(Ray3F): only the sky emits along a missed ray.
+DFC_D V3 light_Le_miss(const SceneView& S, const DLight& lt, V3 d) {
+  if (lt.type != kLightPerez) return {0, 0, 0};
+  const float* q = S.perez + lt.perez;
+  return sat0(perez_sky(q, normalize(xf_vec(q + 16, d))));
+}
+
+// Perez part of Light.evaluateProbabilityDensityFunctionRadianceIncoming.
+DFC_D float perez_pdf(const SceneView& S, const DLight& lt, V3 wi) {
+  const float* q = S.perez + lt.perez;
+  V3 d = normalize(xf_vec(q + 16, wi));
+  float th = acosf(clampf(d.z, -1.0f, 1.0f));
+  float st = sinf(th);
+  if (st == 0.0f) return 0.0f;
+  float phi = atan2f(d.y, d.x);
+  if (phi < 0.0f) phi += 2.0f * kPi;
+  return d2_pdf(q + 48, phi * (1.0f / (2.0f * kPi)), th * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
+}
+
+}  // namespace dfc

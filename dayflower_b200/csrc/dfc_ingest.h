@@ -1,0 +1,39 @@
+// Host-side scene ingest: reference compiled arrays -> device records.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/dayflower_cuda.h"
+#include "dfc_scene.h"
+
+namespace dfc {
+
+// Arrays staged by dfc_scene_put, by reference field name.
+struct Staged {
+  std::map<std::string, std::vector<float>> f32;
+  std::map<std::string, std::vector<int32_t>> i32;
+};
+
+struct HostScene {
+  std::vector<DPrim> prims;
+  std::vector<DMaterial> materials;
+  std::vector<DLight> lights;
+  std::vector<BVH4Node> nodes;
+  std::vector<int> tlas_items;
+  std::vector<int> unbounded;
+  std::vector<int> unbounded_storage;  // non-empty stand-in when there are no unbounded primitives
+  std::vector<F4> tri_pos;
+  std::vector<float> tri_attr, rects, perez;
+  float camera[19] = {0};
+  int tlas_root = -1;
+  int lights_storage_pad = 0;  // 1 when `lights` holds only a placeholder
+  int64_t triangles = 0;
+};
+
+// Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.
+int ingest_scene(const Staged& st, int layout, HostScene* out, std::string* err);
+
+}  // namespace dfc

@@ -1,0 +1,626 @@
+// Wavefront kernels of the B200 render path.
+//
+// One render pass (renderer/gpu/AbstractGPURenderer.java:231-297: one sample
+// per pixel) runs as
+//   raygen -> [trace -> shade] x bounces -> final shade
+// over fixed per-path slots.  A path owns three ray slots (extension, shadow,
+// MIS) and a state record; shade appends the rays it spawns to a compacted
+// ray list and the paths that still have work to a compacted work list, both
+// with one atomic per warp (ballot + popc).  The trace kernel is a persistent
+// grid-stride loop over the ray list walking the two-level 4-wide BVH with a
+// per-thread stack in shared memory.  The path semantics are those of
+// scene/Scene.java:451-619 (radiancePathTracer) with doEstimateDirectLight
+// (:1530) split into a shadow ray and a MIS ray whose results are folded in
+// by the next shade step.
+#include <cuda_runtime.h>
+
+#include "dfc_device.cuh"
+#include "dfc_kernels.h"
+
+namespace dfc {
+
+namespace {
+
+constexpr int kStack = 48;  // traversal stack entries per thread (shared memory)
+constexpr int kTraceBlock = 128;
+
+DFC_D unsigned warp_append(unsigned* counter, bool pred) {
+  const unsigned mask = __ballot_sync(0xffffffffu, pred);
+  const unsigned lane = threadIdx.x & 31u;
+  const int leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (mask != 0u && (int)lane == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
+  return base + (unsigned)__popc(mask & ((1u << lane) - 1u));
+}
+
+// ---- traversal --------------------------------------------------------------
+struct Hit { float t; int prim; int aux; float t_obj; };
+
+struct ObjRay { V3 o, d, inv; float s; };
+DFC_D ObjRay obj_ray(const DPrim& pr, V3 o, V3 d) {
+  ObjRay r;
+  if (pr.identity) { r.o = o; r.d = d; r.s = 1.0f; }
+  else {
+    r.o = xf_point(pr.w2o, o);
+    V3 dr = xf_vec(pr.w2o, d);
+    float l = len(dr);
+    if (l >= 0.99999982f && l <= 1.00000012f) { r.d = dr; r.s = 1.0f; }
+    else { r.d = V3{dr.x / l, dr.y / l, dr.z / l}; r.s = l; }
+  }
+  r.inv = V3{1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
+  return r;
+}
+
+// Object-space test of one analytic primitive; returns the object distance or -1.
+DFC_D float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
+  switch (pr.shape) {
+    case kShapeSphere: return sphere_t(r.o, r.d, kTMin, tmax_obj);
+    case kShapeTriangle: {
+      const float* q = S.tri_attr + (size_t)pr.data * 24;
+      return tri_t(ld3(q), ld3(q + 3), ld3(q + 6), r.o, r.d, kTMin, tmax_obj);
+    }
+    case kShapeRectangle: return rect_t(S.rects + (size_t)pr.data * 16, r.o, r.d, kTMin, tmax_obj);
+    case kShapePlane: return plane_t(r.o, r.d, kTMin, tmax_obj);
+    default: return -1.0f;
+  }
+}
+
+// 4 child slab tests of one node; returns a hit mask and the entry distances.
+DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin, float tmax, float tn[4]) {
+  const float4* p = reinterpret_cast<const float4*>(nodes + ni);
+  const float4 lx = __ldg(p + 0), ly = __ldg(p + 1), lz = __ldg(p + 2), hx = __ldg(p + 3), hy = __ldg(p + 4), hz = __ldg(p + 5);
+  const float ox = -o.x * inv.x, oy = -o.y * inv.y, oz = -o.z * inv.z;
+  const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
+  const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+  unsigned mask = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float x0 = fmaf(lxa[k], inv.x, ox), x1 = fmaf(hxa[k], inv.x, ox);
+    float y0 = fmaf(lya[k], inv.y, oy), y1 = fmaf(hya[k], inv.y, oy);
+    float z0 = fmaf(lza[k], inv.z, oz), z1 = fmaf(hza[k], inv.z, oz);
+    float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    float tfar = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax)) * 1.0000004f;
+    tn[k] = tnear;
+    if (tnear <= tfar && lxa[k] <= hxa[k]) mask |= 1u << k;
+  }
+  return mask;
+}
+
+// Closest (or any) hit in (kTMin, tmax) along a world ray.  stack points at
+// this thread's column of the block's shared stack (stride kTraceBlock).
+// Stack entries: >= 0 node index; -1 end of a bottom level (back to world
+// space); <= -2 enter the bottom level of mesh primitive (-2 - entry).
+template <bool kAny>
+DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* stack, unsigned* overflow) {
+  float best = tmax;
+  bool found = false;
+  for (int u = 0; u < S.unbounded_count; ++u) {
+    const int pi = S.unbounded[u];
+    const DPrim& pr = S.prims[pi];
+    ObjRay r = obj_ray(pr, o, d);
+    float to = prim_t(S, pr, r, best * r.s);
+    if (to > 0.0f) {
+      float tw = to / r.s;
+      if (tw < best) {
+        best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;
+        if (kAny) { out->t = best; return true; }
+      }
+    }
+  }
+  if (S.tlas_root < 0) { out->t = best; return found; }
+  const V3 winv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  int sp = 0;
+  stack[(sp++) * kTraceBlock] = S.tlas_root;
+  bool in_blas = false;
+  ObjRay br;
+  br.s = 1.0f;
+  int bprim = -1;
+  float bbest = 0.0f;
+  while (sp > 0) {
+    const int e = stack[(--sp) * kTraceBlock];
+    if (e == -1) {
+      in_blas = false;
+      best = fminf(best, bbest / br.s);
+      continue;
+    }
+    if (e <= -2) {
+      bprim = -2 - e;
+      const DPrim& pm = S.prims[bprim];
+      br = obj_ray(pm, o, d);
+      bbest = best * br.s;
+      in_blas = true;
+      if (sp + 2 > kStack) { atomicAdd(overflow, 1u); in_blas = false; continue; }
+      stack[(sp++) * kTraceBlock] = -1;
+      stack[(sp++) * kTraceBlock] = pm.data;
+      continue;
+    }
+    float tn[4];
+    const unsigned mask = in_blas ? node_hits(S.nodes, e, br.o, br.inv, 0.0f, bbest, tn) : node_hits(S.nodes, e, o, winv, 0.0f, best, tn);
+    if (!mask) continue;
+    const int4* cp = reinterpret_cast<const int4*>(S.nodes + e) + 6;
+    const int4 ch = __ldg(cp), cn = __ldg(cp + 1);
+    const int cha[4] = {ch.x, ch.y, ch.z, ch.w}, cna[4] = {cn.x, cn.y, cn.z, cn.w};
+    int ent[4];
+    float entt[4];
+    int nent = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!(mask & (1u << k))) continue;
+      const int c = cha[k];
+      if (c >= 0) { ent[nent] = c; entt[nent] = tn[k]; ++nent; continue; }
+      const int first = ~c, cnt = cna[k];
+      if (in_blas) {
+        for (int j = 0; j < cnt; ++j) {
+          const int ti = first + j;
+          const float4* tp = reinterpret_cast<const float4*>(S.tri_pos) + 3 * ti;
+          const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+          const float t = tri_t(V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, V3{cc.x, cc.y, cc.z}, br.o, br.d, kTMin, bbest);
+          if (t > 0.0f && t < bbest) {
+            bbest = t; found = true;
+            out->prim = bprim; out->aux = __float_as_int(a.w); out->t_obj = t;
+            if (kAny) { out->t = t / br.s; return true; }
+          }
+        }
+      } else {
+        const int pi = S.tlas_items[first];
+        const DPrim& pr = S.prims[pi];
+        if (pr.shape == kShapeMesh) { ent[nent] = -2 - pi; entt[nent] = tn[k]; ++nent; continue; }
+        ObjRay r = obj_ray(pr, o, d);
+        const float to = prim_t(S, pr, r, best * r.s);
+        if (to > 0.0f) {
+          const float tw = to / r.s;
+          if (tw < best) {
+            best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;
+            if (kAny) { out->t = best; return true; }
+          }
+        }
+      }
+    }
+    // push far-to-near so that the nearest entry is popped first
+    for (int x = 1; x < nent; ++x) {
+      for (int y = x; y > 0 && entt[y - 1] < entt[y]; --y) {
+        const float tt = entt[y]; entt[y] = entt[y - 1]; entt[y - 1] = tt;
+        const int ii = ent[y]; ent[y] = ent[y - 1]; ent[y - 1] = ii;
+      }
+    }
+    for (int x = 0; x < nent; ++x) {
+      if (sp >= kStack) { atomicAdd(overflow, 1u); break; }
+      stack[(sp++) * kTraceBlock] = ent[x];
+    }
+  }
+  if (in_blas) best = fminf(best, bbest / br.s);
+  out->t = best;
+  return found;
+}
+
+}  // namespace
+
+// ---- path state --------------------------------------------------------------
+constexpr unsigned kAlive = kFlagAlive, kPendShadow = kFlagPendShadow, kPendMis = kFlagPendMis, kShadowAny = kFlagShadowAny,
+                   kNoSample = kFlagNoSample;
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
+  __shared__ int stack_smem[kStack * kTraceBlock];
+  int* stack = stack_smem + threadIdx.x;
+  const unsigned n = *a.ray_count;
+  const unsigned stride = gridDim.x * blockDim.x;
+  // Every lane of a warp runs the loop the same number of times so that the
+  // ballot in warp_append stays convergent (inactive lanes idle through it).
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    if (i < n) {
+      const unsigned ref = a.ray_list[i];
+      const unsigned p = ref >> 3, type = ref & 3u;
+      const bool any = (ref & 4u) != 0u;
+      const size_t slot = (size_t)type * a.paths + p;
+      const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
+      Hit h = {0.0f, -1, -1, 0.0f};
+      bool hit;
+      if (any) hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, &h, stack, a.overflow);
+      else hit = trace_ray<false>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, &h, stack, a.overflow);
+      a.hits[slot] = make_float4(h.t, __int_as_float(hit ? h.prim : -1), __int_as_float(h.aux), h.t_obj);
+    }
+  }
+}
+
+__global__ void k_raygen(RaygenArgs a) {
+  // No early return: every lane of the warp takes part in warp_append's ballot.
+  const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in_range = p < a.paths;
+  bool ok = false;
+  if (in_range) {
+    const unsigned pix = p % a.pixels;
+    const unsigned sample = a.sample_base + p / a.pixels;
+    const unsigned x = pix % a.width, y = pix / a.width;
+    const uint32_t key = rng_path_key(a.seed, pix, sample);
+    V3 o = {0, 0, 0}, d = {0, 0, 1};
+    ok = camera_ray(a.scene.camera, (float)x, (float)y, rng_uniform(key, kDimPixelX), rng_uniform(key, kDimPixelY),
+                    rng_uniform(key, kDimLensU), rng_uniform(key, kDimLensV), &o, &d);
+    a.beta[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);  // w: etaScale
+    a.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.meta[p] = make_uint4(pix, key, 0u, ok ? kAlive : kNoSample);  // z: bounce | dimension step << 16
+    a.ray_o[p] = make_float4(o.x, o.y, o.z, kTMin);
+    a.ray_d[p] = make_float4(d.x, d.y, d.z, kFltMax);
+    // a path without a camera ray (fisheye outside the disc) still goes through
+    // shade once to be retired; it traces nothing and adds no film sample.
+    a.work_list[p] = p;
+  }
+  const unsigned slot = warp_append(a.ray_count, ok);
+  if (ok) a.ray_list[slot] = p << 3;
+  if (p == 0) *a.work_count = a.paths;
+}
+
+DFC_D V3 surface_of(const SceneView& S, const DPrim& pr, int aux, V3 o, V3 d, float t_obj, Surface* sf) {
+  // the object ray as the intersector saw it
+  V3 oo = o, od = d;
+  if (!pr.identity) {
+    oo = xf_point(pr.w2o, o);
+    od = normalize(xf_vec(pr.w2o, d));
+  }
+  switch (pr.shape) {
+    case kShapeSphere: *sf = sphere_surface(oo, od, t_obj); break;
+    case kShapeRectangle: *sf = rect_surface(S.rects + (size_t)pr.data * 16, oo, od, t_obj); break;
+    case kShapePlane: *sf = plane_surface(oo, od, t_obj); break;
+    default: *sf = triangle_surface(S.tri_attr + (size_t)aux * 24, oo, od, t_obj); break;
+  }
+  surface_to_world(pr, *sf);
+  return sf->p;
+}
+
+// World distance of a hit as SurfaceIntersection3F.transform (geometry/
+// SurfaceIntersection3F.java:389) forms it: from the object ray's origin mapped
+// back to world space to the world hit point.
+DFC_D float world_t(const DPrim& pr, V3 o, const Surface& sf) {
+  if (pr.identity) return len(sf.p - o);
+  return len(sf.p - xf_point(pr.o2w, xf_point(pr.w2o, o)));
+}
+
+// Area-light pdf for a direction (Shape3F.evaluateProbabilityDensityFunction and
+// the Sphere3F override), in the light's object space.
+DFC_D float area_light_pdf(const SceneView& S, const DLight& lt, V3 p, V3 wi) {
+  V3 ref = xf_point(lt.w2o, p);
+  V3 w = normalize(xf_vec(lt.w2o, wi));
+  if (lt.shape == kShapeTriangle) {
+    const float* q = S.tri_attr + (size_t)lt.shape_data * 24;
+    float t = tri_t(ld3(q), ld3(q + 3), ld3(q + 6), ref, w, 0.001f, kFltMax);
+    if (!(t > 0.0f)) return 0.0f;
+    Surface s = triangle_surface(q, ref, w, t);
+    V3 dp = s.p - ref;
+    float pd = dot(dp, dp) / (fabsf(dot(normalize(s.s.w), -w)) * lt.area);
+    return (isinf(pd) || isnan(pd)) ? 0.0f : pd;
+  }
+  if (lt.shape == kShapeSphere) {
+    float t = sphere_t(ref, w, 0.001f, kFltMax);
+    if (!(t > 0.0f)) return 0.0f;
+    Surface s = sphere_surface(ref, w, t);
+    V3 dp = s.p - ref;
+    float pd = dot(dp, dp) / fabsf(dot(s.s.w, -w)) * (4.0f * kPi);
+    return (isinf(pd) || isnan(pd)) ? 0.0f : pd;
+  }
+  return 0.0f;
+}
+
+DFC_D void film_add(const ShadeArgs& a, unsigned pix, V3 L) {
+  if (!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z))) return;  // AbstractCPURenderer.java:231
+  if (luminance(L) < -1.0e-5f) return;
+  float* f = reinterpret_cast<float*>(a.film_sum + pix);
+  atomicAdd(f + 0, L.x); atomicAdd(f + 1, L.y); atomicAdd(f + 2, L.z); atomicAdd(f + 3, 1.0f);
+  float* g = reinterpret_cast<float*>(a.film_sq + pix);
+  atomicAdd(g + 0, L.x * L.x); atomicAdd(g + 1, L.y * L.y); atomicAdd(g + 2, L.z * L.z);
+}
+
+// One shade step of the path tracer for every path on the work list.
+__global__ void k_shade_path(ShadeArgs a) {
+  const unsigned n = *a.work_count;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const SceneView& S = a.scene;
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool spawn_ext = false, spawn_shadow = false, spawn_mis = false, keep = false, shadow_any = false;
+    unsigned p = 0;
+    if (i < n) {
+      p = a.work_list[i];
+      uint4 meta = a.meta[p];
+      float4 b4 = a.beta[p];
+      float4 l4 = a.radiance[p];
+      V3 beta = {b4.x, b4.y, b4.z}, L = {l4.x, l4.y, l4.z};
+      float eta_scale = b4.w;
+      unsigned flags = meta.w;
+      int bounce = (int)(meta.z & 0xffffu), dimb = (int)(meta.z >> 16);
+      const uint32_t key = meta.y;
+      const size_t P = a.paths;
+      // 1. fold in the light rays of the previous step
+      if (flags & kPendShadow) {
+        const float4 hs = a.hits[P + p];
+        const float4 c = a.pend_shadow[p];
+        const int hp = __float_as_int(hs.y);
+        bool vis;
+        if (flags & kShadowAny) vis = hp < 0;
+        else vis = hp >= 0 && S.prims[hp].light == __float_as_int(c.w);
+        if (vis) L = L + V3{c.x, c.y, c.z};
+      }
+      if (flags & kPendMis) {
+        const float4 hm = a.hits[2 * P + p];
+        const float4 c = a.pend_mis[p];
+        const int li = __float_as_int(c.w);
+        const int hp = __float_as_int(hm.y);
+        const float4 md = a.ray_d[2 * P + p];
+        const V3 wi = {md.x, md.y, md.z};
+        if (hp >= 0) {
+          const DPrim& hpr = S.prims[hp];
+          if (hpr.light == li) {
+            const DLight& lt = S.lights[li];
+            const float4 mo = a.ray_o[2 * P + p];
+            Surface s;
+            surface_of(S, hpr, __float_as_int(hm.z), V3{mo.x, mo.y, mo.z}, wi, hm.w, &s);
+            if (lt.two_sided || dot(s.s.w, -wi) > 0.0f) L = L + mul(V3{c.x, c.y, c.z}, ld3(lt.radiance));
+          }
+        } else {
+          V3 Le = light_Le_miss(S, S.lights[li], wi);
+          L = L + mul(V3{c.x, c.y, c.z}, Le);
+        }
+      }
+      flags &= ~(kPendShadow | kPendMis | kShadowAny);
+      bool alive = (flags & kAlive) != 0u;
+      if (alive) {
+        const float4 h = a.hits[p];
+        const float4 ro = a.ray_o[p], rd = a.ray_d[p];
+        const V3 ray_o = {ro.x, ro.y, ro.z}, ray_d = {rd.x, rd.y, rd.z};
+        const int hp = __float_as_int(h.y);
+        const bool spec = (flags & kFlagSpecular) != 0u;
+        const bool rec = a.record_primary && bounce == 0 && dimb == 0 && p < a.pixels;
+        if (rec && hp < 0) { a.primary_prim[p] = -1; a.primary_t[p] = __int_as_float(0x7fc00000); }
+        if (hp < 0) {
+          if (bounce == 0 && a.preview) L = {1, 1, 1};
+          else if (bounce == 0 || spec) {
+            for (int k = 0; k < S.light_count; ++k) L = L + mul(beta, light_Le_miss(S, S.lights[k], ray_d));
+          }
+          alive = false;
+        } else {
+          const DPrim& pr = S.prims[hp];
+          Surface sf;
+          surface_of(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
+          // SurfaceIntersection3F.transform: t = |origin - world point|
+          if (rec) { a.primary_prim[p] = hp; a.primary_t[p] = world_t(pr, ray_o, sf); }
+          const V3 wo = -ray_d;
+          if (bounce == 0 || spec) {
+            V3 Le;
+            if (pr.light >= 0) {
+              const DLight& lt = S.lights[pr.light];
+              Le = (lt.two_sided || dot(sf.s.w, wo) > 0.0f) ? ld3(lt.radiance) : V3{0, 0, 0};
+            } else {
+              Le = ld3(S.materials[pr.material].emission);
+            }
+            L = L + mul(beta, Le);
+          }
+          if (bounce >= a.max_bounce) {
+            alive = false;
+          } else {
+            const DMaterial& m = S.materials[pr.material];
+            Bsdf B;
+            if (!build_bsdf(m, sf, ray_d, &B)) {
+              // Scene.java:494: no BSDF, continue straight through without counting a bounce
+              a.ray_o[p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
+              a.ray_d[p] = make_float4(ray_d.x, ray_d.y, ray_d.z, kFltMax);
+              spawn_ext = true;
+              ++dimb;
+            } else {
+              const V3 ns = sf.s.w;
+              if (bsdf_nonspec(B) > 0 && S.light_count > 0) {
+                const int nl = S.light_count;
+                const int li = min((int)(rng_uniform(key, bounce_dim(dimb, kDimLightPick)) * nl), nl - 1);
+                const DLight& lt = S.lights[li];
+                const float lscale = (float)nl;  // Color3F.divide(x, 1 / lightCount)
+                LightS ls;
+                const bool have = light_sample(S, lt, sf, rng_uniform(key, bounce_dim(dimb, kDimLightSampleU)),
+                                               rng_uniform(key, bounce_dim(dimb, kDimLightSampleV)),
+                                               rng_uniform(key, bounce_dim(dimb, kDimSunPick)), &ls);
+                const bool delta = light_is_delta(lt.type);
+                if (have && !is_black(ls.L) && ls.pdf > 0.0f) {
+                  V3 f = bsdf_f(B, kAllButSpecular, ls.wi) * fabsf(dot(ls.wi, ns));
+                  if (!is_black(f)) {
+                    float w = 1.0f;
+                    if (!delta) w = (ls.pdf * ls.pdf) / (ls.pdf * ls.pdf + bsdf_pdf(B, kAllButSpecular, ls.wi) * bsdf_pdf(B, kAllButSpecular, ls.wi));
+                    V3 c = mul(beta, mul(f, ls.L) * (w / ls.pdf)) * lscale;
+                    V3 toL = ls.p - sf.p;
+                    float dist = len(toL);
+                    V3 sd = normalize(toL);
+                    a.ray_o[P + p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
+                    a.ray_d[P + p] = make_float4(sd.x, sd.y, sd.z, fabsf(dist) + 0.001f);
+                    a.pend_shadow[p] = make_float4(c.x, c.y, c.z, __int_as_float(li));
+                    shadow_any = lt.type != kLightDiffuseArea;
+                    flags |= kPendShadow | (shadow_any ? kShadowAny : 0u);
+                    spawn_shadow = true;
+                  }
+                }
+                if (!delta) {
+                  BSample bs;
+                  if (bsdf_sample(B, kAllButSpecular, rng_uniform(key, bounce_dim(dimb, kDimMisSampleU)),
+                                  rng_uniform(key, bounce_dim(dimb, kDimMisSampleV)), &bs)) {
+                    V3 f = bs.f * fabsf(dot(bs.wi, ns));
+                    if (!is_black(f) && bs.pdf > 0.0f) {
+                      float w = 1.0f;
+                      bool ok = true;
+                      if (!is_spec(bs.type)) {
+                        float lp = lt.type == kLightDiffuseArea ? area_light_pdf(S, lt, sf.p, bs.wi) : (lt.type == kLightPerez ? perez_pdf(S, lt, bs.wi) : 0.0f);
+                        if (lp == 0.0f) ok = false;
+                        else w = (bs.pdf * bs.pdf) / (bs.pdf * bs.pdf + lp * lp);
+                      }
+                      if (ok) {
+                        V3 c = mul(beta, f * (w / bs.pdf)) * lscale;
+                        a.ray_o[2 * P + p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
+                        a.ray_d[2 * P + p] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, kFltMax);
+                        a.pend_mis[p] = make_float4(c.x, c.y, c.z, __int_as_float(li));
+                        flags |= kPendMis;
+                        spawn_mis = true;
+                      }
+                    }
+                  }
+                }
+              }
+              BSample bs;
+              bool cont = bsdf_sample(B, kAll, rng_uniform(key, bounce_dim(dimb, kDimBsdfU)), rng_uniform(key, bounce_dim(dimb, kDimBsdfV)), &bs);
+              if (cont && (is_black(bs.f) || bs.pdf == 0.0f)) cont = false;
+              if (cont) {
+                beta = mul(beta, bs.f * (fabsf(dot(bs.wi, ns)) / bs.pdf));
+                const bool sp2 = is_spec(bs.type);
+                flags = sp2 ? (flags | kFlagSpecular) : (flags & ~kFlagSpecular);
+                if ((bs.type & kTrans) && sp2) eta_scale *= dot(wo, sf.g.w) > 0.0f ? B.eta * B.eta : 1.0f / (B.eta * B.eta);
+                a.ray_o[p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
+                a.ray_d[p] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, kFltMax);
+                V3 rr = beta * eta_scale;
+                float mx = fmaxf(rr.x, fmaxf(rr.y, rr.z));
+                if (mx < 1.0f && bounce >= a.min_rr) {
+                  float q = fmaxf(0.05f, 1.0f - mx);
+                  if (rng_uniform(key, bounce_dim(dimb, kDimRoulette)) < q) cont = false;
+                  else beta = beta * (1.0f / (1.0f - q));
+                }
+              }
+              if (cont) { spawn_ext = true; ++bounce; ++dimb; }
+              else alive = false;
+            }
+          }
+        }
+      }
+      if (alive && !spawn_ext) alive = false;
+      if (a.last_step && alive) { alive = false; spawn_ext = false; }
+      flags = alive ? (flags | kAlive) : (flags & ~kAlive);
+      keep = alive || spawn_shadow || spawn_mis;
+      if (a.last_step) { keep = false; spawn_shadow = spawn_mis = false; }
+      if (!keep && !(flags & kNoSample)) film_add(a, meta.x, L);
+      a.beta[p] = make_float4(beta.x, beta.y, beta.z, eta_scale);
+      a.radiance[p] = make_float4(L.x, L.y, L.z, 0.0f);
+      a.meta[p] = make_uint4(meta.x, meta.y, ((unsigned)bounce & 0xffffu) | ((unsigned)dimb << 16), flags);
+    }
+    // appends (all lanes of the warp take part)
+    const unsigned r0 = warp_append(a.next_ray_count, spawn_ext);
+    if (spawn_ext) a.next_ray_list[r0] = p << 3;
+    const unsigned r1 = warp_append(a.next_ray_count, spawn_shadow);
+    if (spawn_shadow) a.next_ray_list[r1] = (p << 3) | (shadow_any ? 4u : 0u) | 1u;
+    const unsigned r2 = warp_append(a.next_ray_count, spawn_mis);
+    if (spawn_mis) a.next_ray_list[r2] = (p << 3) | 2u;
+    const unsigned w = warp_append(a.next_work_count, keep);
+    if (keep) a.next_work_list[w] = p;
+  }
+}
+
+// RAY_CASTING (Scene.java:675) and DEPTH_CAMERA (Scene.java:327) on the
+// primary hits; AO spawns its occlusion rays (Scene.java:272).
+__global__ void k_shade_primary(ShadeArgs a, int algorithm) {
+  const unsigned n = *a.work_count;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const SceneView& S = a.scene;
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    if (i >= n) continue;
+    const unsigned p = a.work_list[i];
+    const uint4 meta = a.meta[p];
+    if (!(meta.w & kAlive)) { if (algorithm == DFC_ALGO_AO) a.radiance[p] = make_float4(0, 0, 0, -2.0f); continue; }
+    const float4 h = a.hits[p];
+    const float4 ro = a.ray_o[p], rd = a.ray_d[p];
+    const V3 ray_o = {ro.x, ro.y, ro.z}, ray_d = {rd.x, rd.y, rd.z};
+    const int hp = __float_as_int(h.y);
+    if (a.record_primary && p < a.pixels && hp < 0) { a.primary_prim[p] = -1; a.primary_t[p] = __int_as_float(0x7fc00000); }
+    V3 L = {0, 0, 0};
+    if (hp < 0) {
+      if (a.preview) L = {1, 1, 1};
+      else if (algorithm == DFC_ALGO_RAY_CASTING) for (int k = 0; k < S.light_count; ++k) L = L + light_Le_miss(S, S.lights[k], ray_d);
+      if (algorithm == DFC_ALGO_AO) { a.radiance[p] = make_float4(L.x, L.y, L.z, -1.0f); continue; }
+      film_add(a, meta.x, L);
+      continue;
+    }
+    const DPrim& pr = S.prims[hp];
+    Surface sf;
+    surface_of(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
+    if (a.record_primary && p < a.pixels) { a.primary_prim[p] = hp; a.primary_t[p] = world_t(pr, ray_o, sf); }
+    if (algorithm == DFC_ALGO_RAY_CASTING) {
+      float c = fabsf(dot(sf.s.w, ray_d)) * 0.5f;
+      film_add(a, meta.x, V3{c, c, c});
+    } else if (algorithm == DFC_ALGO_DEPTH) {
+      V3 dd = sf.p - ray_o;
+      float in = clampf(1.0f / (dot(dd, dd) * 0.5f), 0.0f, 1.0f);
+      film_add(a, meta.x, V3{in, in, in});
+    } else {
+      // AO: store the geometric basis' hit point and spawn samples into the AO ray pool
+      a.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      for (int s = 0; s < a.ao_samples; ++s) {
+        V3 dl = uniform_hemisphere(rng_uniform(meta.y, kDimBounceBase + 2 * s), rng_uniform(meta.y, kDimBounceBase + 2 * s + 1));
+        V3 dw = normalize(to_world(dl, ONB{normalize(sf.g.u), normalize(sf.g.v), sf.g.w}));
+        size_t slot = (size_t)p * a.ao_samples + s;
+        a.ao_o[slot] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
+        a.ao_d[slot] = make_float4(dw.x, dw.y, dw.z, kFltMax);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_ao(AoArgs a) {
+  __shared__ int stack_smem[kStack * kTraceBlock];
+  int* stack = stack_smem + threadIdx.x;
+  const size_t n = (size_t)a.paths * a.samples;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const size_t i = base + threadIdx.x;
+    if (i >= n) continue;
+    const unsigned p = (unsigned)(i / a.samples);
+    if (a.radiance[p].w < 0.0f) continue;  // primary miss
+    const float4 ro = a.ao_o[i], rd = a.ao_d[i];
+    Hit h = {0.0f, -1, -1, 0.0f};
+    float v;
+    if (a.max_distance > 0.0f) {
+      bool hit = trace_ray<false>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, &h, stack, a.overflow);
+      v = hit ? clampf(h.t, 0.0f, a.max_distance) / a.max_distance : 1.0f;
+    } else {
+      bool hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, &h, stack, a.overflow);
+      v = hit ? 0.0f : 1.0f;
+    }
+    a.ao_value[i] = v;
+  }
+}
+
+__global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples) {
+  const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.paths) return;
+  const uint4 meta = a.meta[p];
+  const float4 r = a.radiance[p];
+  V3 L;
+  if (r.w < -1.5f) return;  // no camera ray: no sample (AbstractCPURenderer.java:221)
+  if (r.w < 0.0f) L = {r.x, r.y, r.z};
+  else {
+    float acc = 0.0f;
+    for (int s = 0; s < samples; ++s) acc += ao_value[(size_t)p * samples + s];
+    float v = acc * (kPi / samples);
+    v = v / kPi;
+    L = {v, v, v};
+  }
+  film_add(a, meta.x, L);
+}
+
+// Film resolve: mean radiance -> tone mapper -> sRGB -> RGBA8
+// (renderer/gpu/AbstractImageKernel.java:1104-1160, 1189-1325).
+__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pixels) return;
+  const float4 s = film_sum[i];
+  V3 c = s.w > 0.0f ? V3{s.x / s.w, s.y / s.w, s.z / s.w} : V3{0, 0, 0};
+  switch (tone_mapper) {
+    case 2: c = V3{c.x / (1.0f + c.x), c.y / (1.0f + c.y), c.z / (1.0f + c.z)}; break;  // Reinhard
+    case 0: {  // filmic ACES (Narkowicz fit)
+      auto f = [](float x) { return clampf((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f), 0.0f, 1.0f); };
+      c = V3{f(c.x), f(c.y), f(c.z)};
+      break;
+    }
+    default: break;
+  }
+  auto enc = [](float v) {
+    v = clampf(v, 0.0f, 1.0f);
+    // sRGB redo-gamma with the ColorSpaceF parameters (break point 0.00304, gamma 2.4)
+    const float slope = 12.923210180787857f, slope_match = 1.0553409f, offset = 0.0553409f;
+    v = v <= 0.00304f ? v * slope : slope_match * powf(v, 1.0f / 2.4f) - offset;
+    return (unsigned char)(clampf(v, 0.0f, 1.0f) * 255.0f + 0.5f);
+  };
+  out[i] = make_uchar4(enc(c.x), enc(c.y), enc(c.z), 255);
+}
+
+}  // namespace dfc

@@ -1,0 +1,89 @@
+// Kernel argument blocks and entry points of the wavefront render path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dfc_scene.h"
+
+namespace dfc {
+
+enum { DFC_ALGO_AO = 0, DFC_ALGO_DEPTH = 1, DFC_ALGO_PATH = 2, DFC_ALGO_RAY_CASTING = 3, DFC_ALGO_RAY_TRACING = 4 };
+
+// Path flags (PathMeta.w)
+enum : unsigned { kFlagAlive = 1u, kFlagSpecular = 2u, kFlagPendShadow = 4u, kFlagPendMis = 8u, kFlagShadowAny = 16u, kFlagNoSample = 32u };
+
+struct TraceArgs {
+  SceneView scene;
+  const unsigned* ray_list;
+  const unsigned* ray_count;
+  const float4* ray_o;  // 3 slots per path: [type * paths + p]
+  const float4* ray_d;
+  float4* hits;         // t_world, prim (int bits, -1 miss), aux (int bits), t_object
+  unsigned paths;
+  unsigned* overflow;
+};
+
+struct RaygenArgs {
+  SceneView scene;
+  unsigned paths, pixels, width, sample_base;
+  uint32_t seed;
+  float4* beta;
+  float4* radiance;
+  uint4* meta;          // pixel, rng key, bounce | step << 16, flags
+  float4* ray_o;
+  float4* ray_d;
+  unsigned* ray_list;
+  unsigned* ray_count;
+  unsigned* work_list;
+  unsigned* work_count;
+};
+
+struct ShadeArgs {
+  SceneView scene;
+  unsigned paths, pixels;
+  int max_bounce, min_rr, preview, last_step, record_primary, ao_samples;
+  const unsigned* work_list;
+  const unsigned* work_count;
+  unsigned* next_work_list;
+  unsigned* next_work_count;
+  unsigned* next_ray_list;
+  unsigned* next_ray_count;
+  float4* beta;
+  float4* radiance;
+  uint4* meta;
+  float4* ray_o;
+  float4* ray_d;
+  const float4* hits;
+  float4* pend_shadow;
+  float4* pend_mis;
+  float4* film_sum;
+  float4* film_sq;
+  int* primary_prim;
+  float* primary_t;
+  float4* ao_o;
+  float4* ao_d;
+};
+
+struct AoArgs {
+  SceneView scene;
+  unsigned paths;
+  int samples;
+  float max_distance;
+  const float4* radiance;
+  const float4* ao_o;
+  const float4* ao_d;
+  float* ao_value;
+  unsigned* overflow;
+};
+
+__global__ void k_raygen(RaygenArgs a);
+__global__ void k_trace(TraceArgs a);
+__global__ void k_shade_path(ShadeArgs a);
+__global__ void k_shade_primary(ShadeArgs a, int algorithm);
+__global__ void k_trace_ao(AoArgs a);
+__global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);
+__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out);
+
+constexpr int kTraceThreads = 128;
+
+}  // namespace dfc

@@ -1,0 +1,124 @@
+// Device-resident scene layout of libdayflower_cuda (shared by the host-side
+// ingest in dfc_ingest.cpp and the kernels).
+//
+// The compiled arrays of the reference (renderer/gpu/AbstractSceneKernel.java:
+// 1777-1852) are decoded once on the host into these records:
+//   * DPrim      one 128-byte record per primitive: 3x4 object-to-world and
+//                world-to-object rows, shape kind and data index, resolved
+//                material index and area-light index;
+//   * DMaterial  one record per distinct compiled material with its constant
+//                textures already evaluated (only ConstantTexture is supported);
+//   * DLight     one record per entry of lightIDAndOffsetArray, in its order;
+//   * BVH4Node   128-byte 4-wide nodes, child boxes stored as SoA float4
+//                (one 128-byte line per node fetch).  The top level is built
+//                over primitive world boxes, every mesh gets its own
+//                object-space bottom level;
+//   * triangles  float4 x3 per triangle (positions, v0.w = triangle index),
+//                reordered by the bottom-level builds, and the compiled
+//                24-float rows kept in their original order for shading.
+#pragma once
+
+#include <cstdint>
+
+namespace dfc {
+
+// 16-byte vector with the layout of CUDA's float4 (device code reads it as float4).
+struct alignas(16) F4 { float x, y, z, w; };
+
+// Reference type ids (each class's public static final int ID).
+enum : int {
+  kShapeCone = 2, kShapeCylinder = 5, kShapeDisk = 6, kShapeHyperboloid = 7, kShapeParaboloid = 9, kShapePlane = 10,
+  kShapePolygon = 11, kShapeRectangle = 13, kShapeCuboid = 14, kShapeSphere = 15, kShapeTorus = 16, kShapeTriangle = 17,
+  kShapeMesh = 18
+};
+enum : int { kLightDiffuseArea = 1, kLightDirectional = 2, kLightImage = 3, kLightPerez = 4, kLightPoint = 5, kLightSpot = 7 };
+
+// Resolved material kinds (one shading routine each).
+enum : int {
+  kMatNone = 0,        // no BSDF: rays pass through (Scene.java:494-500)
+  kMatLambert = 1,     // MatteMaterial, angle 0
+  kMatOrenNayar = 2,   // MatteMaterial, angle > 0
+  kMatMirror = 3,      // MirrorMaterial
+  kMatGlassSpec = 4,   // GlassMaterial, zero roughness (FresnelSpecularBXDF)
+  kMatGlassRough = 5,  // GlassMaterial, rough (TorranceSparrow BRDF + BTDF)
+  kMatMetal = 6,       // MetalMaterial
+  kMatPlastic = 7,     // PlasticMaterial
+  kMatKinds = 8
+};
+
+struct alignas(16) DPrim {
+  float o2w[12];
+  float w2o[12];
+  int shape;       // reference shape id
+  int data;        // triangle index / rectangle index / bottom-level root node
+  int material;    // DMaterial index
+  int light;       // DLight index of its DiffuseAreaLight, -1 if none
+  int identity;    // 1 if both matrices are the identity
+  int tri_first;   // mesh: first triangle (in the reordered intersection array)
+  int tri_count;   // mesh: triangle count
+  int pad;
+};
+static_assert(sizeof(DPrim) == 128, "DPrim is one 128-byte line");
+
+struct alignas(16) DMaterial {
+  int kind;
+  int has_kr, has_kt, pad0;
+  float emission[3];
+  float eta;
+  float c0[3];     // kd (matte/plastic), kr (mirror/glass), unused (metal)
+  float ax;
+  float c1[3];     // ks (plastic), kt (glass), metal eta
+  float ay;
+  float c2[3];     // metal k
+  float on_a;
+  float on_b;
+  float pad1[3];
+};
+static_assert(sizeof(DMaterial) == 96, "DMaterial layout");
+
+struct alignas(16) DLight {
+  int type;
+  int shape;       // DiffuseAreaLight: shape id
+  int shape_data;  // DiffuseAreaLight: triangle index (triangle shapes)
+  int two_sided;
+  float radiance[3];  // area radiance / point & spot intensity / directional radiance / Perez sun colour
+  float area;
+  float pos[3];       // point/spot position
+  float radius;       // directional and Perez radius
+  float dir[3];       // directional direction
+  float cos_cone;
+  float o2w[12];
+  float w2o[12];
+  float cos_cone_delta;
+  int perez;          // float offset of the Perez record in the Perez pool
+  float pad[2];
+};
+
+struct alignas(16) BVH4Node {
+  float lox[4], loy[4], loz[4];
+  float hix[4], hiy[4], hiz[4];
+  int child[4];   // >= 0 internal node, < 0 leaf whose first item is ~child
+  int count[4];   // items in a leaf (0 for internal or empty slots)
+};
+static_assert(sizeof(BVH4Node) == 128, "BVH4Node is one 128-byte line");
+
+// Everything a kernel needs to read the scene (passed by value).
+struct SceneView {
+  const DPrim* prims;
+  int prim_count;
+  const DMaterial* materials;
+  const DLight* lights;
+  int light_count;
+  const BVH4Node* nodes;        // top level and all bottom levels
+  int tlas_root;                // -1 if no bounded primitive
+  const int* tlas_items;        // primitive index per top-level leaf item
+  const int* unbounded;         // primitives with an infinite bounding volume (planes)
+  int unbounded_count;
+  const F4* tri_pos;            // 3 per triangle, reordered; v0.w holds the triangle index
+  const float* tri_attr;        // shape3FTriangle3FArray, 24 floats per triangle, original order
+  const float* rects;           // shape3FRectangle3FArray
+  const float* perez;           // lightPerezLightArray
+  const float* camera;          // 19 floats
+};
+
+}  // namespace dfc

@@ -1,0 +1,285 @@
+"""Scene compiler: flattens a :class:`~dayflower_b200.scene.model.Scene` into the
+named arrays that ``renderer/gpu/AbstractSceneKernel.java:1777-1852``
+(``doSetupScene``) uploads, i.e. the ``CompiledScene`` caches of
+``scene/compiler/SceneCompiler.java:81``.
+
+Two layouts are produced:
+
+* ``layout_version = 1`` is the reference packing.  Texture and modifier
+  references are packed four to an int with ``utility/Ints.java:258``
+  (8-bit ids and 8-bit relative offsets), light references 16/16 with
+  ``Ints.java:237``.  Compiling a scene that needs more than 256 textures
+  raises ``ValueError``, as ``Ints.pack`` throws ``IllegalArgumentException``.
+* ``layout_version = 2`` widens the material records: each 32-bit slot of a v1
+  material becomes four int32 lanes (the four packed bytes, or the plain value
+  followed by three zeros), and material offsets count lanes.  Everything else
+  is identical.  Large scenes (thousands of distinct textures) need it.
+
+Offsets follow the reference: shape and material offsets are absolute array
+indices, bounding-volume, texture and light offsets are relative structure
+indices (the device multiplies them by the structure length).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, List
+
+import numpy as np
+
+from . import model as M
+from .perez import perez_record
+
+ARRAY_NAMES_F32 = [
+    "boundingVolume3FAxisAlignedBoundingBox3FArray", "boundingVolume3FBoundingSphere3FArray",
+    "shape3FCone3FArray", "shape3FCylinder3FArray", "shape3FDisk3FArray", "shape3FHyperboloid3FArray",
+    "shape3FParaboloid3FArray", "shape3FPolygon3FArray", "shape3FRectangle3FArray", "shape3FRectangularCuboid3FArray",
+    "shape3FTorus3FArray", "shape3FTriangle3FArray",
+    "textureBlendTextureArray", "textureBullseyeTextureArray", "textureCheckerboardTextureArray",
+    "textureConstantTextureArray", "textureLDRImageTextureArray", "textureMarbleTextureArray",
+    "texturePolkaDotTextureArray", "textureSimplexFractionalBrownianMotionTextureArray",
+    "modifierNormalMapLDRImageModifierArray", "modifierSimplexNoiseNormalMapModifierArray",
+    "lightDiffuseAreaLightArray", "lightDirectionalLightArray", "lightImageLightArray", "lightPerezLightArray",
+    "lightPointLightArray", "lightSpotLightArray", "cameraArray", "primitiveMatrix44FArray",
+]
+ARRAY_NAMES_I32 = [
+    "shape3FTriangleMesh3FArray", "textureLDRImageTextureOffsetArray",
+    "materialBullseyeMaterialArray", "materialCheckerboardMaterialArray", "materialClearCoatMaterialArray",
+    "materialDisneyMaterialArray", "materialGlassMaterialArray", "materialGlossyMaterialArray",
+    "materialMatteMaterialArray", "materialMetalMaterialArray", "materialMirrorMaterialArray",
+    "materialPlasticMaterialArray", "materialPolkaDotMaterialArray", "materialSubstrateMaterialArray",
+    "materialTranslucentMaterialArray", "materialUberMaterialArray",
+    "modifierNormalMapLDRImageModifierOffsetArray", "lightIDAndOffsetArray", "lightImageLightOffsetArray",
+    "lightPerezLightOffsetArray", "primitiveArray",
+]
+
+
+class CompiledScene:
+    """The compiled arrays plus bookkeeping (``scene/compiler/CompiledScene.java``)."""
+
+    def __init__(self, arrays: Dict[str, np.ndarray], layout_version: int, stats: Dict[str, int]):
+        self.arrays = arrays
+        self.layout_version = layout_version
+        self.stats = stats
+
+    def nbytes(self) -> int:
+        return int(sum(a.nbytes for a in self.arrays.values()))
+
+
+def _scene_lib():
+    from .._native import load_scene_compiler
+    return load_scene_compiler()
+
+
+def build_mesh_bvh_stream(tris: np.ndarray, tri_offset_base: int, aabb_base: int):
+    """Returns (int32 stream, float32 aabbs) for one mesh (host helper in csrc/scene_compiler.cpp)."""
+    lib = _scene_lib()
+    n = tris.shape[0]
+    cap = 2 * n + 1
+    stream = np.zeros(cap * 8, dtype=np.int32)
+    boxes = np.zeros(cap * 8, dtype=np.float32)
+    t = np.ascontiguousarray(tris, dtype=np.float32)
+    nodes = lib.dfc_sc_build_mesh_bvh(t.ctypes.data_as(ctypes.c_void_p), ctypes.c_longlong(n), ctypes.c_longlong(tri_offset_base),
+                                      ctypes.c_longlong(aabb_base), stream.ctypes.data_as(ctypes.c_void_p),
+                                      boxes.ctypes.data_as(ctypes.c_void_p), ctypes.c_longlong(cap))
+    if nodes <= 0:
+        raise RuntimeError("mesh BVH build failed")
+    return stream[: nodes * 8].copy(), boxes[: nodes * 8].copy()
+
+
+def _pack8(a, b, c, d) -> int:
+    """``utility/Ints.java:258``."""
+    for v in (a, b, c, d):
+        if not 0 <= v <= 255:
+            raise ValueError("texture/modifier reference out of range for layout 1: %d (use layout_version=2)" % v)
+    x = (a & 0xFF) | ((b & 0xFF) << 8) | ((c & 0xFF) << 16) | ((d & 0xFF) << 24)
+    return int(np.int32(np.uint32(x)))
+
+
+def _pack16(a, b) -> int:
+    """``utility/Ints.java:237``."""
+    if not (0 <= a <= 65535 and 0 <= b <= 65535):
+        raise ValueError("reference out of range for a 16/16 pack: %d %d" % (a, b))
+    return int(np.int32(np.uint32(((a & 0xFFFF) << 16) | (b & 0xFFFF))))
+
+
+def _world_aabb(points_obj: np.ndarray, o2w: np.ndarray):
+    p = np.asarray(points_obj, dtype=np.float64).reshape(-1, 3)
+    lo, hi = p.min(axis=0), p.max(axis=0)
+    corners = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+    m = o2w.astype(np.float64)
+    w = corners @ m[:3, :3].T + m[:3, 3]
+    return w.min(axis=0), w.max(axis=0)
+
+
+def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> CompiledScene:
+    if layout_version not in (1, 2):
+        raise ValueError("layout_version must be 1 or 2")
+    lanes = 4 if layout_version == 2 else 1
+    f32: Dict[str, List[np.ndarray]] = {k: [] for k in ARRAY_NAMES_F32}
+    i32: Dict[str, List[np.ndarray]] = {k: [] for k in ARRAY_NAMES_I32}
+    sizes = {k: 0 for k in ARRAY_NAMES_F32 + ARRAY_NAMES_I32}
+
+    def push(name, arr):
+        bucket = f32 if name in f32 else i32
+        a = np.asarray(arr, dtype=np.float32 if name in f32 else np.int32).reshape(-1)
+        off = sizes[name]
+        bucket[name].append(a)
+        sizes[name] += a.size
+        return off
+
+    # ---- textures (ConstantTexture only), deduplicated by value
+    tex_index: Dict[tuple, int] = {}
+
+    def tex(color) -> int:
+        c = tuple(float(np.float32(x)) for x in (np.broadcast_to(np.asarray(color, dtype=np.float32), (3,))))
+        if c not in tex_index:
+            tex_index[c] = sizes["textureConstantTextureArray"] // 4
+            push("textureConstantTextureArray", [c[0], c[1], c[2], 0.0])
+        return tex_index[c]
+
+    def slot(a=(0, 0), b=(0, 0)):
+        if layout_version == 2:
+            return [a[0], a[1], b[0], b[1]]
+        return [_pack8(a[0], a[1], b[0], b[1])]
+
+    def plain(v):
+        return [int(v), 0, 0, 0] if layout_version == 2 else [int(v)]
+
+    def pad_to(rec, length):
+        return rec + [0] * (length * lanes - len(rec))
+
+    T = M.TEX_CONSTANT
+    noop = (M.MOD_NOOP, 0)
+    mat_offsets: Dict[int, tuple] = {}
+
+    def material(m: M.Material):
+        key = id(m)
+        if key in mat_offsets:
+            return mat_offsets[key]
+        em = (T, tex(m.emission))
+        head = slot(em, noop)
+        if isinstance(m, M.Matte):
+            rec, name, length = head + slot((T, tex([m.angle] * 3)), (T, tex(m.kd))), "materialMatteMaterialArray", 2
+        elif isinstance(m, M.Mirror):
+            rec, name, length = head + slot((T, tex(m.kr))), "materialMirrorMaterialArray", 2
+        elif isinstance(m, M.Glass):
+            rec = head + slot((T, tex([m.eta] * 3))) + slot((T, tex(m.kr)), (T, tex(m.kt))) + \
+                slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + plain(m.remap_roughness)
+            name, length = "materialGlassMaterialArray", 8
+        elif isinstance(m, M.Metal):
+            rec = head + slot((T, tex(m.eta)), (T, tex(m.k))) + slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + \
+                plain(m.remap_roughness)
+            name, length = "materialMetalMaterialArray", 4
+        elif isinstance(m, M.Plastic):
+            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness] * 3))) + plain(m.remap_roughness)
+            name, length = "materialPlasticMaterialArray", 4
+        else:
+            raise ValueError("unsupported material %r" % type(m).__name__)
+        off = push(name, pad_to(rec, length))
+        mat_offsets[key] = (m.ID, off)
+        return mat_offsets[key]
+
+    # ---- shapes
+    shape_offsets: Dict[int, tuple] = {}
+    mesh_jobs = []
+
+    def shape(s: M.Shape):
+        key = id(s)
+        if key in shape_offsets:
+            return shape_offsets[key]
+        if isinstance(s, M.Triangle):
+            off = push("shape3FTriangle3FArray", s.to_array())
+        elif isinstance(s, M.Rectangle):
+            off = push("shape3FRectangle3FArray", s.to_array())
+        elif isinstance(s, (M.Sphere, M.Plane)):
+            off = 0
+        elif isinstance(s, M.TriangleMesh):
+            tri_base = push("shape3FTriangle3FArray", s.triangles)
+            aabb_base = sizes["boundingVolume3FAxisAlignedBoundingBox3FArray"] // 8
+            stream, boxes = build_mesh_bvh_stream(s.triangles, tri_base, aabb_base)
+            push("boundingVolume3FAxisAlignedBoundingBox3FArray", boxes)
+            off = push("shape3FTriangleMesh3FArray", stream)
+            mesh_jobs.append(off)
+        else:
+            raise ValueError("unsupported shape %r" % type(s).__name__)
+        shape_offsets[key] = (s.ID, off)
+        return shape_offsets[key]
+
+    # ---- lights (scene order)
+    light_refs: Dict[int, tuple] = {}
+    rel_count = {M.LIGHT_DIFFUSE_AREA: 0, M.LIGHT_DIRECTIONAL: 0, M.LIGHT_POINT: 0, M.LIGHT_SPOT: 0, M.LIGHT_PEREZ: 0}
+    light_ids = []
+    for L in scene.lights:
+        if isinstance(L, M.DiffuseAreaLight):
+            sid, soff = shape(L.shape)
+            if isinstance(L.shape, M.Triangle):
+                area = 0.5 * float(np.linalg.norm(np.cross(L.shape.b - L.shape.a, L.shape.c - L.shape.a)))
+            elif isinstance(L.shape, M.Sphere):
+                area = 4.0 * np.pi
+            else:
+                area = 0.0
+            rec = np.zeros(40, dtype=np.float32)
+            rec[0:16] = L.transform.object_to_world.reshape(-1)
+            rec[16:32] = L.transform.world_to_object.reshape(-1)
+            rec[32:35] = L.radiance
+            rec[35], rec[36], rec[37], rec[38] = sid, soff, area, 1.0 if L.two_sided else 0.0
+            push("lightDiffuseAreaLightArray", rec)
+        elif isinstance(L, M.PointLight):
+            push("lightPointLightArray", np.concatenate([L.intensity, L.position, [0, 0]]))
+        elif isinstance(L, M.SpotLight):
+            rec = np.zeros(24, dtype=np.float32)
+            rec[0:16] = L.transform.world_to_object.reshape(-1)
+            rec[16:19] = L.intensity
+            rec[19:22] = L.position
+            rec[22], rec[23] = L.cos_cone, L.cos_cone_minus_delta
+            push("lightSpotLightArray", rec)
+        elif isinstance(L, M.DirectionalLight):
+            push("lightDirectionalLightArray", np.concatenate([L.radiance, L.direction, [L.radius, 0.0]]))
+        elif isinstance(L, M.PerezLight):
+            off = push("lightPerezLightArray", perez_record(L.turbidity, L.sun_direction_world))
+            push("lightPerezLightOffsetArray", [off])
+        else:
+            raise ValueError("unsupported light %r" % type(L).__name__)
+        rel = rel_count[L.ID]
+        rel_count[L.ID] += 1
+        light_refs[id(L)] = (L.ID, rel)
+        light_ids.append(_pack16(L.ID, rel))
+    push("lightIDAndOffsetArray", light_ids)
+
+    # ---- primitives
+    for p in scene.primitives:
+        sid, soff = shape(p.shape)
+        mid, moff = material(p.material)
+        o2w = p.transform.object_to_world
+        if isinstance(p.shape, M.Plane):
+            bvid, bvoff = M.BV_INFINITE, 0
+        else:
+            if isinstance(p.shape, M.Sphere):
+                pts = np.array([[-1, -1, -1], [1, 1, 1]], dtype=np.float32)
+            elif isinstance(p.shape, M.Triangle):
+                pts = np.stack([p.shape.a, p.shape.b, p.shape.c])
+            elif isinstance(p.shape, M.Rectangle):
+                pts = p.shape.corners()
+            else:
+                pts = p.shape.triangles[:, 0:9].reshape(-1, 3)
+            lo, hi = _world_aabb(pts, o2w)
+            bvid = M.BV_AABB
+            bvoff = sizes["boundingVolume3FAxisAlignedBoundingBox3FArray"] // 8
+            push("boundingVolume3FAxisAlignedBoundingBox3FArray", [hi[0], hi[1], hi[2], lo[0], lo[1], lo[2], 0, 0])
+        al = 0
+        if p.area_light is not None:
+            lid, lrel = light_refs[id(p.area_light)]
+            al = _pack16(lid, lrel)
+        push("primitiveArray", [p.instance_id, al, bvid, bvoff, mid, moff, sid, soff])
+        push("primitiveMatrix44FArray", p.transform.to_array())
+
+    push("cameraArray", scene.camera.to_array(resolution))
+
+    arrays = {}
+    for k, parts in f32.items():
+        arrays[k] = np.concatenate(parts).astype(np.float32) if parts else np.zeros(0, dtype=np.float32)
+    for k, parts in i32.items():
+        arrays[k] = np.concatenate(parts).astype(np.int32) if parts else np.zeros(0, dtype=np.int32)
+    stats = {"primitives": len(scene.primitives), "lights": len(scene.lights),
+             "triangles": sizes["shape3FTriangle3FArray"] // 24, "textures": len(tex_index), "meshes": len(mesh_jobs)}
+    return CompiledScene(arrays, layout_version, stats)

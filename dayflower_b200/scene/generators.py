@@ -1,0 +1,167 @@
+"""Seeded synthetic scenes for the benchmark configurations and the tests.
+
+No public scene, dataset or benchmark suite is read: every scene is generated
+from a fixed seed with the shapes and sizes its configuration names.
+
+* :func:`cornell_box` - five 100-unit walls (Rectangle3F), a glass and a
+  mirror sphere of radius 16.5, and a 30x30 light of radiance 12 under the
+  ceiling.  The light is two Triangle3F with DiffuseAreaLights, because the
+  CPU renderer can only sample area lights on spheres and triangles
+  (geometry/Shape3F.java:104-108).
+* :func:`terrain_spheres` - a fractal value-noise heightfield (8 octaves,
+  amplitude 0.15 of the extent) with 2*n*n triangles, log-uniform spheres with
+  matte/plastic/metal/glass materials (roughness U(0.05, 0.6)), lit by a Perez
+  sun and sky.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import model as M
+
+
+def cornell_box(resolution=(512, 512), light_radiance=12.0) -> M.Scene:
+    cam = M.Camera(eye=(50.0, 50.0, 220.0), look_at=(50.0, 50.0, 0.0), fov_x_deg=40.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="cornell")
+    grey = M.Matte(kd=(0.75, 0.75, 0.75))
+    red = M.Matte(kd=(0.75, 0.25, 0.25))
+    green = M.Matte(kd=(0.25, 0.75, 0.25))
+    walls = [
+        (M.Rectangle((0, 0, 0), (0, 0, 100), (100, 0, 100)), grey),        # floor, normal +y
+        (M.Rectangle((0, 100, 0), (100, 100, 0), (100, 100, 100)), grey),  # ceiling, normal -y
+        (M.Rectangle((0, 0, 0), (100, 0, 0), (100, 100, 0)), grey),        # back, normal +z
+        (M.Rectangle((0, 0, 0), (0, 100, 0), (0, 100, 100)), red),         # left, normal +x
+        (M.Rectangle((100, 0, 0), (100, 0, 100), (100, 100, 100)), green),  # right, normal -x
+    ]
+    for shape, mat in walls:
+        sc.add(M.Primitive(shape, mat))
+    sc.add(M.Primitive(M.Sphere(), M.Glass(eta=1.5), M.Transform.translate_scale((30.0, 16.5, 45.0), 16.5)))
+    sc.add(M.Primitive(M.Sphere(), M.Mirror(kr=(0.999, 0.999, 0.999)), M.Transform.translate_scale((72.0, 16.5, 70.0), 16.5)))
+    black = M.Matte(kd=(0.0, 0.0, 0.0))
+    y = 99.0
+    tris = [M.Triangle((35, y, 35), (65, y, 35), (65, y, 65)), M.Triangle((35, y, 35), (65, y, 65), (35, y, 65))]
+    for t in tris:
+        light = M.DiffuseAreaLight(t, (light_radiance,) * 3)
+        sc.lights.append(light)
+        sc.add(M.Primitive(t, black, area_light=light))
+    return sc
+
+
+def _value_noise(xs: np.ndarray, zs: np.ndarray, octaves: int, rng: np.random.Generator) -> np.ndarray:
+    """Fractal value noise on [0,1)^2, amplitude halving per octave, range about [-1, 1]."""
+    out = np.zeros((zs.size, xs.size), dtype=np.float64)
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        f = 4 * (2 ** o)
+        lattice = rng.uniform(-1.0, 1.0, size=(f + 2, f + 2))
+        gx, gz = xs * f, zs * f
+        ix, iz = np.floor(gx).astype(np.int64), np.floor(gz).astype(np.int64)
+        fx, fz = gx - ix, gz - iz
+        sx, sz = fx * fx * (3 - 2 * fx), fz * fz * (3 - 2 * fz)
+        a = lattice[np.ix_(iz, ix)]
+        b = lattice[np.ix_(iz, ix + 1)]
+        c = lattice[np.ix_(iz + 1, ix)]
+        d = lattice[np.ix_(iz + 1, ix + 1)]
+        top = a + (b - a) * sx[None, :]
+        bot = c + (d - c) * sx[None, :]
+        out += amp * (top + (bot - top) * sz[:, None])
+        total += amp
+        amp *= 0.5
+    return out / total
+
+
+def heightfield_mesh(cells: int, extent: float, seed: int, octaves: int = 8, amplitude_fraction: float = 0.15):
+    """Returns (TriangleMesh, height function data) for a cells x cells grid centred at the origin (y up)."""
+    rng = np.random.default_rng(seed)
+    n = cells + 1
+    t = np.linspace(0.0, 1.0, n, endpoint=False) + 0.5 / n
+    h = _value_noise(t, t, octaves, rng) * (amplitude_fraction * extent)
+    xs = np.linspace(-extent / 2, extent / 2, n)
+    zs = np.linspace(-extent / 2, extent / 2, n)
+    X, Z = np.meshgrid(xs, zs)
+    P = np.stack([X, h, Z], axis=-1).reshape(-1, 3)
+    # smooth vertex normals from central differences
+    dhdx = np.gradient(h, xs, axis=1)
+    dhdz = np.gradient(h, zs, axis=0)
+    N = np.stack([-dhdx, np.ones_like(h), -dhdz], axis=-1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    N = N.reshape(-1, 3)
+    U, V = np.meshgrid(np.linspace(0, 1, n), np.linspace(0, 1, n))
+    UV = np.stack([U, V], axis=-1).reshape(-1, 2)
+    i = np.arange(cells)
+    I, J = np.meshgrid(i, i)  # J rows (z), I cols (x)
+    v00 = (J * n + I).reshape(-1)
+    v10 = v00 + 1
+    v01 = v00 + n
+    v11 = v01 + 1
+    # counter-clockwise seen from +y so that the geometric normal points up
+    idx = np.concatenate([np.stack([v00, v01, v10], 1), np.stack([v10, v01, v11], 1)], axis=0)
+    mesh = M.TriangleMesh.from_positions(P.astype(np.float32), idx, uvs=UV.astype(np.float32), normals=N.astype(np.float32))
+    return mesh, (xs, zs, h)
+
+
+def _height_at(hf, x, z):
+    xs, zs, h = hf
+    fx = np.interp(x, xs, np.arange(xs.size))
+    fz = np.interp(z, zs, np.arange(zs.size))
+    ix, iz = np.clip(np.floor(fx).astype(int), 0, xs.size - 2), np.clip(np.floor(fz).astype(int), 0, zs.size - 2)
+    tx, tz = fx - ix, fz - iz
+    a, b, c, d = h[iz, ix], h[iz, ix + 1], h[iz + 1, ix], h[iz + 1, ix + 1]
+    return (a * (1 - tx) + b * tx) * (1 - tz) + (c * (1 - tx) + d * tx) * tz
+
+
+def terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2, extent=100.0, turbidity=2.5,
+                    sun_elevation_deg=35.0, sun_azimuth_deg=40.0) -> M.Scene:
+    mesh, hf = heightfield_mesh(cells, extent, seed)
+    rng = np.random.default_rng(seed + 1000)
+    cam = M.Camera(eye=(0.0, 0.30 * extent, 0.62 * extent), look_at=(0.0, 0.0, -0.05 * extent), fov_x_deg=55.0,
+                   resolution=resolution)
+    sc = M.Scene(camera=cam, name="terrain_spheres")
+    sc.add(M.Primitive(mesh, M.Matte(kd=(0.45, 0.42, 0.35))))
+    radii = np.exp(rng.uniform(math.log(0.1), math.log(2.0), size=n_spheres))
+    xs = rng.uniform(-0.45 * extent, 0.45 * extent, size=n_spheres)
+    zs = rng.uniform(-0.45 * extent, 0.45 * extent, size=n_spheres)
+    ys = _height_at(hf, xs, zs) + radii * 0.8
+    kinds = rng.integers(0, 4, size=n_spheres)
+    for k in range(n_spheres):
+        col = tuple(float(c) for c in rng.uniform(0.1, 0.9, size=3))
+        rough = float(rng.uniform(0.05, 0.6))
+        if kinds[k] == 0:
+            mat = M.Matte(kd=col)
+        elif kinds[k] == 1:
+            mat = M.Plastic(kd=col, ks=(0.5, 0.5, 0.5), roughness=rough)
+        elif kinds[k] == 2:
+            mat = M.Metal(roughness_u=rough, roughness_v=rough)
+        else:
+            mat = M.Glass(eta=1.5, roughness_u=rough, roughness_v=rough)
+        sc.add(M.Primitive(M.Sphere(), mat, M.Transform.translate_scale((xs[k], ys[k], zs[k]), radii[k])))
+    el, az = math.radians(sun_elevation_deg), math.radians(sun_azimuth_deg)
+    sun = (math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az))
+    sc.lights.append(M.PerezLight(turbidity=turbidity, sun_direction_world=sun))
+    return sc
+
+
+def small_mixed_scene(resolution=(96, 64), seed=7, cells=24, n_spheres=24, with_lights=True) -> M.Scene:
+    """A small scene that exercises every supported shape, material and light type."""
+    sc = terrain_spheres(cells=cells, n_spheres=n_spheres, resolution=resolution, seed=seed, extent=20.0)
+    rng = np.random.default_rng(seed + 5)
+    sc.add(M.Primitive(M.Rectangle((-6, 0.5, -6), (-6, 4.5, -6), (-2, 4.5, -6)), M.Matte(kd=(0.6, 0.6, 0.2), angle=20.0)))
+    sc.add(M.Primitive(M.Triangle((2, 1, -5), (6, 1, -5), (4, 5, -5)), M.Mirror(kr=(0.9, 0.9, 0.9))))
+    sc.add(M.Primitive(M.Plane(), M.Matte(kd=(0.3, 0.3, 0.3)), M.Transform.from_matrix(
+        np.array([[1, 0, 0, 0], [0, 0, 1, -3.0], [0, -1, 0, 0], [0, 0, 0, 1]], dtype=np.float64))))
+    sc.add(M.Primitive(M.Sphere(), M.Glass(eta=1.5), M.Transform.translate_scale((0.0, 3.0, 0.0), 1.5)))
+    if with_lights:
+        sc.lights.append(M.PointLight((3.0, 8.0, 4.0), (60.0, 60.0, 60.0)))
+        sc.lights.append(M.SpotLight((-4.0, 9.0, 3.0), (0.0, 0.0, 0.0), (80.0, 70.0, 60.0), 25.0, 5.0))
+        sc.lights.append(M.DirectionalLight((0.3, 1.0, 0.2), (0.8, 0.8, 0.8)))
+        tri = M.Triangle((-2, 7, -2), (2, 7, -2), (2, 7, 2))
+        al = M.DiffuseAreaLight(tri, (6.0, 6.0, 6.0))
+        sc.lights.append(al)
+        sc.add(M.Primitive(tri, M.Matte(kd=(0.0, 0.0, 0.0)), area_light=al))
+        sl = M.DiffuseAreaLight(M.Sphere(), (4.0, 3.0, 2.0), transform=M.Transform.translate_scale((5.0, 6.0, 1.0), 0.7))
+        sc.lights.append(sl)
+        sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((5.0, 6.0, 1.0), 0.7), area_light=sl))
+    del rng
+    return sc

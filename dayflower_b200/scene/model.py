@@ -1,0 +1,327 @@
+"""Scene model: the objects Dayflower's scene compiler flattens.
+
+This mirrors the parts of ``org.dayflower.scene`` that the GPU render path
+consumes (``scene/Scene.java``, ``scene/Primitive.java``, ``scene/Camera.java``,
+the shapes under ``geometry/shape/``, the materials under ``scene/material/``
+and the lights under ``scene/light/``).  It exists so that scenes can be built
+and compiled without a JVM; the renderer itself only ever sees the compiled
+arrays produced by :mod:`dayflower_b200.scene.compiler`.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+# Type ids: the ``public static final int ID`` of each reference class.
+SHAPE_CONE, SHAPE_CYLINDER, SHAPE_DISK, SHAPE_HYPERBOLOID = 2, 5, 6, 7
+SHAPE_PARABOLOID, SHAPE_PLANE, SHAPE_POLYGON, SHAPE_RECTANGLE = 9, 10, 11, 13
+SHAPE_CUBOID, SHAPE_SPHERE, SHAPE_TORUS, SHAPE_TRIANGLE, SHAPE_MESH = 14, 15, 16, 17, 18
+MAT_DISNEY, MAT_GLASS, MAT_MATTE, MAT_METAL, MAT_MIRROR, MAT_PLASTIC = 4, 7, 11, 12, 13, 14
+TEX_CONSTANT = 4
+MOD_NOOP = 2
+LIGHT_DIFFUSE_AREA, LIGHT_DIRECTIONAL, LIGHT_IMAGE, LIGHT_PEREZ = 1, 2, 3, 4
+LIGHT_POINT, LIGHT_SPOT = 5, 7
+BV_AABB, BV_SPHERE, BV_INFINITE = 1, 2, 3
+
+
+def _v(x) -> np.ndarray:
+    return np.asarray(x, dtype=np.float32).reshape(3)
+
+
+def normalize(v) -> np.ndarray:
+    v = np.asarray(v, dtype=np.float64)
+    return (v / np.linalg.norm(v)).astype(np.float32)
+
+
+class Transform:
+    """``scene/Transform.java``: an object-to-world matrix and its inverse.
+
+    Matrices are row-major 4x4 (``Matrix44F.toArray`` order)."""
+
+    def __init__(self, object_to_world: Optional[np.ndarray] = None):
+        m = np.eye(4, dtype=np.float64) if object_to_world is None else np.asarray(object_to_world, dtype=np.float64)
+        self.object_to_world = m.astype(np.float32)
+        self.world_to_object = np.linalg.inv(m).astype(np.float32)
+
+    @staticmethod
+    def translate_scale(position, scale=1.0) -> "Transform":
+        m = np.eye(4)
+        m[0, 0] = m[1, 1] = m[2, 2] = float(scale)
+        m[:3, 3] = np.asarray(position, dtype=np.float64)
+        return Transform(m)
+
+    @staticmethod
+    def from_matrix(m) -> "Transform":
+        return Transform(np.asarray(m, dtype=np.float64))
+
+    def to_array(self) -> np.ndarray:
+        """``CompiledPrimitiveCache.toMatrix44Fs(Transform)``: O2W then W2O."""
+        return np.concatenate([self.object_to_world.reshape(-1), self.world_to_object.reshape(-1)]).astype(np.float32)
+
+
+# ---------------------------------------------------------------- shapes ----
+class Shape:
+    ID = 0
+
+
+class Sphere(Shape):
+    """``geometry/shape/Sphere3F``: the unit sphere; radius comes from the transform."""
+    ID = SHAPE_SPHERE
+
+
+class Plane(Shape):
+    """``geometry/shape/Plane3F``: the plane z = 0 in object space."""
+    ID = SHAPE_PLANE
+
+
+class Triangle(Shape):
+    """``geometry/shape/Triangle3F`` with per-vertex texture coordinates and normals."""
+    ID = SHAPE_TRIANGLE
+
+    def __init__(self, a, b, c, uv=((0, 0), (0, 1), (1, 1)), normals=None):
+        self.a, self.b, self.c = _v(a), _v(b), _v(c)
+        self.uv = np.asarray(uv, dtype=np.float32).reshape(3, 2)
+        if normals is None:
+            n = normalize(np.cross(normalize(self.b - self.a), normalize(self.c - self.a)))
+            normals = (n, n, n)
+        self.normals = np.asarray(normals, dtype=np.float32).reshape(3, 3)
+
+    def to_array(self) -> np.ndarray:
+        """``CompiledShape3FCache.toTriangle3F``: 24 floats."""
+        out = np.zeros(24, dtype=np.float32)
+        out[0:3], out[3:6], out[6:9] = self.a, self.b, self.c
+        out[9:15] = self.uv.reshape(-1)
+        out[15:24] = self.normals.reshape(-1)
+        return out
+
+
+class TriangleMesh(Shape):
+    """``geometry/shape/TriangleMesh3F``: triangles given as (N, 24) compiled rows."""
+    ID = SHAPE_MESH
+
+    def __init__(self, triangles: np.ndarray):
+        t = np.ascontiguousarray(triangles, dtype=np.float32)
+        assert t.ndim == 2 and t.shape[1] == 24
+        self.triangles = t
+
+    @staticmethod
+    def from_positions(positions: np.ndarray, indices: np.ndarray, uvs=None, normals=None) -> "TriangleMesh":
+        """Builds the (N, 24) rows from an indexed vertex list."""
+        p = np.asarray(positions, dtype=np.float32)
+        idx = np.asarray(indices, dtype=np.int64).reshape(-1, 3)
+        n = idx.shape[0]
+        rows = np.zeros((n, 24), dtype=np.float32)
+        rows[:, 0:3], rows[:, 3:6], rows[:, 6:9] = p[idx[:, 0]], p[idx[:, 1]], p[idx[:, 2]]
+        if uvs is not None:
+            uv = np.asarray(uvs, dtype=np.float32)
+            rows[:, 9:11], rows[:, 11:13], rows[:, 13:15] = uv[idx[:, 0]], uv[idx[:, 1]], uv[idx[:, 2]]
+        else:
+            rows[:, 9:15] = np.array([0, 0, 0, 1, 1, 1], dtype=np.float32)
+        if normals is not None:
+            nn = np.asarray(normals, dtype=np.float32)
+            rows[:, 15:18], rows[:, 18:21], rows[:, 21:24] = nn[idx[:, 0]], nn[idx[:, 1]], nn[idx[:, 2]]
+        else:
+            a, b, c = rows[:, 0:3].astype(np.float64), rows[:, 3:6].astype(np.float64), rows[:, 6:9].astype(np.float64)
+            e1 = b - a
+            e2 = c - a
+            e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+            e2 /= np.linalg.norm(e2, axis=1, keepdims=True)
+            g = np.cross(e1, e2)
+            g /= np.linalg.norm(g, axis=1, keepdims=True)
+            rows[:, 15:18] = rows[:, 18:21] = rows[:, 21:24] = g.astype(np.float32)
+        return TriangleMesh(rows)
+
+
+class Rectangle(Shape):
+    """``geometry/shape/Rectangle3F`` given by corners a, b, c (d = a + (c - b))."""
+    ID = SHAPE_RECTANGLE
+
+    def __init__(self, a, b, c):
+        self.a, self.b, self.c = _v(a), _v(b), _v(c)
+        self.d = self.a + (self.c - self.b)
+        self.normal = normalize(np.cross(normalize(self.b - self.a), normalize(self.c - self.a)))
+
+    def to_array(self) -> np.ndarray:
+        """``CompiledShape3FCache.toRectangle3F``: 16 floats."""
+        out = np.zeros(16, dtype=np.float32)
+        out[0:3] = self.a
+        out[3:6] = self.b - self.a
+        out[6:9] = self.c - self.b
+        out[9:12] = self.normal
+        return out
+
+    def corners(self) -> np.ndarray:
+        return np.stack([self.a, self.b, self.c, self.d])
+
+
+# ------------------------------------------------------------- materials ----
+@dataclass(eq=False)
+class Material:
+    emission: Sequence[float] = (0.0, 0.0, 0.0)
+    ID = 0
+
+
+@dataclass(eq=False)
+class Matte(Material):
+    """``scene/material/MatteMaterial``."""
+    kd: Sequence[float] = (0.5, 0.5, 0.5)
+    angle: float = 0.0
+    ID = MAT_MATTE
+
+
+@dataclass(eq=False)
+class Mirror(Material):
+    """``scene/material/MirrorMaterial``."""
+    kr: Sequence[float] = (0.5, 0.5, 0.5)
+    ID = MAT_MIRROR
+
+
+@dataclass(eq=False)
+class Glass(Material):
+    """``scene/material/GlassMaterial``."""
+    kr: Sequence[float] = (1.0, 1.0, 1.0)
+    kt: Sequence[float] = (1.0, 1.0, 1.0)
+    eta: float = 1.5
+    roughness_u: float = 0.0
+    roughness_v: float = 0.0
+    remap_roughness: bool = True
+    ID = MAT_GLASS
+
+
+@dataclass(eq=False)
+class Metal(Material):
+    """``scene/material/MetalMaterial``: conductor with eta and k colours (copper defaults)."""
+    eta: Sequence[float] = (0.2004, 0.9240, 1.1022)
+    k: Sequence[float] = (3.9129, 2.4528, 2.1421)
+    roughness_u: float = 0.01
+    roughness_v: float = 0.01
+    remap_roughness: bool = True
+    ID = MAT_METAL
+
+
+@dataclass(eq=False)
+class Plastic(Material):
+    """``scene/material/PlasticMaterial``."""
+    kd: Sequence[float] = (0.2, 0.2, 0.5)
+    ks: Sequence[float] = (0.5, 0.5, 0.5)
+    roughness: float = 0.05
+    remap_roughness: bool = True
+    ID = MAT_PLASTIC
+
+
+# ---------------------------------------------------------------- lights ----
+class Light:
+    ID = 0
+
+
+class DiffuseAreaLight(Light):
+    """``scene/light/DiffuseAreaLight``: emits from a shape attached to a primitive."""
+    ID = LIGHT_DIFFUSE_AREA
+
+    def __init__(self, shape: Shape, radiance, transform: Optional[Transform] = None, two_sided: bool = False):
+        self.shape = shape
+        self.radiance = _v(radiance)
+        self.transform = transform or Transform()
+        self.two_sided = two_sided
+
+
+class PointLight(Light):
+    ID = LIGHT_POINT
+
+    def __init__(self, position, intensity):
+        self.position, self.intensity = _v(position), _v(intensity)
+
+
+class SpotLight(Light):
+    """``scene/light/SpotLight``: cone about +z of its transform."""
+    ID = LIGHT_SPOT
+
+    def __init__(self, position, look_at, intensity, cone_angle_deg=30.0, cone_delta_deg=5.0):
+        self.position = _v(position)
+        self.intensity = _v(intensity)
+        w = normalize(_v(look_at) - self.position)
+        up = np.array([0, 1, 0], dtype=np.float32) if abs(w[1]) < 0.99 else np.array([1, 0, 0], dtype=np.float32)
+        u = normalize(np.cross(up, w))
+        v = np.cross(w, u)
+        m = np.eye(4)
+        m[:3, 0], m[:3, 1], m[:3, 2], m[:3, 3] = u, v, w, self.position
+        self.transform = Transform(m)
+        self.cos_cone = math.cos(math.radians(cone_angle_deg))
+        self.cos_cone_minus_delta = math.cos(math.radians(cone_angle_deg - cone_delta_deg))
+
+
+class DirectionalLight(Light):
+    ID = LIGHT_DIRECTIONAL
+
+    def __init__(self, direction, radiance, radius=10.0):
+        self.direction, self.radiance, self.radius = normalize(direction), _v(radiance), float(radius)
+
+
+class PerezLight(Light):
+    """``scene/light/PerezLight``: Preetham sun and sky (precomputed in :mod:`perez`)."""
+    ID = LIGHT_PEREZ
+
+    def __init__(self, turbidity=2.0, sun_direction_world=(1.0, 1.0, -1.0)):
+        self.turbidity = float(turbidity)
+        self.sun_direction_world = normalize(sun_direction_world)
+
+
+# ------------------------------------------------------ camera, primitives ----
+class Camera:
+    """``scene/Camera.java`` reduced to what ``CompiledCameraCache.toCamera`` stores."""
+
+    def __init__(self, eye, look_at, up=(0, 1, 0), fov_x_deg=40.0, resolution=(800, 800), aperture_radius=0.0,
+                 focal_distance=40.0, lens_fisheye=False):
+        self.eye = _v(eye)
+        self.w = normalize(_v(look_at) - self.eye)
+        self.u = normalize(np.cross(self.w, _v(up)))
+        # u points to the image's right and v up: Camera.createPrimaryRay maps
+        # image x to +u and image row 0 (top) to +v through the negated tan(fovY/2).
+        self.v = np.cross(self.u, self.w).astype(np.float32)
+        self.fov_x_deg = float(fov_x_deg)
+        self.resolution = (int(resolution[0]), int(resolution[1]))
+        self.aperture_radius = float(aperture_radius)
+        self.focal_distance = float(focal_distance)
+        self.lens = 0 if lens_fisheye else 1
+
+    def to_array(self, resolution=None) -> np.ndarray:
+        rx, ry = resolution or self.resolution
+        fx = math.radians(self.fov_x_deg)
+        fy = 2.0 * math.atan(math.tan(fx * 0.5) * (ry / rx))  # AngleF.fieldOfViewY
+        out = np.zeros(19, dtype=np.float32)
+        out[0] = math.tan(+fx * 0.5)
+        out[1] = math.tan(-fy * 0.5)
+        out[2] = self.lens
+        out[3:6], out[6:9], out[9:12] = self.u, self.v, self.w
+        out[12:15] = self.eye
+        out[15] = self.aperture_radius
+        out[16] = self.focal_distance
+        out[17], out[18] = rx, ry
+        return out
+
+
+class Primitive:
+    """``scene/Primitive.java``: shape + material + transform (+ optional area light)."""
+
+    def __init__(self, shape: Shape, material: Material, transform: Optional[Transform] = None,
+                 area_light: Optional[DiffuseAreaLight] = None, instance_id: int = 0):
+        self.shape = shape
+        self.material = material
+        self.transform = transform or Transform()
+        self.area_light = area_light
+        self.instance_id = instance_id
+
+
+@dataclass
+class Scene:
+    camera: Camera
+    primitives: List[Primitive] = field(default_factory=list)
+    lights: List[Light] = field(default_factory=list)
+    name: str = "scene"
+
+    def add(self, p: Primitive) -> Primitive:
+        self.primitives.append(p)
+        return p

@@ -1,0 +1,157 @@
+/*
+ * dayflower_cuda.h - C ABI of libdayflower_cuda, the B200 render path that
+ * stands in for Dayflower's GPURenderer.
+ *
+ * Every entry point takes plain pointers and sizes.  Each one names the member
+ * of the reference's GPURenderer API (org.dayflower.renderer.gpu, paths are
+ * relative to src/main/java/org/dayflower/) that it replaces; INTEGRATION.md
+ * shows the Java, ctypes and C bindings.
+ *
+ * Ownership: the caller owns every host array it passes; the library copies
+ * what it keeps before returning.  The library owns all device memory.
+ *
+ * Errors: every call returns a dfc_status.  DFC_E_INVALID_ARG stands where the
+ * reference throws NullPointerException or IllegalArgumentException,
+ * DFC_E_UNSUPPORTED where the scene uses a shape, material, texture or light
+ * this renderer does not implement.  dfc_last_error() gives the message of the
+ * last failing call on a handle.
+ *
+ * Threading: a handle is not re-entrant (calls on one handle take its lock);
+ * dfc_render_shutdown() may be called from any thread while dfc_render() runs.
+ * Different handles are independent.
+ */
+#ifndef DAYFLOWER_CUDA_H
+#define DAYFLOWER_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum dfc_status {
+  DFC_OK = 0,
+  DFC_E_INVALID_ARG = 1,   /* NullPointerException / IllegalArgumentException */
+  DFC_E_UNSUPPORTED = 2,   /* unknown or unimplemented shape, material, texture or light id */
+  DFC_E_OOM = 3,           /* device allocation failed */
+  DFC_E_CUDA = 4,          /* any other CUDA runtime error */
+  DFC_E_TIMEOUT = 5,       /* a device-side iteration bound ran out (traversal stack overflow etc.) */
+  DFC_E_STOPPED = 6,       /* dfc_render_shutdown() ended the render early */
+  DFC_E_STATE = 7          /* call out of order (e.g. render before setup) */
+} dfc_status;
+
+/* RenderingAlgorithm ordinals, renderer/RenderingAlgorithm.java:33-53 */
+enum {
+  DFC_AMBIENT_OCCLUSION = 0,
+  DFC_DEPTH_CAMERA = 1,
+  DFC_PATH_TRACING = 2,
+  DFC_RAY_CASTING = 3,
+  DFC_RAY_TRACING = 4
+};
+
+/* Tone mapper ids, renderer/gpu/AbstractGPURenderer.java:54-79 */
+enum {
+  DFC_TONE_MAPPER_FILMIC_CURVE_ACES_MODIFIED_VERSION_1 = 0,
+  DFC_TONE_MAPPER_NONE = 1,
+  DFC_TONE_MAPPER_REINHARD = 2,
+  DFC_TONE_MAPPER_REINHARD_MODIFIED_VERSION_1 = 3,
+  DFC_TONE_MAPPER_REINHARD_MODIFIED_VERSION_2 = 4,
+  DFC_TONE_MAPPER_UNREAL_3 = 5
+};
+
+/* Element types for dfc_scene_put */
+enum { DFC_F32 = 0, DFC_I32 = 1 };
+
+typedef struct dfc_renderer dfc_renderer;
+
+/* new GPURenderer(rendererObserver), renderer/gpu/GPURenderer.java:43-57.
+ * Binds CUDA device `device`.  Defaults follow AbstractGPURenderer.java:148-158:
+ * 800x800 image, PATH_TRACING, maximum distance 20, maximum bounce 20,
+ * Russian roulette from bounce 5, 10 AO samples, tone mapper NONE. */
+int dfc_create(int device, dfc_renderer** out);
+
+/* dispose(), renderer/gpu/AbstractKernel.java:166.  Frees all device memory. */
+int dfc_destroy(dfc_renderer* r);
+
+/* Message of the last failing call on this handle ("" if none). */
+const char* dfc_last_error(const dfc_renderer* r);
+
+/* setScene(scene) part 1: one Aparapi put() of a CompiledScene array,
+ * renderer/gpu/AbstractSceneKernel.java:1777-1852.  `name` is the kernel field
+ * the reference uploads (e.g. "primitiveArray", "shape3FTriangle3FArray");
+ * `type` is DFC_F32 or DFC_I32; `count` elements are copied. */
+int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t count, int type);
+
+/* setScene(scene) part 2: decodes the staged arrays, builds the acceleration
+ * structure and uploads the scene.  layout_version 1 is the reference packing
+ * (scene/compiler/*, utility/Ints.java:237/:258); 2 widens material records to
+ * four int32 lanes per packed slot (no 8-bit texture limit). */
+int dfc_scene_commit(dfc_renderer* r, int layout_version);
+
+/* setImage(), AbstractGPURenderer.java:417-440: film resolution.  0,0 takes the
+ * resolution from the compiled camera. */
+int dfc_set_image(dfc_renderer* r, int width, int height);
+
+/* setMaximumBounce :448, setMinimumBounceRussianRoulette :468,
+ * setRenderingAlgorithm :504, setSamples :515 (AO rays), setMaximumDistance :458,
+ * setToneMapper :524, setPreviewMode :478 */
+int dfc_set_maximum_bounce(dfc_renderer* r, int maximum_bounce);
+int dfc_set_minimum_bounce_russian_roulette(dfc_renderer* r, int minimum_bounce);
+int dfc_set_rendering_algorithm(dfc_renderer* r, int algorithm);
+int dfc_set_samples(dfc_renderer* r, int samples);
+int dfc_set_maximum_distance(dfc_renderer* r, float maximum_distance);
+int dfc_set_tone_mapper(dfc_renderer* r, int tone_mapper);
+int dfc_set_preview_mode(dfc_renderer* r, int preview_mode);
+
+/* Seed of the counter-based random numbers (no reference counterpart: the
+ * Aparapi kernel seeds its per-pixel generators from ThreadLocalRandom). */
+int dfc_set_seed(dfc_renderer* r, uint32_t seed);
+
+/* setup(), AbstractGPURenderer.java:532: allocates the film and the wavefront
+ * queues for the current image and clears the film. */
+int dfc_setup(dfc_renderer* r);
+
+/* render(renderPasses), AbstractGPURenderer.java:322: renderPasses passes of one
+ * sample per pixel each.  *completed receives the passes done (may be NULL).
+ * Returns DFC_E_STOPPED if dfc_render_shutdown() interrupted it. */
+int dfc_render(dfc_renderer* r, int render_passes, int* completed);
+
+/* renderShutdown(), AbstractGPURenderer.java:342: asynchronous stop request. */
+int dfc_render_shutdown(dfc_renderer* r);
+
+/* clear(), AbstractGPURenderer.java:409: resets the film (next render starts at pass 0). */
+int dfc_clear(dfc_renderer* r);
+
+/* updateCamera(), AbstractSceneKernel.java:278: new 19-float compiled camera. */
+int dfc_update_camera(dfc_renderer* r, const float* camera19);
+
+/* updateMatrix44Fs(), AbstractSceneKernel.java:292: new object-to-world/world-to-object
+ * pairs, 32 floats per primitive, primitive_count * 32 floats. */
+int dfc_update_matrices(dfc_renderer* r, const float* matrices, int64_t primitive_count);
+
+/* getImage(): the film as RGBA8 after tone mapping and sRGB encoding
+ * (renderer/gpu/AbstractImageKernel.java:1104-1160), width*height*4 bytes. */
+int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t capacity_bytes);
+
+/* The radiance film: per pixel sum of accepted samples (3 floats), sum of their
+ * squares (3 floats) and sample count (1 float), width*height*7 floats. */
+int dfc_read_film(dfc_renderer* r, float* dst, int64_t capacity_floats);
+
+/* Per-pixel primitive index hit by the first pass's primary ray (-1 on a miss)
+ * and its world-space distance.  Either pointer may be NULL. */
+int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t capacity);
+
+/* Counters since the last dfc_setup/dfc_clear: passes, paths, rays traced,
+ * kernel launches.  out[4]. */
+int dfc_read_counters(dfc_renderer* r, int64_t* out4);
+
+/* Device time of the last dfc_render call, split by stage in milliseconds:
+ * out[0] total, [1] ray generation, [2] traversal, [3] shading, [4] film. */
+int dfc_read_stage_times(dfc_renderer* r, float* out5);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DAYFLOWER_CUDA_H */
