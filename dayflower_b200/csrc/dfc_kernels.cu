@@ -100,7 +100,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* 
     const DPrim& pr = S.prims[pi];
     ObjRay r = obj_ray(pr, o, d);
     float to = prim_t(S, pr, r, best * r.s);
-    if (to > 0.0f) {
+    if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
       float tw = to / r.s;
       if (tw < best) {
         best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;
@@ -156,7 +156,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* 
           const float4* tp = reinterpret_cast<const float4*>(S.tri_pos) + 3 * ti;
           const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
           const float t = tri_t(V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, V3{cc.x, cc.y, cc.z}, br.o, br.d, kTMin, bbest);
-          if (t > 0.0f && t < bbest) {
+          if (t > kTMin && t < bbest) {
             bbest = t; found = true;
             out->prim = bprim; out->aux = __float_as_int(a.w); out->t_obj = t;
             if (kAny) { out->t = t / br.s; return true; }
@@ -168,7 +168,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* 
         if (pr.shape == kShapeMesh) { ent[nent] = -2 - pi; entt[nent] = tn[k]; ++nent; continue; }
         ObjRay r = obj_ray(pr, o, d);
         const float to = prim_t(S, pr, r, best * r.s);
-        if (to > 0.0f) {
+        if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
           const float tw = to / r.s;
           if (tw < best) {
             best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;

@@ -113,7 +113,8 @@ def _height_at(hf, x, z):
 
 
 def terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2, extent=100.0, turbidity=2.5,
-                    sun_elevation_deg=35.0, sun_azimuth_deg=40.0) -> M.Scene:
+                    sun_elevation_deg=35.0, sun_azimuth_deg=40.0, kinds=(0, 1, 2, 3)) -> M.Scene:
+    """kinds: allowed sphere materials, 0 matte, 1 plastic, 2 metal, 3 glass (drawn uniformly)."""
     mesh, hf = heightfield_mesh(cells, extent, seed)
     rng = np.random.default_rng(seed + 1000)
     cam = M.Camera(eye=(0.0, 0.30 * extent, 0.62 * extent), look_at=(0.0, 0.0, -0.05 * extent), fov_x_deg=55.0,
@@ -124,7 +125,7 @@ def terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2,
     xs = rng.uniform(-0.45 * extent, 0.45 * extent, size=n_spheres)
     zs = rng.uniform(-0.45 * extent, 0.45 * extent, size=n_spheres)
     ys = _height_at(hf, xs, zs) + radii * 0.8
-    kinds = rng.integers(0, 4, size=n_spheres)
+    kinds = np.asarray(kinds)[rng.integers(0, len(kinds), size=n_spheres)]
     for k in range(n_spheres):
         col = tuple(float(c) for c in rng.uniform(0.1, 0.9, size=3))
         rough = float(rng.uniform(0.05, 0.6))
