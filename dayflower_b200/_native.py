@@ -32,6 +32,7 @@ SIGNATURES = [
     ("dfc_set_tone_mapper", _c_int, [_c_p, _c_int]),
     ("dfc_set_preview_mode", _c_int, [_c_p, _c_int]),
     ("dfc_set_seed", _c_int, [_c_p, _c_u32]),
+    ("dfc_set_stage_timing", _c_int, [_c_p, _c_int]),
     ("dfc_setup", _c_int, [_c_p]),
     ("dfc_render", _c_int, [_c_p, _c_int, ctypes.POINTER(_c_int)]),
     ("dfc_render_shutdown", _c_int, [_c_p]),

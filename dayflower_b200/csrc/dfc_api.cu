@@ -59,7 +59,7 @@ struct dfc_renderer {
   Staged staged;
   bool have_scene = false;
   HostScene host;
-  DevBuf d_prims, d_mats, d_lights, d_nodes, d_tlas_items, d_unbounded, d_tri_pos, d_tri_attr, d_rects, d_perez, d_camera;
+  DevBuf d_prims, d_mats, d_lights, d_nodes, d_tlas_items, d_tlas_bound, d_unbounded, d_tri_pos, d_tri_attr, d_rects, d_perez, d_camera;
   SceneView view{};
   // film and wavefront
   bool set_up = false;
@@ -68,9 +68,14 @@ struct dfc_renderer {
   DevBuf d_film_sum, d_film_sq, d_primary_prim, d_primary_t, d_rgba;
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_overflow, d_ray_total;
+  DevBuf d_sort_keys, d_sort_bins, d_sorted;
   DevBuf d_ao_o, d_ao_d, d_ao_v;
   int64_t pass = 0, total_paths = 0, launches = 0;
   float last_ms[5] = {0, 0, 0, 0, 0};
+  // optional per-stage timing: event pairs around every launch of a render call
+  int stage_timing = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_marks;  // (stage, index of the start event)
   int sm_count = 148;
 };
 
@@ -100,9 +105,35 @@ cudaError_t upload(dfc_renderer* r, DevBuf& b, const std::vector<T>& v) {
 __global__ void k_sum_counts(const unsigned* counts, int steps, unsigned long long* total) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     unsigned long long s = 0;
-    for (int i = 0; i < steps; ++i) s += counts[2 * i];
+    for (int i = 0; i < steps; ++i) s += counts[4 * i];
     *total += s;
   }
+}
+
+// Stage ids for dfc_read_stage_times: 1 ray generation, 2 traversal, 3 shading.
+int stage_begin(dfc_renderer* r, int stage) {
+  if (!r->stage_timing) return -1;
+  const size_t need = r->ev_marks.size() * 2 + 2;
+  while (r->ev_pool.size() < need) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    r->ev_pool.push_back(e);
+  }
+  const int i = (int)r->ev_marks.size() * 2;
+  cudaEventRecord(r->ev_pool[i], r->stream);
+  r->ev_marks.push_back({stage, i});
+  return i;
+}
+void stage_end(dfc_renderer* r, int i) {
+  if (i >= 0) cudaEventRecord(r->ev_pool[i + 1], r->stream);
+}
+void collect_stages(dfc_renderer* r) {
+  for (int k = 1; k < 5; ++k) r->last_ms[k] = 0.0f;
+  for (auto& m : r->ev_marks) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, r->ev_pool[m.second], r->ev_pool[m.second + 1]) == cudaSuccess) r->last_ms[m.first] += ms;
+  }
+  r->ev_marks.clear();
 }
 
 int alloc_wavefront(dfc_renderer* r) {
@@ -129,6 +160,8 @@ int alloc_wavefront(dfc_renderer* r) {
   }
   DFC_CK(r->d_overflow.ensure(16), "counters");
   DFC_CK(r->d_ray_total.ensure(16), "counters");
+  DFC_CK(r->d_sort_keys.ensure(P), "sort");
+  DFC_CK(r->d_sorted.ensure(P * 4), "sort");
   return DFC_OK;
 }
 
@@ -159,11 +192,11 @@ ShadeArgs shade_args(dfc_renderer* r, int step) {
   a.ao_samples = r->ao_samples;
   unsigned* counts = r->d_counts.as<unsigned>();
   a.work_list = r->d_work_list[step & 1].as<unsigned>();
-  a.work_count = counts + 2 * step + 1;
+  a.work_count = counts + 4 * step + 1;
   a.next_work_list = r->d_work_list[(step + 1) & 1].as<unsigned>();
-  a.next_work_count = counts + 2 * (step + 1) + 1;
+  a.next_work_count = counts + 4 * (step + 1) + 1;
   a.next_ray_list = r->d_ray_list[(step + 1) & 1].as<unsigned>();
-  a.next_ray_count = counts + 2 * (step + 1);
+  a.next_ray_count = counts + 4 * (step + 1);
   a.beta = r->d_beta.as<float4>();
   a.radiance = r->d_rad.as<float4>();
   a.meta = r->d_meta.as<uint4>();
@@ -186,7 +219,8 @@ TraceArgs trace_args(dfc_renderer* r, int step) {
   t.scene = r->view;
   unsigned* counts = r->d_counts.as<unsigned>();
   t.ray_list = r->d_ray_list[step & 1].as<unsigned>();
-  t.ray_count = counts + 2 * step;
+  t.ray_count = counts + 4 * step;
+  t.fetch = counts + 4 * step + 2;
   t.ray_o = r->d_ray_o.as<float4>();
   t.ray_d = r->d_ray_d.as<float4>();
   t.hits = r->d_hits.as<float4>();
@@ -199,7 +233,7 @@ TraceArgs trace_args(dfc_renderer* r, int step) {
 int enqueue_pass(dfc_renderer* r) {
   const int algo = r->algorithm;
   const int steps = algo == DFC_PATH_TRACING ? r->max_bounce + 4 : 1;
-  const size_t counts_bytes = (size_t)(steps + 2) * 2 * sizeof(unsigned);
+  const size_t counts_bytes = (size_t)(steps + 2) * 4 * sizeof(unsigned);
   DFC_CK(r->d_counts.ensure(counts_bytes), "counters");
   DFC_CK(cudaMemsetAsync(r->d_counts.p, 0, counts_bytes, r->stream), "counters");
   unsigned* counts = r->d_counts.as<unsigned>();
@@ -219,17 +253,39 @@ int enqueue_pass(dfc_renderer* r) {
   g.ray_count = counts;
   g.work_list = r->d_work_list[0].as<unsigned>();
   g.work_count = counts + 1;
+  int ev = stage_begin(r, 1);
   k_raygen<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(g);
+  stage_end(r, ev);
   r->launches++;
   const int trace_grid = r->sm_count * 6;
   const int shade_grid = r->sm_count * 8;
   if (algo == DFC_PATH_TRACING) {
+    const size_t bins_bytes = (size_t)steps * 2 * kSortBins * sizeof(unsigned);
+    DFC_CK(r->d_sort_bins.ensure(bins_bytes), "sort");
+    DFC_CK(cudaMemsetAsync(r->d_sort_bins.p, 0, bins_bytes, r->stream), "sort");
     for (int s = 0; s < steps; ++s) {
+      ev = stage_begin(r, 2);
       k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, s));
+      stage_end(r, ev);
       ShadeArgs a = shade_args(r, s);
       a.last_step = s == steps - 1;
+      SortArgs so{};
+      so.scene = r->view;
+      so.paths = r->paths;
+      so.work_list = a.work_list;
+      so.work_count = a.work_count;
+      so.meta = a.meta;
+      so.hits = a.hits;
+      so.keys = r->d_sort_keys.as<unsigned char>();
+      so.bins = r->d_sort_bins.as<unsigned>() + (size_t)s * 2 * kSortBins;
+      so.sorted = r->d_sorted.as<unsigned>();
+      ev = stage_begin(r, 3);
+      k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
+      k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
+      a.work_list = so.sorted;
       k_shade_path<<<shade_grid, 256, 0, r->stream>>>(a);
-      r->launches += 2;
+      stage_end(r, ev);
+      r->launches += 4;
     }
   } else {
     k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, 0));
@@ -295,6 +351,7 @@ int dfc_destroy(dfc_renderer* r) {
   }
   cudaEventDestroy(r->ev0);
   cudaEventDestroy(r->ev1);
+  for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
   cudaStream_t s = r->stream;
   delete r;  // DevBuf destructors free device memory
   cudaStreamDestroy(s);
@@ -334,6 +391,7 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   DFC_CK(upload(r, r->d_lights, hs.lights), "scene upload");
   DFC_CK(upload(r, r->d_nodes, hs.nodes), "scene upload");
   DFC_CK(upload(r, r->d_tlas_items, hs.tlas_items), "scene upload");
+  DFC_CK(upload(r, r->d_tlas_bound, hs.tlas_bound), "scene upload");
   DFC_CK(upload(r, r->d_unbounded, hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded), "scene upload");
   DFC_CK(upload(r, r->d_tri_pos, hs.tri_pos), "scene upload");
   DFC_CK(upload(r, r->d_tri_attr, hs.tri_attr), "scene upload");
@@ -351,6 +409,7 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   v.nodes = r->d_nodes.as<BVH4Node>();
   v.tlas_root = hs.tlas_root;
   v.tlas_items = r->d_tlas_items.as<int>();
+  v.tlas_bound = r->d_tlas_bound.as<F4>();
   v.unbounded = r->d_unbounded.as<int>();
   v.unbounded_count = (int)hs.unbounded.size();
   v.tri_pos = r->d_tri_pos.as<F4>();
@@ -408,6 +467,13 @@ int dfc_set_maximum_distance(dfc_renderer* r, float v) {
   return DFC_OK;
 }
 
+int dfc_set_stage_timing(dfc_renderer* r, int on) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  r->stage_timing = on ? 1 : 0;
+  return DFC_OK;
+}
+
 int dfc_set_seed(dfc_renderer* r, uint32_t seed) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
   std::lock_guard<std::mutex> lk(r->mu);
@@ -457,6 +523,7 @@ int dfc_render(dfc_renderer* r, int passes, int* completed) {
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, r->ev0, r->ev1);
   r->last_ms[0] = ms;
+  collect_stages(r);
   unsigned ov = 0;
   DFC_CK(cudaMemcpy(&ov, r->d_overflow.p, 4, cudaMemcpyDeviceToHost), "readback");
   if (completed) *completed = done;

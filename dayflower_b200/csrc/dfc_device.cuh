@@ -134,6 +134,14 @@ DFC_D bool camera_ray(const float* c, float ix, float iy, float px, float py, fl
 // ---------------------------------------------------------- intersection --
 DFC_D float gamma_n(int n) { const float e = 5.9604645e-8f; return (n * e) / (1.0f - n * e); }
 
+// Double-precision edge functions (Triangle3F.java:537-546), taken only when a
+// float edge function is exactly zero; kept out of line to keep the hot loop small.
+__device__ __noinline__ void tri_edges_fp64(float x0, float y0, float x1, float y1, float x2, float y2, float* e0, float* e1, float* e2) {
+  *e0 = (float)((double)y2 * (double)x1 - (double)x2 * (double)y1);
+  *e1 = (float)((double)y0 * (double)x2 - (double)x0 * (double)y2);
+  *e2 = (float)((double)y1 * (double)x0 - (double)x1 * (double)y0);
+}
+
 // geometry/shape/Triangle3F.java:505 watertight test; returns -1 on a miss.
 DFC_D float tri_t(V3 a, V3 b, V3 c, V3 o, V3 d, float tmin, float tmax) {
   V3 p0 = a - o, p1 = b - o, p2 = c - o;
@@ -151,11 +159,7 @@ DFC_D float tri_t(V3 a, V3 b, V3 c, V3 o, V3 d, float tmin, float tmax) {
   float e0 = x1 * y2 - y1 * x2;
   float e1 = x2 * y0 - y2 * x0;
   float e2 = x0 * y1 - y0 * x1;
-  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) {
-    e0 = (float)((double)y2 * (double)x1 - (double)x2 * (double)y1);
-    e1 = (float)((double)y0 * (double)x2 - (double)x0 * (double)y2);
-    e2 = (float)((double)y1 * (double)x0 - (double)x1 * (double)y0);
-  }
+  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) tri_edges_fp64(x0, y0, x1, y1, x2, y2, &e0, &e1, &e2);
   if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
   const float det = e0 + e1 + e2;
   if (det == 0.0f) return -1.0f;
@@ -196,7 +200,19 @@ DFC_D EF ef_div(EF a, EF b) {
   return {v, ndn(fminf(fminf(d0, d1), fminf(d2, d3))), nup(fmaxf(fmaxf(d0, d1), fmaxf(d2, d3)))};
 }
 // geometry/shape/Sphere3F.java:507, unit sphere; returns -1 on a miss.
+__device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax);
+// A float pre-test that only rejects rays that clearly miss (the closest
+// approach of the line is outside the sphere by a margin far above rounding),
+// so that most candidate spheres never reach the interval-arithmetic test.
 DFC_D float sphere_t(V3 o, V3 d, float tmin, float tmax) {
+  const float b = o.x * d.x + o.y * d.y + o.z * d.z;
+  const float oo = o.x * o.x + o.y * o.y + o.z * o.z;
+  const float disc = b * b - (oo - 1.0f);
+  // float rounding of b*b and oo is below 1e-6 (1 + oo); reject only beyond 1e-5 (1 + oo)
+  if (disc < -1.0e-5f * (1.0f + oo)) return -1.0f;
+  return sphere_t_exact(o, d, tmin, tmax);
+}
+__device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax) {
   EF ox = ef(o.x), oy = ef(o.y), oz = ef(o.z), dx = ef(d.x), dy = ef(d.y), dz = ef(d.z);
   EF a = ef_add(ef_add(ef_mul(dx, dx), ef_mul(dy, dy)), ef_mul(dz, dz));
   EF b = ef_mul(ef(2.0f), ef_add(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_mul(dz, oz)));

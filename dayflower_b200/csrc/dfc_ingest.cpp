@@ -294,6 +294,39 @@ struct Decoder {
     }
   }
 
+  // World bounding sphere of a top-level item, used by the traversal to reject
+  // candidates before the exact object-space test.  Spheres: the image of the
+  // unit sphere under the object-to-world map lies within the largest singular
+  // value of its 3x3 part around the translated origin.  Meshes are marked with
+  // a negative radius (they are entered, not tested).  Others: the box's sphere.
+  F4 bounding_sphere(const DPrim& pr, const Box& b) {
+    if (pr.shape == kShapeMesh) return F4{0, 0, 0, -1};
+    if (pr.shape == kShapeSphere) {
+      const float* m = pr.o2w;
+      double a[3][3] = {{m[0], m[1], m[2]}, {m[4], m[5], m[6]}, {m[8], m[9], m[10]}};
+      double ata[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) ata[i][j] = a[0][i] * a[0][j] + a[1][i] * a[1][j] + a[2][i] * a[2][j];
+      double v[3] = {1, 1, 1}, lam = 0;
+      for (int it = 0; it < 64; ++it) {
+        double w[3] = {ata[0][0] * v[0] + ata[0][1] * v[1] + ata[0][2] * v[2], ata[1][0] * v[0] + ata[1][1] * v[1] + ata[1][2] * v[2],
+                       ata[2][0] * v[0] + ata[2][1] * v[1] + ata[2][2] * v[2]};
+        double nw = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        if (nw == 0) break;
+        lam = nw;
+        for (int k = 0; k < 3; ++k) v[k] = w[k] / nw;
+      }
+      // the Frobenius norm bounds the largest singular value from above; take the
+      // smaller of the two bounds with a relative margin
+      double frob = std::sqrt(ata[0][0] + ata[1][1] + ata[2][2]);
+      double r = std::fmin(std::sqrt(lam) * (1.0 + 1e-4), frob);
+      return F4{m[3], m[7], m[11], (float)(r * (1.0 + 1e-5))};
+    }
+    float c[3], r2 = 0;
+    for (int k = 0; k < 3; ++k) { c[k] = 0.5f * (b.lo[k] + b.hi[k]); float h = 0.5f * (b.hi[k] - b.lo[k]); r2 += h * h; }
+    return F4{c[0], c[1], c[2], std::sqrt(r2) * 1.0001f + 1e-6f};
+  }
+
   // Collects the triangle offsets of one mesh by walking its threaded stream.
   void mesh_triangles(int off, std::vector<int>& tris) {
     const auto& M = I("shape3FTriangleMesh3FArray");
@@ -343,6 +376,7 @@ struct Decoder {
     std::vector<BlasInfo> blas_info;
     std::vector<Box> tlas_boxes;
     std::vector<int> tlas_prims;
+    std::vector<F4> tlas_spheres;
     for (int p = 0; p < np; ++p) {
       const int32_t* q = P.data() + (size_t)p * 8;
       const float* m = X.data() + (size_t)p * 32;
@@ -443,18 +477,23 @@ struct Decoder {
         }
         tlas_boxes.push_back(b);
         tlas_prims.push_back(p);
+        tlas_spheres.push_back(bounding_sphere(pr, b));
       }
       hs.prims.push_back(pr);
     }
     if (!tlas_boxes.empty()) {
       std::vector<int> order;
-      hs.tlas_root = build_bvh4(tlas_boxes, 1, hs.nodes, order);
+      hs.tlas_root = build_bvh4(tlas_boxes, 4, hs.nodes, order);
       hs.tlas_items.resize(order.size());
-      for (size_t k = 0; k < order.size(); ++k) hs.tlas_items[k] = tlas_prims[order[k]];
+      hs.tlas_bound.resize(order.size());
+      for (size_t k = 0; k < order.size(); ++k) {
+        hs.tlas_items[k] = tlas_prims[order[k]];
+        hs.tlas_bound[k] = tlas_spheres[order[k]];
+      }
     } else {
       hs.tlas_root = -1;
     }
-    if (hs.tlas_items.empty()) hs.tlas_items.push_back(0);
+    if (hs.tlas_items.empty()) { hs.tlas_items.push_back(0); hs.tlas_bound.push_back(F4{0, 0, 0, -1}); }
     if (hs.unbounded.empty()) hs.unbounded_storage.push_back(0);
     if (hs.tri_pos.empty()) hs.tri_pos.assign(3, F4{0, 0, 0, 0});
     if (hs.nodes.empty()) hs.nodes.push_back(BVH4Node{});

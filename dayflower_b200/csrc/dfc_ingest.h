@@ -23,6 +23,7 @@ struct HostScene {
   std::vector<DLight> lights;
   std::vector<BVH4Node> nodes;
   std::vector<int> tlas_items;
+  std::vector<F4> tlas_bound;
   std::vector<int> unbounded;
   std::vector<int> unbounded_storage;  // non-empty stand-in when there are no unbounded primitives
   std::vector<F4> tri_pos;

@@ -53,7 +53,8 @@ DFC_D ObjRay obj_ray(const DPrim& pr, V3 o, V3 d) {
 }
 
 // Object-space test of one analytic primitive; returns the object distance or -1.
-DFC_D float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
+// Out of line: called at top-level leaves only, it keeps the traversal loop small.
+__device__ __noinline__ float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
   switch (pr.shape) {
     case kShapeSphere: return sphere_t(r.o, r.d, kTMin, tmax_obj);
     case kShapeTriangle: {
@@ -64,6 +65,20 @@ DFC_D float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float t
     case kShapePlane: return plane_t(r.o, r.d, kTMin, tmax_obj);
     default: return -1.0f;
   }
+}
+
+// Conservative world-space rejection of a top-level item by its bounding
+// sphere (centre, radius): false only when the ray line passes outside the
+// sphere by a clear margin, or the whole sphere lies beyond the current best.
+DFC_D bool sphere_may_hit(float4 bs, V3 o, V3 d, float best) {
+  const float ox = bs.x - o.x, oy = bs.y - o.y, oz = bs.z - o.z;
+  const float tca = ox * d.x + oy * d.y + oz * d.z;
+  const float oc2 = ox * ox + oy * oy + oz * oz;
+  const float d2 = oc2 - tca * tca;
+  const float r2 = bs.w * bs.w;
+  if (d2 > r2 * 1.001f + 1.0e-5f * oc2 + 1.0e-12f) return false;
+  if (tca - bs.w * 1.001f > best * 1.0001f + 1.0e-6f * fabsf(tca)) return false;
+  return true;
 }
 
 // 4 child slab tests of one node; returns a hit mask and the entry distances.
@@ -91,10 +106,13 @@ DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin
 // this thread's column of the block's shared stack (stride kTraceBlock).
 // Stack entries: >= 0 node index; -1 end of a bottom level (back to world
 // space); <= -2 enter the bottom level of mesh primitive (-2 - entry).
-template <bool kAny>
-DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* stack, unsigned* overflow) {
+DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit* out, int* stack, unsigned* overflow) {
   float best = tmax;
   bool found = false;
+  // A ray with a non-finite origin or direction hits nothing in the reference
+  // (every bounding-volume and shape test compares false against NaN); here a
+  // NaN would pass every slab test (fmaxf drops NaN), so stop it up front.
+  if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) { out->t = tmax; return false; }
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
@@ -163,16 +181,25 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* 
           }
         }
       } else {
-        const int pi = S.tlas_items[first];
-        const DPrim& pr = S.prims[pi];
-        if (pr.shape == kShapeMesh) { ent[nent] = -2 - pi; entt[nent] = tn[k]; ++nent; continue; }
-        ObjRay r = obj_ray(pr, o, d);
-        const float to = prim_t(S, pr, r, best * r.s);
-        if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
-          const float tw = to / r.s;
-          if (tw < best) {
-            best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;
-            if (kAny) { out->t = best; return true; }
+        for (int j = 0; j < cnt; ++j) {
+          const int pi = S.tlas_items[first + j];
+          const float4 bs = __ldg(reinterpret_cast<const float4*>(S.tlas_bound) + first + j);
+          if (bs.w < 0.0f) {
+            if (nent < 4) { ent[nent] = -2 - pi; entt[nent] = tn[k]; ++nent; }
+            else if (sp < kStack) stack[(sp++) * kTraceBlock] = -2 - pi;
+            else atomicAdd(overflow, 1u);
+            continue;
+          }
+          if (!sphere_may_hit(bs, o, d, best)) continue;
+          const DPrim& pr = S.prims[pi];
+          ObjRay r = obj_ray(pr, o, d);
+          const float to = prim_t(S, pr, r, best * r.s);
+          if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
+            const float tw = to / r.s;
+            if (tw < best) {
+              best = tw; found = true; out->prim = pi; out->aux = pr.data; out->t_obj = to;
+              if (kAny) { out->t = best; return true; }
+            }
           }
         }
       }
@@ -200,26 +227,177 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, Hit* out, int* 
 constexpr unsigned kAlive = kFlagAlive, kPendShadow = kFlagPendShadow, kPendMis = kFlagPendMis, kShadowAny = kFlagShadowAny,
                    kNoSample = kFlagNoSample;
 
+// ---- persistent traversal with per-lane refill ---------------------------
+// The same walk as trace_ray, held in registers across iterations so that a
+// lane whose ray is done takes a new ray from the queue instead of idling
+// until the slowest lane of its warp finishes (ray costs are heavy-tailed).
+struct Trav {
+  V3 o, d, winv;
+  float best, bbest;
+  ObjRay br;
+  int sp, bprim;
+  bool any, found, in_blas;
+  Hit h;
+};
+
+DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack) {
+  T.o = o; T.d = d; T.best = tmax; T.bbest = 0.0f; T.any = any; T.found = false; T.in_blas = false;
+  T.sp = 0; T.bprim = -1; T.br.s = 1.0f;
+  T.h.t = tmax; T.h.prim = -1; T.h.aux = -1; T.h.t_obj = 0.0f;
+  if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
+  for (int u = 0; u < S.unbounded_count; ++u) {
+    const int pi = S.unbounded[u];
+    const DPrim& pr = S.prims[pi];
+    ObjRay r = obj_ray(pr, o, d);
+    const float to = prim_t(S, pr, r, T.best * r.s);
+    if (to > kTMin) {
+      const float tw = to / r.s;
+      if (tw < T.best) {
+        T.best = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+        if (any) return;
+      }
+    }
+  }
+  T.winv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
+}
+
+// Stack entries (32 bits):
+//   0x00000000 | node                 an interior node
+//   0x80000000 | first << 2 | (n - 1) a leaf of n items starting at `first`
+//   0xC0000000 | prim                 enter the bottom level of mesh primitive `prim`
+//   0xFFFFFFFF                        end of a bottom level (back to world space)
+constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0xC0000000u, kEndBlas = 0xFFFFFFFFu;
+
+#define DFC_CSWAP(ta, ea, tb, eb) \
+  if (tb < ta) { const float tt_ = ta; ta = tb; tb = tt_; const unsigned ee_ = ea; ea = eb; eb = ee_; }
+
+// Processes one stack entry; returns true once the ray is finished.
+DFC_D bool trav_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow) {
+  if (T.sp == 0) return true;
+  const unsigned e = (unsigned)stack[(--T.sp) * kTraceBlock];
+  if ((e & kTagMask) == 0u) {
+    // interior node: test the four children, push the hit ones far-to-near
+    float tn[4];
+    const unsigned mask = T.in_blas ? node_hits(S.nodes, (int)e, T.br.o, T.br.inv, 0.0f, T.bbest, tn)
+                                    : node_hits(S.nodes, (int)e, T.o, T.winv, 0.0f, T.best, tn);
+    if (!mask) return T.sp == 0;
+    const int4* cp = reinterpret_cast<const int4*>(S.nodes + e) + 6;
+    const int4 ch = __ldg(cp), cn = __ldg(cp + 1);
+    const float inf = __int_as_float(0x7f800000);
+    auto entry = [](int c, int n) -> unsigned { return c >= 0 ? (unsigned)c : (kTagLeaf | ((unsigned)(~c) << 2) | (unsigned)(n - 1)); };
+    float t0 = (mask & 1u) ? tn[0] : inf, t1 = (mask & 2u) ? tn[1] : inf, t2 = (mask & 4u) ? tn[2] : inf, t3 = (mask & 8u) ? tn[3] : inf;
+    unsigned e0 = entry(ch.x, cn.x), e1 = entry(ch.y, cn.y), e2 = entry(ch.z, cn.z), e3 = entry(ch.w, cn.w);
+    DFC_CSWAP(t0, e0, t1, e1);
+    DFC_CSWAP(t2, e2, t3, e3);
+    DFC_CSWAP(t0, e0, t2, e2);
+    DFC_CSWAP(t1, e1, t3, e3);
+    DFC_CSWAP(t1, e1, t2, e2);
+    const int n = __popc(mask);
+    if (T.sp + n > kStack) { atomicAdd(overflow, 1u); return T.sp == 0; }
+    // ascending t0 <= t1 <= t2 <= t3 (misses last as +inf): push the n hits far first
+    if (n > 3) stack[(T.sp++) * kTraceBlock] = (int)e3;
+    if (n > 2) stack[(T.sp++) * kTraceBlock] = (int)e2;
+    if (n > 1) stack[(T.sp++) * kTraceBlock] = (int)e1;
+    stack[(T.sp++) * kTraceBlock] = (int)e0;
+    return false;
+  }
+  if ((e & kTagMask) == kTagLeaf) {
+    const int first = (int)((e & ~kTagMask) >> 2), cnt = (int)(e & 3u) + 1;
+    if (T.in_blas) {
+      for (int j = 0; j < cnt; ++j) {
+        const float4* tp = reinterpret_cast<const float4*>(S.tri_pos) + 3 * (first + j);
+        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+        const float t = tri_t(V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, V3{cc.x, cc.y, cc.z}, T.br.o, T.br.d, kTMin, T.bbest);
+        if (t > kTMin && t < T.bbest) {
+          T.bbest = t; T.found = true;
+          T.h.prim = T.bprim; T.h.aux = __float_as_int(a.w); T.h.t_obj = t;
+          if (T.any) { T.best = t / T.br.s; T.in_blas = false; T.sp = 0; return true; }
+        }
+      }
+    } else {
+      for (int j = 0; j < cnt; ++j) {
+        const int pi = S.tlas_items[first + j];
+        const float4 bs = __ldg(reinterpret_cast<const float4*>(S.tlas_bound) + first + j);
+        if (bs.w < 0.0f) {  // a mesh: enter its bottom level next
+          if (T.sp < kStack) stack[(T.sp++) * kTraceBlock] = (int)(kTagMesh | (unsigned)pi);
+          else atomicAdd(overflow, 1u);
+          continue;
+        }
+        if (!sphere_may_hit(bs, T.o, T.d, T.best)) continue;
+        const DPrim& pr = S.prims[pi];
+        ObjRay r = obj_ray(pr, T.o, T.d);
+        const float to = prim_t(S, pr, r, T.best * r.s);
+        if (to > kTMin) {
+          const float tw = to / r.s;
+          if (tw < T.best) {
+            T.best = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+            if (T.any) { T.sp = 0; return true; }
+          }
+        }
+      }
+    }
+    return T.sp == 0;
+  }
+  if (e == kEndBlas) {
+    T.in_blas = false;
+    T.best = fminf(T.best, T.bbest / T.br.s);
+    return T.sp == 0;
+  }
+  // enter a mesh's bottom level
+  T.bprim = (int)(e & ~kTagMask);
+  const DPrim& pm = S.prims[T.bprim];
+  T.br = obj_ray(pm, T.o, T.d);
+  T.bbest = T.best * T.br.s;
+  if (T.sp + 2 > kStack) { atomicAdd(overflow, 1u); return T.sp == 0; }
+  T.in_blas = true;
+  stack[(T.sp++) * kTraceBlock] = (int)kEndBlas;
+  stack[(T.sp++) * kTraceBlock] = pm.data;
+  return false;
+}
+
+constexpr unsigned kNoRay = 0xffffffffu;
+constexpr int kRefill = 8;        // refill a warp's idle lanes once this many are idle
+constexpr int kStepsPerRefill = 24;
+
 __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
   __shared__ int stack_smem[kStack * kTraceBlock];
   int* stack = stack_smem + threadIdx.x;
   const unsigned n = *a.ray_count;
-  const unsigned stride = gridDim.x * blockDim.x;
-  // Every lane of a warp runs the loop the same number of times so that the
-  // ballot in warp_append stays convergent (inactive lanes idle through it).
-  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    const unsigned i = base + threadIdx.x;
-    if (i < n) {
-      const unsigned ref = a.ray_list[i];
-      const unsigned p = ref >> 3, type = ref & 3u;
-      const bool any = (ref & 4u) != 0u;
-      const size_t slot = (size_t)type * a.paths + p;
-      const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
-      Hit h = {0.0f, -1, -1, 0.0f};
-      bool hit;
-      if (any) hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, &h, stack, a.overflow);
-      else hit = trace_ray<false>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, &h, stack, a.overflow);
-      a.hits[slot] = make_float4(h.t, __int_as_float(hit ? h.prim : -1), __int_as_float(h.aux), h.t_obj);
+  const unsigned lane = threadIdx.x & 31u;
+  Trav T;
+  unsigned cur = kNoRay;
+  size_t slot = 0;
+  bool pool_empty = false;  // warp-uniform
+  while (true) {
+    const bool idle = cur == kNoRay;
+    const unsigned idle_mask = __ballot_sync(0xffffffffu, idle);
+    if (!pool_empty && __popc(idle_mask) >= kRefill) {
+      const int leader = __ffs(idle_mask) - 1;
+      unsigned base = 0;
+      if ((int)lane == leader) base = atomicAdd(a.fetch, (unsigned)__popc(idle_mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (base + (unsigned)__popc(idle_mask) >= n) pool_empty = true;
+      if (idle) {
+        const unsigned i = base + (unsigned)__popc(idle_mask & ((1u << lane) - 1u));
+        if (i < n) {
+          cur = i;
+          const unsigned ref = a.ray_list[i];
+          const unsigned p = ref >> 3, type = ref & 3u;
+          slot = (size_t)type * a.paths + p;
+          const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
+          trav_init(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
+        }
+      }
+    }
+    if (pool_empty && __all_sync(0xffffffffu, cur == kNoRay)) break;
+    if (cur != kNoRay) {
+      bool done = false;
+      for (int it = 0; it < kStepsPerRefill && !done; ++it) done = trav_step(a.scene, T, stack, a.overflow);
+      if (done) {
+        a.hits[slot] = make_float4(T.best, __int_as_float(T.found ? T.h.prim : -1), __int_as_float(T.h.aux), T.h.t_obj);
+        cur = kNoRay;
+      }
     }
   }
 }
@@ -505,6 +683,52 @@ __global__ void k_shade_path(ShadeArgs a) {
   }
 }
 
+// ---- material sort of the shade work list -----------------------------------
+// Shading diverges badly when one warp holds paths on different materials (each
+// material is a different BSDF routine), so the work list of every step is
+// counting-sorted by material kind before shading.
+__global__ void k_sort_count(SortArgs a) {
+  __shared__ unsigned cnt[kSortBins];
+  if (threadIdx.x < kSortBins) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const unsigned n = *a.work_count;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned p = a.work_list[i];
+    int key = kMatKinds + 1;
+    if (a.meta[p].w & kFlagAlive) {
+      const int hp = __float_as_int(a.hits[p].y);
+      key = hp < 0 ? kMatKinds : a.scene.materials[a.scene.prims[hp].material].kind;
+    }
+    a.keys[i] = (unsigned char)key;
+    atomicAdd(&cnt[key], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < kSortBins && cnt[threadIdx.x]) atomicAdd(&a.bins[threadIdx.x], cnt[threadIdx.x]);
+}
+
+__global__ void k_sort_scatter(SortArgs a) {
+  __shared__ unsigned start[kSortBins];
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int k = 0; k < kSortBins; ++k) { start[k] = acc; acc += a.bins[k]; }
+  }
+  __syncthreads();
+  const unsigned n = *a.work_count;
+  const unsigned lane = threadIdx.x & 31u;
+  for (unsigned base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const unsigned i = base + threadIdx.x;
+    const bool valid = i < n;
+    const int key = valid ? (int)a.keys[i] : -1;
+    // one atomic per distinct key in the warp
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    unsigned pos = 0;
+    if (valid && (int)lane == leader) pos = atomicAdd(&a.bins[kSortBins + key], (unsigned)__popc(peers));
+    pos = __shfl_sync(0xffffffffu, pos, leader);
+    if (valid) a.sorted[start[key] + pos + (unsigned)__popc(peers & ((1u << lane) - 1u))] = a.work_list[i];
+  }
+}
+
 // RAY_CASTING (Scene.java:675) and DEPTH_CAMERA (Scene.java:327) on the
 // primary hits; AO spawns its occlusion rays (Scene.java:272).
 __global__ void k_shade_primary(ShadeArgs a, int algorithm) {
@@ -569,10 +793,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(AoArgs a) {
     Hit h = {0.0f, -1, -1, 0.0f};
     float v;
     if (a.max_distance > 0.0f) {
-      bool hit = trace_ray<false>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, &h, stack, a.overflow);
+      bool hit = trace_ray(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, false, &h, stack, a.overflow);
       v = hit ? clampf(h.t, 0.0f, a.max_distance) / a.max_distance : 1.0f;
     } else {
-      bool hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, &h, stack, a.overflow);
+      bool hit = trace_ray(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, true, &h, stack, a.overflow);
       v = hit ? 0.0f : 1.0f;
     }
     a.ao_value[i] = v;

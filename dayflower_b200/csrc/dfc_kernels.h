@@ -21,6 +21,7 @@ struct TraceArgs {
   float4* hits;         // t_world, prim (int bits, -1 miss), aux (int bits), t_object
   unsigned paths;
   unsigned* overflow;
+  unsigned* fetch;      // rays handed out so far in this launch (starts at 0)
 };
 
 struct RaygenArgs {
@@ -75,6 +76,24 @@ struct AoArgs {
   float* ao_value;
   unsigned* overflow;
 };
+
+// Material sort of a shade work list: key = material kind of the extension
+// hit (0 .. kMatKinds-1), kMatKinds for a miss, kMatKinds + 1 for a path with
+// nothing left to shade (pending light rays only).
+constexpr int kSortBins = kMatKinds + 2;
+struct SortArgs {
+  SceneView scene;
+  unsigned paths;
+  const unsigned* work_list;
+  const unsigned* work_count;
+  const uint4* meta;
+  const float4* hits;
+  unsigned char* keys;     // one per work item
+  unsigned* bins;          // kSortBins counts, then kSortBins cursors
+  unsigned* sorted;        // the work list in key order
+};
+__global__ void k_sort_count(SortArgs a);
+__global__ void k_sort_scatter(SortArgs a);
 
 __global__ void k_raygen(RaygenArgs a);
 __global__ void k_trace(TraceArgs a);

@@ -112,6 +112,7 @@ struct SceneView {
   const BVH4Node* nodes;        // top level and all bottom levels
   int tlas_root;                // -1 if no bounded primitive
   const int* tlas_items;        // primitive index per top-level leaf item
+  const F4* tlas_bound;         // per leaf item: world bounding sphere (centre, radius); radius < 0 for meshes
   const int* unbounded;         // primitives with an infinite bounding volume (planes)
   int unbounded_count;
   const F4* tri_pos;            // 3 per triangle, reordered; v0.w holds the triangle index

@@ -120,6 +120,7 @@ class GPURenderer:
     def setToneMapper(self, v: int): self._check(self._lib.dfc_set_tone_mapper(self._h, int(v)))
     def setPreviewMode(self, v: bool): self._check(self._lib.dfc_set_preview_mode(self._h, 1 if v else 0))
     def setSeed(self, seed: int): self._check(self._lib.dfc_set_seed(self._h, int(seed) & 0xFFFFFFFF))
+    def setStageTiming(self, on: bool): self._check(self._lib.dfc_set_stage_timing(self._h, 1 if on else 0))
 
     def setRenderingAlgorithm(self, algorithm):
         if algorithm is None:
@@ -215,6 +216,10 @@ class GPURenderer:
         return {"passes": int(out[0]), "paths": int(out[1]), "rays": int(out[2]), "launches": int(out[3])}
 
     def lastRenderMillis(self) -> float:
+        return self.stageMillis()["total"]
+
+    def stageMillis(self):
+        """Device milliseconds of the last render call: total and, with stage timing on, per stage."""
         out = np.zeros(5, dtype=np.float32)
         self._check(self._lib.dfc_read_stage_times(self._h, out.ctypes.data_as(ctypes.c_void_p)))
-        return float(out[0])
+        return {"total": float(out[0]), "raygen": float(out[1]), "trace": float(out[2]), "shade": float(out[3]), "film": float(out[4])}

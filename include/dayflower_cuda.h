@@ -108,6 +108,11 @@ int dfc_set_preview_mode(dfc_renderer* r, int preview_mode);
  * Aparapi kernel seeds its per-pixel generators from ThreadLocalRandom). */
 int dfc_set_seed(dfc_renderer* r, uint32_t seed);
 
+/* Per-stage device timing of later dfc_render calls (CUDA events around every
+ * launch; no reference counterpart: the reference times whole passes only,
+ * AbstractGPURenderer.java:281-291).  Read with dfc_read_stage_times. */
+int dfc_set_stage_timing(dfc_renderer* r, int on);
+
 /* setup(), AbstractGPURenderer.java:532: allocates the film and the wavefront
  * queues for the current image and clears the film. */
 int dfc_setup(dfc_renderer* r);
@@ -147,7 +152,8 @@ int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t capa
 int dfc_read_counters(dfc_renderer* r, int64_t* out4);
 
 /* Device time of the last dfc_render call, split by stage in milliseconds:
- * out[0] total, [1] ray generation, [2] traversal, [3] shading, [4] film. */
+ * out[0] total, [1] ray generation, [2] traversal, [3] shading, [4] film.
+ * Stages [1]-[4] are filled only while dfc_set_stage_timing is on. */
 int dfc_read_stage_times(dfc_renderer* r, float* out5);
 
 #ifdef __cplusplus
