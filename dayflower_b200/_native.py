@@ -44,6 +44,7 @@ SIGNATURES = [
     ("dfc_read_primary_hits", _c_int, [_c_p, _c_p, _c_p, _c_i64]),
     ("dfc_read_counters", _c_int, [_c_p, _c_p]),
     ("dfc_read_stage_times", _c_int, [_c_p, _c_p]),
+    ("dfc_trace_rays_noalloc", _c_int, [_c_p, _c_p, _c_p, _c_p, _c_i64]),
 ]
 
 

@@ -641,3 +641,106 @@ int dfc_read_stage_times(dfc_renderer* r, float* out5) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dfc_trace_rays_noalloc: closest-hit traversal of caller-supplied rays that
+// makes no device allocation.  It is for callers that must not have the
+// library allocate device memory on their behalf: a host that owns a fixed
+// device arena and hands out every byte itself, or an interactive loop that
+// cannot afford cudaMalloc/cudaFree, which may synchronise the whole device.
+// Rays, hits and the committed scene live in memory the caller or
+// dfc_scene_commit already owns; the traversal's own scratch (the ray list
+// k_trace walks, its ray count, its fetch cursor and its overflow flag) lives
+// in the static device array below instead of a cudaMalloc'd buffer.
+//
+// The scratch is one array per device per process.  Two calls on one device
+// that overlapped in time would race on it, so every call holds
+// g_noalloc_mu from its first launch until its stream has drained.
+
+constexpr int64_t kNoAllocMaxRays = int64_t(1) << 20;   // 1,048,576 rays per call
+constexpr int kNoAllocHeader = 64;                        // words: [0] ray count, [1] fetch cursor, [2] overflow flag
+constexpr int kNoAllocMaxDevices = 64;
+
+// 4 MiB + 256 B of device memory, set aside when the module loads.
+static __device__ __align__(256) unsigned g_noalloc_scratch[kNoAllocHeader + kNoAllocMaxRays];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// First kernel of every call: the fetch cursor and the overflow flag must be
+// zero when k_trace starts, and are set here in stream order, so nothing
+// depends on the load-time zero fill or on how an earlier call ended.
+__global__ void k_noalloc_prepare(unsigned* scratch, unsigned n) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) scratch[kNoAllocHeader + i] = i << 3;  // slot i, closest-hit ray
+  if (i == 0) { scratch[0] = n; scratch[1] = 0u; scratch[2] = 0u; }
+}
+
+// Once per device, with that device current: resolves the scratch address and
+// loads both kernels, so later calls do no module loading.
+int noalloc_setup(dfc_renderer* r, unsigned** out) {
+  if (r->device < 0 || r->device >= kNoAllocMaxDevices)
+    return fail(r, DFC_E_UNSUPPORTED, "dfc_trace_rays_noalloc supports device ordinals below 64");
+  if (!g_noalloc_ptr[r->device]) {
+    void* p = nullptr;
+    DFC_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch), "dfc_trace_rays_noalloc scratch address");
+    cudaFuncAttributes fa;
+    DFC_CK(cudaFuncGetAttributes(&fa, k_noalloc_prepare), "dfc_trace_rays_noalloc set-up");
+    DFC_CK(cudaFuncGetAttributes(&fa, k_trace), "dfc_trace_rays_noalloc set-up");
+    g_noalloc_ptr[r->device] = static_cast<unsigned*>(p);
+  }
+  *out = g_noalloc_ptr[r->device];
+  return DFC_OK;
+}
+
+bool device_pointer_on(const void* p, int device) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == device;
+}
+
+}  // namespace
+
+extern "C" int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, const float* d_directions, float* d_hits,
+                                      int64_t count) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (count < 0) return fail(r, DFC_E_INVALID_ARG, "count < 0");
+  if (count > kNoAllocMaxRays)
+    return fail(r, DFC_E_INVALID_ARG, "count " + std::to_string(count) + " exceeds the " + std::to_string(kNoAllocMaxRays) +
+                                          "-ray limit of dfc_trace_rays_noalloc's static scratch; split the batch");
+  if (!r->have_scene) return fail(r, DFC_E_STATE, "dfc_trace_rays_noalloc before setScene()");
+  DFC_CK(cudaSetDevice(r->device), "cudaSetDevice");
+  std::lock_guard<std::mutex> glk(g_noalloc_mu);
+  unsigned* scratch = nullptr;
+  if (int rc = noalloc_setup(r, &scratch)) return rc;
+  if (count == 0) return DFC_OK;
+  const void* ptrs[3] = {d_origins, d_directions, d_hits};
+  for (const void* p : ptrs) {
+    if (!p) return fail(r, DFC_E_INVALID_ARG, "ray or hit pointer == NULL");
+    if (reinterpret_cast<uintptr_t>(p) % 16u) return fail(r, DFC_E_INVALID_ARG, "ray and hit arrays must be 16-byte aligned");
+    if (!device_pointer_on(p, r->device))
+      return fail(r, DFC_E_INVALID_ARG, "ray and hit arrays must be device memory of the handle's device");
+  }
+  const unsigned n = (unsigned)count;
+  k_noalloc_prepare<<<(n + 255u) / 256u, 256, 0, r->stream>>>(scratch, n);
+  TraceArgs t{};
+  t.scene = r->view;
+  t.ray_list = scratch + kNoAllocHeader;
+  t.ray_count = scratch;
+  t.fetch = scratch + 1;
+  t.overflow = scratch + 2;
+  t.ray_o = reinterpret_cast<const float4*>(d_origins);
+  t.ray_d = reinterpret_cast<const float4*>(d_directions);
+  t.hits = reinterpret_cast<float4*>(d_hits);
+  t.paths = n;
+  k_trace<<<r->sm_count * 6, kTraceThreads, 0, r->stream>>>(t);
+  DFC_CK(cudaGetLastError(), "dfc_trace_rays_noalloc launch");
+  unsigned ov = 0;
+  DFC_CK(cudaMemcpyAsync(&ov, scratch + 2, 4, cudaMemcpyDeviceToHost, r->stream), "dfc_trace_rays_noalloc readback");
+  DFC_CK(cudaStreamSynchronize(r->stream), "dfc_trace_rays_noalloc");
+  if (ov) return fail(r, DFC_E_TIMEOUT, "traversal stack bound exceeded on " + std::to_string(ov) + " node visits");
+  return DFC_OK;
+}

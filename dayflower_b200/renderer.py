@@ -215,6 +215,14 @@ class GPURenderer:
         self._check(self._lib.dfc_read_counters(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return {"passes": int(out[0]), "paths": int(out[1]), "rays": int(out[2]), "launches": int(out[3])}
 
+    def traceRaysNoAlloc(self, d_origins: int, d_directions: int, d_hits: int, count: int):
+        """Closest hits of ``count`` rays held in device memory (addresses of
+        float4 arrays: origins, directions with tmax in w, hits out), with no
+        device allocation by the library; at most 1,048,576 rays per call."""
+        self._alive()
+        self._check(self._lib.dfc_trace_rays_noalloc(self._h, ctypes.c_void_p(d_origins), ctypes.c_void_p(d_directions),
+                                                     ctypes.c_void_p(d_hits), int(count)))
+
     def lastRenderMillis(self) -> float:
         return self.stageMillis()["total"]
 

@@ -156,6 +156,40 @@ int dfc_read_counters(dfc_renderer* r, int64_t* out4);
  * Stages [1]-[4] are filled only while dfc_set_stage_timing is on. */
 int dfc_read_stage_times(dfc_renderer* r, float* out5);
 
+/* Closest-hit traversal of `count` caller-supplied rays against the committed
+ * scene, with no device allocation.  No counterpart in the reference.
+ *
+ * For callers that must not have the library allocate device memory: a host
+ * that owns a fixed device arena and hands out every byte itself, or an
+ * interactive loop that cannot afford cudaMalloc/cudaFree, which may
+ * synchronise the whole device.  The traversal scratch (ray list, ray count,
+ * fetch cursor, overflow flag) is a static device array of 4 MiB + 256 B in
+ * this library, one per device per process.
+ *
+ * All three arrays are device memory of the handle's device, 16-byte aligned,
+ * `count` float4 each:
+ *   d_origins[i]    = (x, y, z, unused)
+ *   d_directions[i] = (dx, dy, dz, tmax)   hits need t in (0.0001, tmax)
+ *   d_hits[i]       = (t, primitive index as int32 bits or -1 on a miss,
+ *                      shape-specific int32 bits, t in object space)
+ * t is the ray parameter, the distance for a unit direction.  Nothing the
+ * caller passes must start at zero: the call zeroes the scratch's fetch cursor
+ * and overflow flag itself before it traverses.
+ *
+ * Limit: count <= 1048576 (DFC_E_INVALID_ARG beyond, with the limit in the
+ * message; split larger batches).  count == 0 does only the set-up.
+ * Set-up: the first call on each device resolves the scratch address with
+ * cudaGetSymbolAddress and loads the kernels; make that first call (count 0
+ * suffices) before any stream capture begins on that device.
+ * Concurrency: calls on one device that overlapped in time would race on the
+ * one scratch array, so the library runs them one after another under a
+ * process-wide lock.  The call uses the handle's stream and returns once the
+ * hits are written; make the rays visible to that stream first (synchronise
+ * the stream that produced them).  DFC_E_STATE before dfc_scene_commit,
+ * DFC_E_TIMEOUT if the traversal stack bound ran out. */
+int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, const float* d_directions, float* d_hits,
+                           int64_t count);
+
 #ifdef __cplusplus
 }
 #endif
