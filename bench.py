@@ -39,6 +39,17 @@ CONFIG = {"workload": "terrain_2.1M_tris+2000_spheres_perez_1920x1080_pt64spp_bo
           "l2": "inputs larger than L2 (scene + wavefront > 126 MB)"}
 
 
+# Algorithmic bytes of one traced ray in k_trace: ray-list entry (4 B), origin
+# and direction records (2 x 16 B), hit record (16 B).  BVH node and triangle
+# fetches are data-dependent and not counted.
+TRACE_RECORD_BYTES = 52
+# DRAM bytes (read + write) per traced ray of k_trace from an ncu capture of
+# one whole path-tracing pass of this workload at 1 spp; scaled to a launch by
+# its rays.
+TRACE_DRAM_BYTES_PER_RAY = None
+TRACE_TRAFFIC_SOURCE = None
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -125,7 +136,7 @@ def run_reference(args, rank):
     compiled = build_scene(args.cells)
     res = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(compiled, rows=8)
+        r = cpu_baseline(compiled, rows=24)
         if i >= args.warmup:
             res.append(r)
     v = statistics.median(x["value"] for x in res)
@@ -169,7 +180,10 @@ def main():
 
     for _ in range(args.warmup):
         step()
-    c0 = r.getCounters()
+    # Per-launch device events for the roofline of the traversal kernel; they
+    # stay on through the timed steps so k_trace is timed live.
+    r.setStageTiming(True)
+    step()
     clocks = ClockSampler(local)
     clocks.start()
     if world > 1:
@@ -178,11 +192,13 @@ def main():
     ms = []
     rays = 0
     launches = 0
+    trace_ms = 0.0
     for _ in range(args.steps):
         ms.append(step())
         c = r.getCounters()
         rays += c["rays"]
         launches += c["launches"]
+        trace_ms += r.stageMillis()["trace"]
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = sum(ms)
@@ -217,9 +233,10 @@ def main():
 
     if rank == 0:
         peak, peak_kind = peaks()
-        # Dominant stage: traversal; algorithmic bytes per traced ray = ray record in (32 B) + hit out (16 B).
-        rays_per_step = rays / args.steps
-        achieved = rays_per_step * 48 / (total_ms / args.steps / 1000.0) / 1e9
+        trace_launches = args.steps * args.spp * (CONFIG["max_bounce"] + 4)
+        rays_per_launch = rays / trace_launches
+        launch_ms = trace_ms / trace_launches
+        achieved = rays_per_launch * TRACE_RECORD_BYTES / (launch_ms / 1000.0) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -227,12 +244,15 @@ def main():
             "rays_per_s": world * rays / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "k_trace (whole pass, ray+hit records only)", "peak_kind": peak_kind},
+                         "traffic": None if TRACE_DRAM_BYTES_PER_RAY is None else rays_per_launch * TRACE_DRAM_BYTES_PER_RAY, "peak_kind": peak_kind,
+                         "kernel": "k_trace", "launches": trace_launches, "launch_ms": launch_ms, "rays_per_launch": rays_per_launch,
+                         "algorithmic_bytes_per_ray": TRACE_RECORD_BYTES, "trace_share": trace_ms / total_ms,
+                         "traffic_source": TRACE_TRAFFIC_SOURCE},
             "clocks": clk,
             "e2e": e2e,
         }
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(compiled)
+            line["cpu_baseline"] = cpu_baseline(compiled, rows=144)
         print(json.dumps(line), flush=True)
     r.dispose()
     if world > 1:

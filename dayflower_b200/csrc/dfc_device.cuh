@@ -182,6 +182,58 @@ DFC_D float tri_t(V3 a, V3 b, V3 c, V3 o, V3 d, float tmin, float tmax) {
   return t;
 }
 
+// The ray-only part of tri_t, computed once per ray and space: the dominant
+// axis kz and the shear (sx, sy, sz).
+struct Shear { int kz; float sx, sy, sz; };
+DFC_D Shear make_shear(V3 d) {
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  Shear s;
+  s.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  const float dX = s.kz == 0 ? d.y : (s.kz == 1 ? d.z : d.x);
+  const float dY = s.kz == 0 ? d.z : (s.kz == 1 ? d.x : d.y);
+  const float dZ = s.kz == 0 ? d.x : (s.kz == 1 ? d.y : d.z);
+  s.sx = -dX / dZ; s.sy = -dY / dZ; s.sz = 1.0f / dZ;
+  return s;
+}
+
+// tri_t with the shear precomputed; the same arithmetic step for step, so the
+// result is bit-identical.  Vertex components are permuted by selects, not
+// branches, so lanes with different dominant axes do not diverge.
+DFC_D float tri_t_sheared(float4 A, float4 B, float4 C, V3 o, const Shear& sh, float tmin, float tmax) {
+  const V3 p0 = {A.x - o.x, A.y - o.y, A.z - o.z}, p1 = {B.x - o.x, B.y - o.y, B.z - o.z}, p2 = {C.x - o.x, C.y - o.y, C.z - o.z};
+  const bool k0 = sh.kz == 0, k1 = sh.kz == 1;
+  float x0 = k0 ? p0.y : (k1 ? p0.z : p0.x), y0 = k0 ? p0.z : (k1 ? p0.x : p0.y), z0 = k0 ? p0.x : (k1 ? p0.y : p0.z);
+  float x1 = k0 ? p1.y : (k1 ? p1.z : p1.x), y1 = k0 ? p1.z : (k1 ? p1.x : p1.y), z1 = k0 ? p1.x : (k1 ? p1.y : p1.z);
+  float x2 = k0 ? p2.y : (k1 ? p2.z : p2.x), y2 = k0 ? p2.z : (k1 ? p2.x : p2.y), z2 = k0 ? p2.x : (k1 ? p2.y : p2.z);
+  x0 = x0 + sh.sx * z0; y0 = y0 + sh.sy * z0;
+  x1 = x1 + sh.sx * z1; y1 = y1 + sh.sy * z1;
+  x2 = x2 + sh.sx * z2; y2 = y2 + sh.sy * z2;
+  float e0 = x1 * y2 - y1 * x2;
+  float e1 = x2 * y0 - y2 * x0;
+  float e2 = x0 * y1 - y0 * x1;
+  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) tri_edges_fp64(x0, y0, x1, y1, x2, y2, &e0, &e1, &e2);
+  if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
+  const float det = e0 + e1 + e2;
+  if (det == 0.0f) return -1.0f;
+  z0 *= sh.sz; z1 *= sh.sz; z2 *= sh.sz;
+  const float ts = e0 * z0 + e1 * z1 + e2 * z2;
+  if (det < 0.0f && (ts >= tmin || ts < tmax * det)) return -1.0f;
+  if (det > 0.0f && (ts <= tmin || ts > tmax * det)) return -1.0f;
+  const float inv = 1.0f / det;
+  const float t = ts * inv;
+  const float mz = fmaxf(fabsf(z0), fmaxf(fabsf(z1), fabsf(z2)));
+  const float mx = fmaxf(fabsf(x0), fmaxf(fabsf(x1), fabsf(x2)));
+  const float my = fmaxf(fabsf(y0), fmaxf(fabsf(y1), fabsf(y2)));
+  const float dz = gamma_n(3) * mz;
+  const float ddx = gamma_n(5) * (mx + mz);
+  const float ddy = gamma_n(5) * (my + mz);
+  const float de = 2.0f * (gamma_n(2) * mx * my + ddy * mx + ddx * my);
+  const float me = fmaxf(fabsf(e0), fmaxf(fabsf(e1), fabsf(e2)));
+  const float dt = 3.0f * (gamma_n(3) * me * mz + de * mz + dz * me) * fabsf(inv);
+  if (t <= dt) return -1.0f;
+  return t;
+}
+
 // utility/EFloat.java: running float interval for the sphere test.
 struct EF { float v, lo, hi; };
 DFC_D EF ef(float v) { return {v, v, v}; }

@@ -231,34 +231,44 @@ constexpr unsigned kAlive = kFlagAlive, kPendShadow = kFlagPendShadow, kPendMis 
 // The same walk as trace_ray, held in registers across iterations so that a
 // lane whose ray is done takes a new ray from the queue instead of idling
 // until the slowest lane of its warp finishes (ray costs are heavy-tailed).
+// Each round has a node phase and a leaf phase (the while-while loop of Aila
+// and Laine, "Understanding the efficiency of ray traversal on GPUs", HPG
+// 2009): lanes walk interior nodes until every lane of the warp holds a leaf
+// (a lane that already holds one keeps walking nodes speculatively), then all
+// lanes test their leaves together, one item per iteration, so node and leaf
+// code do not interleave within a warp.
 struct Trav {
-  V3 o, d, winv;
-  float best, bbest;
-  ObjRay br;
+  V3 o, d;          // world ray
+  V3 co, cd, cinv;  // ray in the current space (world, or a mesh's object space)
+  float cbest;      // closest hit so far in the current space
+  float wbest;      // world closest hit, saved while in a bottom level
+  float s;          // length of the object-space direction before normalisation
+  Shear sh;         // triangle shear of cd
   int sp, bprim;
   bool any, found, in_blas;
   Hit h;
 };
 
 DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack) {
-  T.o = o; T.d = d; T.best = tmax; T.bbest = 0.0f; T.any = any; T.found = false; T.in_blas = false;
-  T.sp = 0; T.bprim = -1; T.br.s = 1.0f;
+  T.o = o; T.d = d; T.co = o; T.cd = d; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
+  T.any = any; T.found = false; T.in_blas = false;
+  T.sp = 0; T.bprim = -1;
   T.h.t = tmax; T.h.prim = -1; T.h.aux = -1; T.h.t_obj = 0.0f;
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
     ObjRay r = obj_ray(pr, o, d);
-    const float to = prim_t(S, pr, r, T.best * r.s);
+    const float to = prim_t(S, pr, r, T.cbest * r.s);
     if (to > kTMin) {
       const float tw = to / r.s;
-      if (tw < T.best) {
-        T.best = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+      if (tw < T.cbest) {
+        T.cbest = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
         if (any) return;
       }
     }
   }
-  T.winv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  T.cinv = V3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
   if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
 }
 
@@ -272,16 +282,20 @@ constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0x
 #define DFC_CSWAP(ta, ea, tb, eb) \
   if (tb < ta) { const float tt_ = ta; ta = tb; tb = tt_; const unsigned ee_ = ea; ea = eb; eb = ee_; }
 
-// Processes one stack entry; returns true once the ray is finished.
-DFC_D bool trav_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow) {
-  if (T.sp == 0) return true;
-  const unsigned e = (unsigned)stack[(--T.sp) * kTraceBlock];
-  if ((e & kTagMask) == 0u) {
-    // interior node: test the four children, push the hit ones far-to-near
+// One step of the node phase.  Pops the top entry: an interior node pushes its
+// hit children far-to-near, a leaf is taken as this lane's pending leaf, and
+// the bottom-level markers switch the ray's space.  A lane that already holds
+// a leaf only walks interior nodes (the leaf must be tested in the space it
+// came from); it returns true when the top entry is anything else.
+DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow, int& lf_first, int& lf_cnt) {
+  const unsigned e = (unsigned)stack[(T.sp - 1) * kTraceBlock];
+  const unsigned tag = e & kTagMask;
+  if (tag != 0u && lf_cnt > 0) return true;
+  --T.sp;
+  if (tag == 0u) {
     float tn[4];
-    const unsigned mask = T.in_blas ? node_hits(S.nodes, (int)e, T.br.o, T.br.inv, 0.0f, T.bbest, tn)
-                                    : node_hits(S.nodes, (int)e, T.o, T.winv, 0.0f, T.best, tn);
-    if (!mask) return T.sp == 0;
+    const unsigned mask = node_hits(S.nodes, (int)e, T.co, T.cinv, 0.0f, T.cbest, tn);
+    if (!mask) return false;
     const int4* cp = reinterpret_cast<const int4*>(S.nodes + e) + 6;
     const int4 ch = __ldg(cp), cn = __ldg(cp + 1);
     const float inf = __int_as_float(0x7f800000);
@@ -294,7 +308,7 @@ DFC_D bool trav_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     DFC_CSWAP(t1, e1, t3, e3);
     DFC_CSWAP(t1, e1, t2, e2);
     const int n = __popc(mask);
-    if (T.sp + n > kStack) { atomicAdd(overflow, 1u); return T.sp == 0; }
+    if (T.sp + n > kStack) { atomicAdd(overflow, 1u); return false; }
     // ascending t0 <= t1 <= t2 <= t3 (misses last as +inf): push the n hits far first
     if (n > 3) stack[(T.sp++) * kTraceBlock] = (int)e3;
     if (n > 2) stack[(T.sp++) * kTraceBlock] = (int)e2;
@@ -302,72 +316,93 @@ DFC_D bool trav_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     stack[(T.sp++) * kTraceBlock] = (int)e0;
     return false;
   }
-  if ((e & kTagMask) == kTagLeaf) {
-    const int first = (int)((e & ~kTagMask) >> 2), cnt = (int)(e & 3u) + 1;
-    if (T.in_blas) {
-      for (int j = 0; j < cnt; ++j) {
-        const float4* tp = reinterpret_cast<const float4*>(S.tri_pos) + 3 * (first + j);
-        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
-        const float t = tri_t(V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, V3{cc.x, cc.y, cc.z}, T.br.o, T.br.d, kTMin, T.bbest);
-        if (t > kTMin && t < T.bbest) {
-          T.bbest = t; T.found = true;
-          T.h.prim = T.bprim; T.h.aux = __float_as_int(a.w); T.h.t_obj = t;
-          if (T.any) { T.best = t / T.br.s; T.in_blas = false; T.sp = 0; return true; }
-        }
-      }
-    } else {
-      for (int j = 0; j < cnt; ++j) {
-        const int pi = S.tlas_items[first + j];
-        const float4 bs = __ldg(reinterpret_cast<const float4*>(S.tlas_bound) + first + j);
-        if (bs.w < 0.0f) {  // a mesh: enter its bottom level next
-          if (T.sp < kStack) stack[(T.sp++) * kTraceBlock] = (int)(kTagMesh | (unsigned)pi);
-          else atomicAdd(overflow, 1u);
-          continue;
-        }
-        if (!sphere_may_hit(bs, T.o, T.d, T.best)) continue;
-        const DPrim& pr = S.prims[pi];
-        ObjRay r = obj_ray(pr, T.o, T.d);
-        const float to = prim_t(S, pr, r, T.best * r.s);
-        if (to > kTMin) {
-          const float tw = to / r.s;
-          if (tw < T.best) {
-            T.best = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
-            if (T.any) { T.sp = 0; return true; }
-          }
-        }
-      }
-    }
-    return T.sp == 0;
+  if (tag == kTagLeaf) {
+    lf_first = (int)((e & ~kTagMask) >> 2);
+    lf_cnt = (int)(e & 3u) + 1;
+    return false;
   }
   if (e == kEndBlas) {
     T.in_blas = false;
-    T.best = fminf(T.best, T.bbest / T.br.s);
-    return T.sp == 0;
+    T.cbest = fminf(T.wbest, T.cbest / T.s);
+    T.co = T.o; T.cd = T.d;
+    T.cinv = V3{1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z};
+    T.s = 1.0f;
+    return false;
   }
   // enter a mesh's bottom level
+  if (T.sp + 2 > kStack) { atomicAdd(overflow, 1u); return false; }
   T.bprim = (int)(e & ~kTagMask);
   const DPrim& pm = S.prims[T.bprim];
-  T.br = obj_ray(pm, T.o, T.d);
-  T.bbest = T.best * T.br.s;
-  if (T.sp + 2 > kStack) { atomicAdd(overflow, 1u); return T.sp == 0; }
+  const ObjRay r = obj_ray(pm, T.o, T.d);
+  T.co = r.o; T.cd = r.d; T.cinv = r.inv; T.s = r.s;
+  T.wbest = T.cbest;
+  T.cbest = T.wbest * r.s;
+  T.sh = make_shear(r.d);
   T.in_blas = true;
   stack[(T.sp++) * kTraceBlock] = (int)kEndBlas;
   stack[(T.sp++) * kTraceBlock] = pm.data;
   return false;
 }
 
+// One item of this lane's pending leaf: a triangle of the current bottom
+// level, or a top-level item (a mesh is queued for its bottom level).
+DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow, int& lf_first, int& lf_cnt) {
+  const int i = lf_first++;
+  --lf_cnt;
+  if (T.in_blas) {
+    const float4* tp = reinterpret_cast<const float4*>(S.tri_pos) + 3 * i;
+    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    const float t = tri_t_sheared(a, b, c, T.co, T.sh, kTMin, T.cbest);
+    if (t > kTMin && t < T.cbest) {
+      T.cbest = t; T.found = true;
+      T.h.prim = T.bprim; T.h.aux = __float_as_int(a.w); T.h.t_obj = t;
+      if (T.any) { T.cbest = t / T.s; T.in_blas = false; T.sp = 0; lf_cnt = 0; }
+    }
+    return;
+  }
+  const int pi = S.tlas_items[i];
+  const float4 bs = __ldg(reinterpret_cast<const float4*>(S.tlas_bound) + i);
+  if (bs.w < 0.0f) {  // a mesh: enter its bottom level in a later node phase
+    if (T.sp < kStack) stack[(T.sp++) * kTraceBlock] = (int)(kTagMesh | (unsigned)pi);
+    else atomicAdd(overflow, 1u);
+    return;
+  }
+  if (!sphere_may_hit(bs, T.o, T.d, T.cbest)) return;
+  const DPrim& pr = S.prims[pi];
+  ObjRay r = obj_ray(pr, T.o, T.d);
+  const float to = prim_t(S, pr, r, T.cbest * r.s);
+  if (to > kTMin) {
+    const float tw = to / r.s;
+    if (tw < T.cbest) {
+      T.cbest = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+      if (T.any) { T.sp = 0; lf_cnt = 0; }
+    }
+  }
+}
+
 constexpr unsigned kNoRay = 0xffffffffu;
 constexpr int kRefill = 8;        // refill a warp's idle lanes once this many are idle
-constexpr int kStepsPerRefill = 24;
+#ifndef DFC_NODE_STEPS
+#define DFC_NODE_STEPS 16
+#endif
+#ifndef DFC_SPECULATE
+#define DFC_SPECULATE 1
+#endif
+constexpr int kNodeSteps = DFC_NODE_STEPS;  // bound of one node phase (the warp then tests its leaves and refills)
+constexpr bool kSpeculate = DFC_SPECULATE != 0;  // lanes holding a leaf keep walking interior nodes
 
+// Every vote below is taken by all 32 lanes at the same point of the loop
+// (lanes without work only skip the work), so full masks are exact.
 __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
   __shared__ int stack_smem[kStack * kTraceBlock];
   int* stack = stack_smem + threadIdx.x;
   const unsigned n = *a.ray_count;
   const unsigned lane = threadIdx.x & 31u;
   Trav T;
+  T.sp = 0;
   unsigned cur = kNoRay;
   size_t slot = 0;
+  int lf_first = 0, lf_cnt = 0;
   bool pool_empty = false;  // warp-uniform
   while (true) {
     const bool idle = cur == kNoRay;
@@ -387,17 +422,26 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
           slot = (size_t)type * a.paths + p;
           const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
           trav_init(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
+          lf_cnt = 0;
         }
       }
     }
-    if (pool_empty && __all_sync(0xffffffffu, cur == kNoRay)) break;
-    if (cur != kNoRay) {
-      bool done = false;
-      for (int it = 0; it < kStepsPerRefill && !done; ++it) done = trav_step(a.scene, T, stack, a.overflow);
-      if (done) {
-        a.hits[slot] = make_float4(T.best, __int_as_float(T.found ? T.h.prim : -1), __int_as_float(T.h.aux), T.h.t_obj);
-        cur = kNoRay;
-      }
+    const bool act = cur != kNoRay;
+    if (pool_empty && !__any_sync(0xffffffffu, act)) break;
+    // node phase
+    bool blocked = false;
+    for (int k = 0; k < kNodeSteps; ++k) {
+      const bool searching = act && T.sp > 0 && lf_cnt == 0;
+      if (!__any_sync(0xffffffffu, searching)) break;
+      if (kSpeculate ? (act && T.sp > 0 && !blocked) : searching) blocked = node_step(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
+    }
+    // leaf phase
+    while (__any_sync(0xffffffffu, lf_cnt > 0)) {
+      if (lf_cnt > 0) leaf_step(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
+    }
+    if (act && T.sp == 0) {
+      a.hits[slot] = make_float4(T.cbest, __int_as_float(T.found ? T.h.prim : -1), __int_as_float(T.h.aux), T.h.t_obj);
+      cur = kNoRay;
     }
   }
 }
