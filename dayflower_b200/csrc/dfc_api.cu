@@ -77,6 +77,7 @@ struct dfc_renderer {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_marks;  // (stage, index of the start event)
   int sm_count = 148;
+  int trace_blocks = 6, ao_blocks = 5;  // resident blocks per SM of k_trace / k_trace_ao (persistent grids)
 };
 
 namespace {
@@ -257,7 +258,7 @@ int enqueue_pass(dfc_renderer* r) {
   k_raygen<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(g);
   stage_end(r, ev);
   r->launches++;
-  const int trace_grid = r->sm_count * 6;
+  const int trace_grid = r->sm_count * r->trace_blocks;
   const int shade_grid = r->sm_count * 8;
   if (algo == DFC_PATH_TRACING) {
     const size_t bins_bytes = (size_t)steps * 2 * kSortBins * sizeof(unsigned);
@@ -304,7 +305,7 @@ int enqueue_pass(dfc_renderer* r) {
       o.ao_d = r->d_ao_d.as<float4>();
       o.ao_value = r->d_ao_v.as<float>();
       o.overflow = r->d_overflow.as<unsigned>();
-      k_trace_ao<<<trace_grid, kTraceThreads, 0, r->stream>>>(o);
+      k_trace_ao<<<r->sm_count * r->ao_blocks, kTraceThreads, 0, r->stream>>>(o);
       k_ao_resolve<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(a, r->d_ao_v.as<float>(), r->ao_samples);
       r->launches += 2;
     }
@@ -333,6 +334,11 @@ int dfc_create(int device, dfc_renderer** out) {
   dfc_renderer* r = new dfc_renderer();
   r->device = device;
   cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, device);
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace, kTraceThreads, 0) == cudaSuccess && nb > 0) r->trace_blocks = nb;
+  nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_ao, kTraceThreads, 0) == cudaSuccess && nb > 0) r->ao_blocks = nb;
+  cudaGetLastError();
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
     delete r;
@@ -736,7 +742,7 @@ extern "C" int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, c
   t.ray_d = reinterpret_cast<const float4*>(d_directions);
   t.hits = reinterpret_cast<float4*>(d_hits);
   t.paths = n;
-  k_trace<<<r->sm_count * 6, kTraceThreads, 0, r->stream>>>(t);
+  k_trace<<<r->sm_count * r->trace_blocks, kTraceThreads, 0, r->stream>>>(t);
   DFC_CK(cudaGetLastError(), "dfc_trace_rays_noalloc launch");
   unsigned ov = 0;
   DFC_CK(cudaMemcpyAsync(&ov, scratch + 2, 4, cudaMemcpyDeviceToHost, r->stream), "dfc_trace_rays_noalloc readback");

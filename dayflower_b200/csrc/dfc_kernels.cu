@@ -239,21 +239,22 @@ constexpr unsigned kAlive = kFlagAlive, kPendShadow = kFlagPendShadow, kPendMis 
 // code do not interleave within a warp.
 struct Trav {
   V3 o, d;          // world ray
-  V3 co, cd, cinv;  // ray in the current space (world, or a mesh's object space)
+  V3 co, cinv;      // origin and inverse direction in the current space (world, or a mesh's object space)
   float cbest;      // closest hit so far in the current space
   float wbest;      // world closest hit, saved while in a bottom level
   float s;          // length of the object-space direction before normalisation
   Shear sh;         // triangle shear of cd
   int sp, bprim;
-  bool any, found, in_blas;
-  Hit h;
+  bool any, in_blas;
+  int prim, aux;    // closest hit so far (prim -1: none)
+  float t_obj;
 };
 
 DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack) {
-  T.o = o; T.d = d; T.co = o; T.cd = d; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
-  T.any = any; T.found = false; T.in_blas = false;
+  T.o = o; T.d = d; T.co = o; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
+  T.any = any; T.in_blas = false;
   T.sp = 0; T.bprim = -1;
-  T.h.t = tmax; T.h.prim = -1; T.h.aux = -1; T.h.t_obj = 0.0f;
+  T.prim = -1; T.aux = -1; T.t_obj = 0.0f;
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
@@ -263,7 +264,7 @@ DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool a
     if (to > kTMin) {
       const float tw = to / r.s;
       if (tw < T.cbest) {
-        T.cbest = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+        T.cbest = tw; T.prim = pi; T.aux = pr.data; T.t_obj = to;
         if (any) return;
       }
     }
@@ -324,7 +325,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   if (e == kEndBlas) {
     T.in_blas = false;
     T.cbest = fminf(T.wbest, T.cbest / T.s);
-    T.co = T.o; T.cd = T.d;
+    T.co = T.o;
     T.cinv = V3{1.0f / T.d.x, 1.0f / T.d.y, 1.0f / T.d.z};
     T.s = 1.0f;
     return false;
@@ -334,7 +335,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   T.bprim = (int)(e & ~kTagMask);
   const DPrim& pm = S.prims[T.bprim];
   const ObjRay r = obj_ray(pm, T.o, T.d);
-  T.co = r.o; T.cd = r.d; T.cinv = r.inv; T.s = r.s;
+  T.co = r.o; T.cinv = r.inv; T.s = r.s;
   T.wbest = T.cbest;
   T.cbest = T.wbest * r.s;
   T.sh = make_shear(r.d);
@@ -354,8 +355,8 @@ DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
     const float t = tri_t_sheared(a, b, c, T.co, T.sh, kTMin, T.cbest);
     if (t > kTMin && t < T.cbest) {
-      T.cbest = t; T.found = true;
-      T.h.prim = T.bprim; T.h.aux = __float_as_int(a.w); T.h.t_obj = t;
+      T.cbest = t;
+      T.prim = T.bprim; T.aux = __float_as_int(a.w); T.t_obj = t;
       if (T.any) { T.cbest = t / T.s; T.in_blas = false; T.sp = 0; lf_cnt = 0; }
     }
     return;
@@ -374,7 +375,7 @@ DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   if (to > kTMin) {
     const float tw = to / r.s;
     if (tw < T.cbest) {
-      T.cbest = tw; T.found = true; T.h.prim = pi; T.h.aux = pr.data; T.h.t_obj = to;
+      T.cbest = tw; T.prim = pi; T.aux = pr.data; T.t_obj = to;
       if (T.any) { T.sp = 0; lf_cnt = 0; }
     }
   }
@@ -393,7 +394,10 @@ constexpr bool kSpeculate = DFC_SPECULATE != 0;  // lanes holding a leaf keep wa
 
 // Every vote below is taken by all 32 lanes at the same point of the loop
 // (lanes without work only skip the work), so full masks are exact.
-__global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
+#ifndef DFC_TRACE_MIN_BLOCKS
+#define DFC_TRACE_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
   __shared__ int stack_smem[kStack * kTraceBlock];
   int* stack = stack_smem + threadIdx.x;
   const unsigned n = *a.ray_count;
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
   Trav T;
   T.sp = 0;
   unsigned cur = kNoRay;
-  size_t slot = 0;
+  unsigned slot = 0;
   int lf_first = 0, lf_cnt = 0;
   bool pool_empty = false;  // warp-uniform
   while (true) {
@@ -419,7 +423,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
           cur = i;
           const unsigned ref = a.ray_list[i];
           const unsigned p = ref >> 3, type = ref & 3u;
-          slot = (size_t)type * a.paths + p;
+          slot = type * a.paths + p;
           const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
           trav_init(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
           lf_cnt = 0;
@@ -440,7 +444,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(TraceArgs a) {
       if (lf_cnt > 0) leaf_step(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
     }
     if (act && T.sp == 0) {
-      a.hits[slot] = make_float4(T.cbest, __int_as_float(T.found ? T.h.prim : -1), __int_as_float(T.h.aux), T.h.t_obj);
+      a.hits[slot] = make_float4(T.cbest, __int_as_float(T.prim), __int_as_float(T.aux), T.t_obj);
       cur = kNoRay;
     }
   }
