@@ -11,6 +11,9 @@
 //   shape3FTriangleMesh3FArray threaded BVH stream (CompiledShape3FCache.java:2652)
 #include "dfc_ingest.h"
 
+#include <algorithm>
+#include <thread>
+
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -25,6 +28,18 @@ namespace {
 enum { kMatDisneyId = 4, kMatGlassId = 7, kMatMatteId = 11, kMatMetalId = 12, kMatMirrorId = 13, kMatPlasticId = 14 };
 enum { kTexConstantId = 4, kModNoOpId = 2 };
 enum { kBVAabbId = 1, kBVSphereId = 2, kBVInfiniteId = 3 };
+
+// Runs f(begin, end) over [0, n) in contiguous chunks on the host's threads.
+template <typename F>
+void parallel_for(size_t n, F&& f) {
+  const unsigned hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+  const size_t parts = n < (1u << 16) ? 1 : hw;
+  if (parts == 1) { f((size_t)0, n); return; }
+  std::vector<std::thread> ws;
+  for (size_t p = 1; p < parts; ++p) ws.emplace_back([&, p] { f(n * p / parts, n * (p + 1) / parts); });
+  f((size_t)0, n / parts);
+  for (auto& w : ws) w.join();
+}
 
 struct Fail {
   int code;
@@ -364,10 +379,8 @@ struct Decoder {
     if (X.size() < (size_t)np * 32) throw Fail{DFC_E_INVALID_ARG, "primitiveMatrix44FArray is shorter than 32 floats per primitive"};
     if (C.size() < 19) throw Fail{DFC_E_INVALID_ARG, "cameraArray needs 19 floats"};
     std::memcpy(hs.camera, C.data(), sizeof hs.camera);
-    hs.tri_attr = T;
     hs.rects = R;
     hs.perez = F("lightPerezLightArray");
-    if (hs.tri_attr.empty()) hs.tri_attr.assign(24, 0.0f);
     if (hs.rects.empty()) hs.rects.assign(16, 0.0f);
     if (hs.perez.empty()) hs.perez.assign(64, 0.0f);
     lights();
@@ -413,26 +426,33 @@ struct Decoder {
           if (it == blas_by_offset.end()) {
             std::vector<int> offs;
             mesh_triangles(soff, offs);
-            std::vector<Box> boxes(offs.size());
-            for (size_t k = 0; k < offs.size(); ++k) {
-              int to = offs[k];
+            for (int to : offs)
               if (to < 0 || to % 24 != 0 || (size_t)to + 24 > T.size()) throw Fail{DFC_E_INVALID_ARG, "mesh triangle offset out of range"};
-              const float* t = T.data() + to;
-              boxes[k].grow_point(t); boxes[k].grow_point(t + 3); boxes[k].grow_point(t + 6);
-            }
             if (offs.empty()) throw Fail{DFC_E_INVALID_ARG, "empty triangle mesh"};
+            std::vector<Box> boxes(offs.size());
+            parallel_for(offs.size(), [&](size_t a, size_t b) {
+              for (size_t k = a; k < b; ++k) {
+                const float* t = T.data() + offs[k];
+                boxes[k].grow_point(t); boxes[k].grow_point(t + 3); boxes[k].grow_point(t + 6);
+              }
+            });
             std::vector<int> order;
             int root = build_bvh4(boxes, 4, hs.nodes, order);
             const int first = (int)(hs.tri_pos.size() / 3);
-            for (int k : order) {
-              const float* t = T.data() + offs[k];
-              float idx;
-              int ti = offs[k] / 24;
-              std::memcpy(&idx, &ti, 4);
-              hs.tri_pos.push_back(F4{t[0], t[1], t[2], idx});
-              hs.tri_pos.push_back(F4{t[3], t[4], t[5], 0.0f});
-              hs.tri_pos.push_back(F4{t[6], t[7], t[8], 0.0f});
-            }
+            hs.tri_pos.resize(hs.tri_pos.size() + 3 * order.size());
+            F4* tp = hs.tri_pos.data() + (size_t)first * 3;
+            parallel_for(order.size(), [&](size_t a, size_t b) {
+              for (size_t j = a; j < b; ++j) {
+                const int off = offs[order[j]];
+                const float* t = T.data() + off;
+                float idx;
+                int ti = off / 24;
+                std::memcpy(&idx, &ti, 4);
+                tp[3 * j] = F4{t[0], t[1], t[2], idx};
+                tp[3 * j + 1] = F4{t[3], t[4], t[5], 0.0f};
+                tp[3 * j + 2] = F4{t[6], t[7], t[8], 0.0f};
+              }
+            });
             // re-base the leaf ranges of this hierarchy onto the global triangle array
             for (size_t n = (size_t)root; n < hs.nodes.size(); ++n) {
               int* ch = hs.nodes[n].child;
@@ -504,12 +524,16 @@ struct Decoder {
 
 }  // namespace
 
-int ingest_scene(const Staged& st, int layout, HostScene* out, std::string* err) {
+int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err) {
   try {
     if (layout != 1 && layout != 2) throw Fail{DFC_E_INVALID_ARG, "layout_version must be 1 or 2"};
     HostScene hs;
     Decoder d(st, layout, hs);
     d.run();
+    // the triangle records go to the device as they are: take them over
+    auto tri = st.f32.find("shape3FTriangle3FArray");
+    if (tri != st.f32.end()) hs.tri_attr = std::move(tri->second);
+    if (hs.tri_attr.empty()) hs.tri_attr.assign(24, 0.0f);
     *out = std::move(hs);
     return DFC_OK;
   } catch (const Fail& f) {

@@ -34,7 +34,8 @@ struct HostScene {
   int64_t triangles = 0;
 };
 
-// Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.
-int ingest_scene(const Staged& st, int layout, HostScene* out, std::string* err);
+// Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.  On
+// success the triangle array is moved out of `st` into out->tri_attr.
+int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err);
 
 }  // namespace dfc
