@@ -63,6 +63,26 @@ def parse():
     return ap.parse_args()
 
 
+def reduce_over_ranks(x, world, device, op="max"):
+    """Max (or sum) of a per-rank scalar over all ranks; the identity at N=1.
+    Every rank calls it at the same point with the same op."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, seconds_per_rank, world, device):
+    """Whole-job throughput of N independent replicas: the units all ranks
+    processed over the slowest rank's time."""
+    total_units = reduce_over_ranks(units_per_rank, world, device, "sum")
+    slowest = reduce_over_ranks(seconds_per_rank, world, device, "max")
+    return total_units / slowest, slowest
+
+
 def build_scene(cells):
     from dayflower_b200.scene import generators as G
     from dayflower_b200.scene.compiler import compile_scene
@@ -201,14 +221,12 @@ def main():
         trace_ms += r.stageMillis()["trace"]
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = sum(ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
     paths_per_step = W * H * args.spp
-    value = world * paths_per_step * args.steps / (total_ms / 1000.0)
+    value, slowest_s = replica_throughput(paths_per_step * args.steps, sum(ms) / 1000.0, world, "cuda")
+    total_ms = slowest_s * 1000.0
+    rays_all = reduce_over_ranks(rays, world, "cuda", "sum")
+    if world > 1:
+        dist.barrier()
 
     # end to end through the public API from host arrays: every step uploads
     # the compiled scene (setScene builds the acceleration structure), sets up
@@ -236,12 +254,9 @@ def main():
         for _ in range(e_steps):
             img = e2e_step()
         dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        e2e_value, _ = replica_throughput(paths_per_step * e_steps, dt, world, "cuda")
         q.dispose()
-        e2e = {"value": world * paths_per_step * e_steps / dt, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(img.nbytes), "steps": e_steps,
                "note": "per step: setScene from host arrays (upload + acceleration build) + setup + render(%d) + RGBA8 read-back" % args.spp}
 
@@ -255,7 +270,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp),
-            "rays_per_s": world * rays / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
+            "rays_per_s": rays_all / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None if TRACE_DRAM_BYTES_PER_RAY is None else rays_per_launch * TRACE_DRAM_BYTES_PER_RAY, "peak_kind": peak_kind,
