@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "_lib")
 ROOT = os.path.dirname(HERE)
 
 CUDA_SOURCES = ["dfc_api.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp"]
-CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h"]
+CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

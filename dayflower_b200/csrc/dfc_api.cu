@@ -60,6 +60,7 @@ struct dfc_renderer {
   bool have_scene = false;
   HostScene host;
   DevBuf d_prims, d_mats, d_lights, d_nodes, d_tlas_items, d_tlas_bound, d_unbounded, d_tri_pos, d_tri_attr, d_rects, d_perez, d_camera;
+  DevBuf d_shapes;
   SceneView view{};
   // film and wavefront
   bool set_up = false;
@@ -215,6 +216,11 @@ ShadeArgs shade_args(dfc_renderer* r, int step) {
   return a;
 }
 
+// The traversal kernel for the committed scene: the one with the disk ... torus
+// tests only when the scene has such primitives.
+using TraceKernel = void (*)(TraceArgs);
+TraceKernel trace_kernel(const dfc_renderer* r) { return r->host.record_shapes ? k_trace_records : k_trace; }
+
 TraceArgs trace_args(dfc_renderer* r, int step) {
   TraceArgs t{};
   t.scene = r->view;
@@ -266,7 +272,7 @@ int enqueue_pass(dfc_renderer* r) {
     DFC_CK(cudaMemsetAsync(r->d_sort_bins.p, 0, bins_bytes, r->stream), "sort");
     for (int s = 0; s < steps; ++s) {
       ev = stage_begin(r, 2);
-      k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, s));
+      trace_kernel(r)<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, s));
       stage_end(r, ev);
       ShadeArgs a = shade_args(r, s);
       a.last_step = s == steps - 1;
@@ -284,12 +290,12 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
       a.work_list = so.sorted;
-      k_shade_path<<<shade_grid, 256, 0, r->stream>>>(a);
+      (r->host.record_shapes ? k_shade_path_records : k_shade_path)<<<shade_grid, 256, 0, r->stream>>>(a);
       stage_end(r, ev);
       r->launches += 4;
     }
   } else {
-    k_trace<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, 0));
+    trace_kernel(r)<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, 0));
     ShadeArgs a = shade_args(r, 0);
     const int kind = algo == DFC_AMBIENT_OCCLUSION ? DFC_ALGO_AO : (algo == DFC_DEPTH_CAMERA ? DFC_ALGO_DEPTH : DFC_ALGO_RAY_CASTING);
     k_shade_primary<<<shade_grid, 256, 0, r->stream>>>(a, kind);
@@ -336,6 +342,9 @@ int dfc_create(int device, dfc_renderer** out) {
   cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, device);
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace, kTraceThreads, 0) == cudaSuccess && nb > 0) r->trace_blocks = nb;
+  nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_records, kTraceThreads, 0) == cudaSuccess && nb > 0)
+    r->trace_blocks = std::min(r->trace_blocks, nb);
   nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_ao, kTraceThreads, 0) == cudaSuccess && nb > 0) r->ao_blocks = nb;
   cudaGetLastError();
@@ -402,6 +411,7 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   DFC_CK(upload(r, r->d_tri_pos, hs.tri_pos), "scene upload");
   DFC_CK(upload(r, r->d_tri_attr, hs.tri_attr), "scene upload");
   DFC_CK(upload(r, r->d_rects, hs.rects), "scene upload");
+  DFC_CK(upload(r, r->d_shapes, hs.shapes), "scene upload");
   DFC_CK(upload(r, r->d_perez, hs.perez), "scene upload");
   std::vector<float> cam(hs.camera, hs.camera + 19);
   DFC_CK(upload(r, r->d_camera, cam), "scene upload");
@@ -421,6 +431,7 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   v.tri_pos = r->d_tri_pos.as<F4>();
   v.tri_attr = r->d_tri_attr.as<float>();
   v.rects = r->d_rects.as<float>();
+  v.shapes = r->d_shapes.as<float>();
   v.perez = r->d_perez.as<float>();
   v.camera = r->d_camera.as<float>();
   r->host = std::move(hs);
@@ -695,6 +706,7 @@ int noalloc_setup(dfc_renderer* r, unsigned** out) {
     cudaFuncAttributes fa;
     DFC_CK(cudaFuncGetAttributes(&fa, k_noalloc_prepare), "dfc_trace_rays_noalloc set-up");
     DFC_CK(cudaFuncGetAttributes(&fa, k_trace), "dfc_trace_rays_noalloc set-up");
+    DFC_CK(cudaFuncGetAttributes(&fa, k_trace_records), "dfc_trace_rays_noalloc set-up");
     g_noalloc_ptr[r->device] = static_cast<unsigned*>(p);
   }
   *out = g_noalloc_ptr[r->device];
@@ -742,7 +754,7 @@ extern "C" int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, c
   t.ray_d = reinterpret_cast<const float4*>(d_directions);
   t.hits = reinterpret_cast<float4*>(d_hits);
   t.paths = n;
-  k_trace<<<r->sm_count * r->trace_blocks, kTraceThreads, 0, r->stream>>>(t);
+  trace_kernel(r)<<<r->sm_count * r->trace_blocks, kTraceThreads, 0, r->stream>>>(t);
   DFC_CK(cudaGetLastError(), "dfc_trace_rays_noalloc launch");
   unsigned ov = 0;
   DFC_CK(cudaMemcpyAsync(&ov, scratch + 2, 4, cudaMemcpyDeviceToHost, r->stream), "dfc_trace_rays_noalloc readback");

@@ -366,6 +366,14 @@ struct Decoder {
     }
   }
 
+  // CompiledShape3FCache.java:90-310 record lengths
+  struct RecordArray { int id; const char* name; int length; size_t base; };
+  RecordArray record_arrays[7] = {
+      {kShapeDisk, "shape3FDisk3FArray", 4, 0}, {kShapeCylinder, "shape3FCylinder3FArray", 4, 0},
+      {kShapeCone, "shape3FCone3FArray", 4, 0}, {kShapeParaboloid, "shape3FParaboloid3FArray", 4, 0},
+      {kShapeHyperboloid, "shape3FHyperboloid3FArray", 16, 0}, {kShapeCuboid, "shape3FRectangularCuboid3FArray", 8, 0},
+      {kShapeTorus, "shape3FTorus3FArray", 2, 0}};
+
   void run() {
     const auto& P = I("primitiveArray");
     const auto& X = F("primitiveMatrix44FArray");
@@ -380,6 +388,13 @@ struct Decoder {
     if (C.size() < 19) throw Fail{DFC_E_INVALID_ARG, "cameraArray needs 19 floats"};
     std::memcpy(hs.camera, C.data(), sizeof hs.camera);
     hs.rects = R;
+    // the record-sized shapes share one float pool on the device
+    for (RecordArray& ra : record_arrays) {
+      ra.base = hs.shapes.size();
+      const auto& A = F(ra.name);
+      hs.shapes.insert(hs.shapes.end(), A.begin(), A.end());
+    }
+    if (hs.shapes.empty()) hs.shapes.assign(4, 0.0f);
     hs.perez = F("lightPerezLightArray");
     if (hs.rects.empty()) hs.rects.assign(16, 0.0f);
     if (hs.perez.empty()) hs.perez.assign(64, 0.0f);
@@ -421,6 +436,17 @@ struct Decoder {
         case kShapeSphere: case kShapePlane:
           pr.data = 0;
           break;
+        case kShapeDisk: case kShapeCylinder: case kShapeCone: case kShapeParaboloid: case kShapeHyperboloid:
+        case kShapeCuboid: case kShapeTorus: {
+          const RecordArray* ra = nullptr;
+          for (const RecordArray& x : record_arrays) if (x.id == pr.shape) ra = &x;
+          const size_t n = F(ra->name).size();
+          if (soff < 0 || soff % ra->length != 0 || (size_t)soff + (size_t)ra->length > n)
+            throw Fail{DFC_E_INVALID_ARG, std::string(ra->name) + " offset out of range"};
+          pr.data = (int)(ra->base + (size_t)soff);
+          hs.record_shapes = true;
+          break;
+        }
         case kShapeMesh: {
           auto it = blas_by_offset.find(soff);
           if (it == blas_by_offset.end()) {

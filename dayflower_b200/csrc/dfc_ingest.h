@@ -28,10 +28,12 @@ struct HostScene {
   std::vector<int> unbounded_storage;  // non-empty stand-in when there are no unbounded primitives
   std::vector<F4> tri_pos;
   std::vector<float> tri_attr, rects, perez;
+  std::vector<float> shapes;  // pool of the record-sized shapes (disk ... torus), DPrim.data = float offset
   float camera[19] = {0};
   int tlas_root = -1;
   int lights_storage_pad = 0;  // 1 when `lights` holds only a placeholder
   int64_t triangles = 0;
+  bool record_shapes = false;  // any disk, cylinder, cone, paraboloid, hyperboloid, cuboid or torus primitive
 };
 
 // Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.  On

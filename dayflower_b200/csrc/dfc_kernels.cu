@@ -16,6 +16,7 @@
 
 #include "dfc_device.cuh"
 #include "dfc_kernels.h"
+#include "dfc_shapes.cuh"
 
 namespace dfc {
 
@@ -54,6 +55,10 @@ DFC_D ObjRay obj_ray(const DPrim& pr, V3 o, V3 d) {
 
 // Object-space test of one analytic primitive; returns the object distance or -1.
 // Out of line: called at top-level leaves only, it keeps the traversal loop small.
+// kRecords adds disk ... torus (the double-precision torus solve enlarges the
+// call tree enough to cost the traversal loop registers, so scenes without
+// those shapes run the instantiation without them).
+template <bool kRecords>
 __device__ __noinline__ float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
   switch (pr.shape) {
     case kShapeSphere: return sphere_t(r.o, r.d, kTMin, tmax_obj);
@@ -63,7 +68,7 @@ __device__ __noinline__ float prim_t(const SceneView& S, const DPrim& pr, const 
     }
     case kShapeRectangle: return rect_t(S.rects + (size_t)pr.data * 16, r.o, r.d, kTMin, tmax_obj);
     case kShapePlane: return plane_t(r.o, r.d, kTMin, tmax_obj);
-    default: return -1.0f;
+    default: return kRecords ? record_shape_t(pr.shape, S.shapes + pr.data, r.o, r.d, kTMin, tmax_obj) : -1.0f;
   }
 }
 
@@ -106,6 +111,7 @@ DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin
 // this thread's column of the block's shared stack (stride kTraceBlock).
 // Stack entries: >= 0 node index; -1 end of a bottom level (back to world
 // space); <= -2 enter the bottom level of mesh primitive (-2 - entry).
+template <bool kRecords>
 DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit* out, int* stack, unsigned* overflow) {
   float best = tmax;
   bool found = false;
@@ -117,7 +123,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
     ObjRay r = obj_ray(pr, o, d);
-    float to = prim_t(S, pr, r, best * r.s);
+    float to = prim_t<kRecords>(S, pr, r, best * r.s);
     if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
       float tw = to / r.s;
       if (tw < best) {
@@ -193,7 +199,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
           if (!sphere_may_hit(bs, o, d, best)) continue;
           const DPrim& pr = S.prims[pi];
           ObjRay r = obj_ray(pr, o, d);
-          const float to = prim_t(S, pr, r, best * r.s);
+          const float to = prim_t<kRecords>(S, pr, r, best * r.s);
           if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
             const float tw = to / r.s;
             if (tw < best) {
@@ -250,6 +256,7 @@ struct Trav {
   float t_obj;
 };
 
+template <bool kRecords>
 DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack) {
   T.o = o; T.d = d; T.co = o; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
   T.any = any; T.in_blas = false;
@@ -260,7 +267,7 @@ DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool a
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
     ObjRay r = obj_ray(pr, o, d);
-    const float to = prim_t(S, pr, r, T.cbest * r.s);
+    const float to = prim_t<kRecords>(S, pr, r, T.cbest * r.s);
     if (to > kTMin) {
       const float tw = to / r.s;
       if (tw < T.cbest) {
@@ -347,6 +354,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
 
 // One item of this lane's pending leaf: a triangle of the current bottom
 // level, or a top-level item (a mesh is queued for its bottom level).
+template <bool kRecords>
 DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow, int& lf_first, int& lf_cnt) {
   const int i = lf_first++;
   --lf_cnt;
@@ -371,7 +379,7 @@ DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   if (!sphere_may_hit(bs, T.o, T.d, T.cbest)) return;
   const DPrim& pr = S.prims[pi];
   ObjRay r = obj_ray(pr, T.o, T.d);
-  const float to = prim_t(S, pr, r, T.cbest * r.s);
+  const float to = prim_t<kRecords>(S, pr, r, T.cbest * r.s);
   if (to > kTMin) {
     const float tw = to / r.s;
     if (tw < T.cbest) {
@@ -397,7 +405,8 @@ constexpr bool kSpeculate = DFC_SPECULATE != 0;  // lanes holding a leaf keep wa
 #ifndef DFC_TRACE_MIN_BLOCKS
 #define DFC_TRACE_MIN_BLOCKS 6
 #endif
-__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) {
+template <bool kRecords>
+__device__ __forceinline__ void trace_rays(const TraceArgs& a) {
   __shared__ int stack_smem[kStack * kTraceBlock];
   int* stack = stack_smem + threadIdx.x;
   const unsigned n = *a.ray_count;
@@ -425,7 +434,7 @@ __global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(Tra
           const unsigned p = ref >> 3, type = ref & 3u;
           slot = type * a.paths + p;
           const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
-          trav_init(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
+          trav_init<kRecords>(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
           lf_cnt = 0;
         }
       }
@@ -441,7 +450,7 @@ __global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(Tra
     }
     // leaf phase
     while (__any_sync(0xffffffffu, lf_cnt > 0)) {
-      if (lf_cnt > 0) leaf_step(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
+      if (lf_cnt > 0) leaf_step<kRecords>(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
     }
     if (act && T.sp == 0) {
       a.hits[slot] = make_float4(T.cbest, __int_as_float(T.prim), __int_as_float(T.aux), T.t_obj);
@@ -449,6 +458,9 @@ __global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(Tra
     }
   }
 }
+
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) { trace_rays<false>(a); }
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace_records(TraceArgs a) { trace_rays<true>(a); }
 
 __global__ void k_raygen(RaygenArgs a) {
   // No early return: every lane of the warp takes part in warp_append's ballot.
@@ -477,6 +489,7 @@ __global__ void k_raygen(RaygenArgs a) {
   if (p == 0) *a.work_count = a.paths;
 }
 
+template <bool kRecords>
 DFC_D V3 surface_of(const SceneView& S, const DPrim& pr, int aux, V3 o, V3 d, float t_obj, Surface* sf) {
   // the object ray as the intersector saw it
   V3 oo = o, od = d;
@@ -488,7 +501,10 @@ DFC_D V3 surface_of(const SceneView& S, const DPrim& pr, int aux, V3 o, V3 d, fl
     case kShapeSphere: *sf = sphere_surface(oo, od, t_obj); break;
     case kShapeRectangle: *sf = rect_surface(S.rects + (size_t)pr.data * 16, oo, od, t_obj); break;
     case kShapePlane: *sf = plane_surface(oo, od, t_obj); break;
-    default: *sf = triangle_surface(S.tri_attr + (size_t)aux * 24, oo, od, t_obj); break;
+    case kShapeTriangle: case kShapeMesh: *sf = triangle_surface(S.tri_attr + (size_t)aux * 24, oo, od, t_obj); break;
+    default:
+      if (kRecords) *sf = record_shape_surface(pr.shape, S.shapes + pr.data, oo, od, t_obj);
+      break;
   }
   surface_to_world(pr, *sf);
   return sf->p;
@@ -537,7 +553,8 @@ DFC_D void film_add(const ShadeArgs& a, unsigned pix, V3 L) {
 }
 
 // One shade step of the path tracer for every path on the work list.
-__global__ void k_shade_path(ShadeArgs a) {
+template <bool kRecords>
+__device__ __forceinline__ void shade_path(const ShadeArgs& a) {
   const unsigned n = *a.work_count;
   const unsigned stride = gridDim.x * blockDim.x;
   const SceneView& S = a.scene;
@@ -579,7 +596,7 @@ __global__ void k_shade_path(ShadeArgs a) {
             const DLight& lt = S.lights[li];
             const float4 mo = a.ray_o[2 * P + p];
             Surface s;
-            surface_of(S, hpr, __float_as_int(hm.z), V3{mo.x, mo.y, mo.z}, wi, hm.w, &s);
+            surface_of<kRecords>(S, hpr, __float_as_int(hm.z), V3{mo.x, mo.y, mo.z}, wi, hm.w, &s);
             if (lt.two_sided || dot(s.s.w, -wi) > 0.0f) L = L + mul(V3{c.x, c.y, c.z}, ld3(lt.radiance));
           }
         } else {
@@ -606,7 +623,7 @@ __global__ void k_shade_path(ShadeArgs a) {
         } else {
           const DPrim& pr = S.prims[hp];
           Surface sf;
-          surface_of(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
+          surface_of<kRecords>(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
           // SurfaceIntersection3F.transform: t = |origin - world point|
           if (rec) { a.primary_prim[p] = hp; a.primary_t[p] = world_t(pr, ray_o, sf); }
           const V3 wo = -ray_d;
@@ -731,6 +748,9 @@ __global__ void k_shade_path(ShadeArgs a) {
   }
 }
 
+__global__ void k_shade_path(ShadeArgs a) { shade_path<false>(a); }
+__global__ void k_shade_path_records(ShadeArgs a) { shade_path<true>(a); }
+
 // ---- material sort of the shade work list -----------------------------------
 // Shading diverges badly when one warp holds paths on different materials (each
 // material is a different BSDF routine), so the work list of every step is
@@ -804,7 +824,7 @@ __global__ void k_shade_primary(ShadeArgs a, int algorithm) {
     }
     const DPrim& pr = S.prims[hp];
     Surface sf;
-    surface_of(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
+    surface_of<true>(S, pr, __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
     if (a.record_primary && p < a.pixels) { a.primary_prim[p] = hp; a.primary_t[p] = world_t(pr, ray_o, sf); }
     if (algorithm == DFC_ALGO_RAY_CASTING) {
       float c = fabsf(dot(sf.s.w, ray_d)) * 0.5f;
@@ -841,10 +861,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(AoArgs a) {
     Hit h = {0.0f, -1, -1, 0.0f};
     float v;
     if (a.max_distance > 0.0f) {
-      bool hit = trace_ray(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, false, &h, stack, a.overflow);
+      bool hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, false, &h, stack, a.overflow);
       v = hit ? clampf(h.t, 0.0f, a.max_distance) / a.max_distance : 1.0f;
     } else {
-      bool hit = trace_ray(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, true, &h, stack, a.overflow);
+      bool hit = trace_ray<true>(a.scene, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, kFltMax, true, &h, stack, a.overflow);
       v = hit ? 0.0f : 1.0f;
     }
     a.ao_value[i] = v;

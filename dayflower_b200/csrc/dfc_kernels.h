@@ -96,8 +96,13 @@ __global__ void k_sort_count(SortArgs a);
 __global__ void k_sort_scatter(SortArgs a);
 
 __global__ void k_raygen(RaygenArgs a);
+// Closest/any hit of the listed rays.  k_trace_records also tests disk,
+// cylinder, cone, paraboloid, hyperboloid, cuboid and torus primitives; launch
+// it when the scene has any (SceneView has no flag for it: the host knows).
 __global__ void k_trace(TraceArgs a);
+__global__ void k_trace_records(TraceArgs a);
 __global__ void k_shade_path(ShadeArgs a);
+__global__ void k_shade_path_records(ShadeArgs a);  // with the disk ... torus surfaces
 __global__ void k_shade_primary(ShadeArgs a, int algorithm);
 __global__ void k_trace_ao(AoArgs a);
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);

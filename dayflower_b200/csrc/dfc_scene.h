@@ -118,6 +118,7 @@ struct SceneView {
   const F4* tri_pos;            // 3 per triangle, reordered; v0.w holds the triangle index
   const float* tri_attr;        // shape3FTriangle3FArray, 24 floats per triangle, original order
   const float* rects;           // shape3FRectangle3FArray
+  const float* shapes;          // disk, cylinder, cone, paraboloid, hyperboloid, cuboid and torus records
   const float* perez;           // lightPerezLightArray
   const float* camera;          // 19 floats
 };

@@ -111,6 +111,12 @@ def _world_aabb(points_obj: np.ndarray, o2w: np.ndarray):
     return w.min(axis=0), w.max(axis=0)
 
 
+# Shapes stored as one fixed-length record each (CompiledShape3FCache.java:90-310).
+_RECORD_SHAPES = {M.Disk: "shape3FDisk3FArray", M.Cylinder: "shape3FCylinder3FArray", M.Cone: "shape3FCone3FArray",
+                  M.Paraboloid: "shape3FParaboloid3FArray", M.Hyperboloid: "shape3FHyperboloid3FArray",
+                  M.RectangularCuboid: "shape3FRectangularCuboid3FArray", M.Torus: "shape3FTorus3FArray"}
+
+
 def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> CompiledScene:
     if layout_version not in (1, 2):
         raise ValueError("layout_version must be 1 or 2")
@@ -193,6 +199,8 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
             off = push("shape3FRectangle3FArray", s.to_array())
         elif isinstance(s, (M.Sphere, M.Plane)):
             off = 0
+        elif isinstance(s, tuple(_RECORD_SHAPES)):
+            off = push(_RECORD_SHAPES[type(s)], s.to_array())
         elif isinstance(s, M.TriangleMesh):
             tri_base = push("shape3FTriangle3FArray", s.triangles)
             aabb_base = sizes["boundingVolume3FAxisAlignedBoundingBox3FArray"] // 8
@@ -258,7 +266,7 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
                 pts = np.array([[-1, -1, -1], [1, 1, 1]], dtype=np.float32)
             elif isinstance(p.shape, M.Triangle):
                 pts = np.stack([p.shape.a, p.shape.b, p.shape.c])
-            elif isinstance(p.shape, M.Rectangle):
+            elif isinstance(p.shape, M.Rectangle) or isinstance(p.shape, tuple(_RECORD_SHAPES)):
                 pts = p.shape.corners()
             else:
                 pts = p.shape.triangles[:, 0:9].reshape(-1, 3)

@@ -166,3 +166,43 @@ def small_mixed_scene(resolution=(96, 64), seed=7, cells=24, n_spheres=24, with_
         sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((5.0, 6.0, 1.0), 0.7), area_light=sl))
     del rng
     return sc
+
+
+def _rot_x(deg, position, scale=1.0):
+    """Object-to-world: rotate about x by `deg`, scale, then translate."""
+    c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))
+    m = np.eye(4)
+    m[:3, :3] = np.array([[1, 0, 0], [0, c, -s], [0, s, c]]) * float(scale)
+    m[:3, 3] = position
+    return M.Transform.from_matrix(m)
+
+
+def quadrics_scene(resolution=(128, 96), with_lights=True) -> M.Scene:
+    """Disk, cylinder, cone, paraboloid, hyperboloid, rectangular cuboid and torus
+    (full and partial sweeps) standing on a ground plane, z-up objects turned
+    upright, lit by a point light, a directional light and a spherical area light."""
+    cam = M.Camera(eye=(0.0, 3.8, 9.0), look_at=(0.0, 1.0, 0.0), fov_x_deg=70.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="quadrics")
+    up = -90.0  # object z -> world y
+    shapes = [
+        (M.Disk(300.0, 0.4, 1.2, 0.0), M.Matte(kd=(0.7, 0.3, 0.3)), _rot_x(up, (-6.0, 0.01, 2.0))),
+        (M.Cylinder(360.0, 0.8, 2.0, 0.0), M.Plastic(kd=(0.2, 0.5, 0.7), ks=(0.3, 0.3, 0.3), roughness=0.2), _rot_x(up, (-3.0, 0.0, 0.0))),
+        (M.Cylinder(270.0, 0.6, 1.5, 0.0), M.Metal(roughness_u=0.3, roughness_v=0.3), _rot_x(up, (-6.0, 0.0, -3.0))),
+        (M.Cone(360.0, 1.0, 2.5), M.Matte(kd=(0.8, 0.7, 0.2)), _rot_x(up, (0.0, 0.0, -2.0))),
+        (M.Paraboloid(360.0, 1.0, 2.0, 0.0), M.Matte(kd=(0.3, 0.8, 0.4)), _rot_x(up, (3.0, 0.0, 0.0))),
+        (M.Hyperboloid(360.0, (0.3, 0.3, 0.0), (1.0, 0.2, 2.0)), M.Plastic(kd=(0.6, 0.3, 0.7), ks=(0.2, 0.2, 0.2), roughness=0.4),
+         _rot_x(up, (6.0, 0.0, -2.0))),
+        (M.RectangularCuboid((-0.7, -0.7, 0.0), (0.7, 0.7, 1.4)), M.Matte(kd=(0.5, 0.5, 0.8)), _rot_x(up, (1.5, 0.0, 3.0))),
+        (M.Torus(0.35, 1.0), M.Metal(roughness_u=0.15, roughness_v=0.15), _rot_x(-60.0, (-1.5, 1.4, 3.5))),
+        (M.Torus(0.25, 0.8), M.Matte(kd=(0.9, 0.5, 0.1)), _rot_x(0.0, (4.5, 2.2, 3.0))),
+    ]
+    for shp, mat, tr in shapes:
+        sc.add(M.Primitive(shp, mat, tr))
+    sc.add(M.Primitive(M.Plane(), M.Matte(kd=(0.6, 0.6, 0.6)), _rot_x(-90.0, (0.0, 0.0, 0.0))))
+    if with_lights:
+        sc.lights.append(M.PointLight((4.0, 9.0, 6.0), (90.0, 90.0, 90.0)))
+        sc.lights.append(M.DirectionalLight((-0.4, 1.0, 0.5), (0.6, 0.6, 0.6)))
+        sl = M.DiffuseAreaLight(M.Sphere(), (8.0, 7.0, 6.0), transform=M.Transform.translate_scale((-4.0, 7.0, 4.0), 0.8))
+        sc.lights.append(sl)
+        sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((-4.0, 7.0, 4.0), 0.8), area_light=sl))
+    return sc

@@ -157,6 +157,147 @@ class Rectangle(Shape):
         return np.stack([self.a, self.b, self.c, self.d])
 
 
+def _rad(degrees) -> float:
+    """``AngleF.degrees(d).getRadians()``: the float of d * pi / 180."""
+    return float(np.float32(math.radians(degrees)))
+
+
+def _box_corners(lo, hi) -> np.ndarray:
+    lo, hi = _v(lo), _v(hi)
+    return np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])], dtype=np.float32)
+
+
+class Disk(Shape):
+    """``geometry/shape/Disk3F``: the annulus ri <= r <= ro at z = zMax, phi <= phiMax."""
+    ID = SHAPE_DISK
+
+    def __init__(self, phi_max_degrees=360.0, radius_inner=0.0, radius_outer=1.0, z_max=0.0):
+        self.phi_max, self.ri, self.ro, self.z_max = _rad(phi_max_degrees), radius_inner, radius_outer, z_max
+
+    def to_array(self):
+        """``CompiledShape3FCache.toDisk3F``: phiMax, radiusInner, radiusOuter, zMax."""
+        return np.array([self.phi_max, self.ri, self.ro, self.z_max], dtype=np.float32)
+
+    def corners(self):
+        return _box_corners((-self.ro, -self.ro, self.z_max), (self.ro, self.ro, self.z_max))
+
+
+class Cylinder(Shape):
+    """``geometry/shape/Cylinder3F``: radius r about z, zMin <= z <= zMax."""
+    ID = SHAPE_CYLINDER
+
+    def __init__(self, phi_max_degrees=360.0, radius=1.0, z_max=1.0, z_min=-1.0):
+        self.phi_max, self.radius, self.z_max, self.z_min = _rad(phi_max_degrees), radius, z_max, z_min
+
+    def to_array(self):
+        """``CompiledShape3FCache.toCylinder3F``: phiMax, radius, zMax, zMin."""
+        return np.array([self.phi_max, self.radius, self.z_max, self.z_min], dtype=np.float32)
+
+    def corners(self):
+        return _box_corners((-self.radius, -self.radius, self.z_min), (self.radius, self.radius, self.z_max))
+
+
+class Cone(Shape):
+    """``geometry/shape/Cone3F``: apex at z = zMax, base radius r at z = 0."""
+    ID = SHAPE_CONE
+
+    def __init__(self, phi_max_degrees=360.0, radius=1.0, z_max=1.0):
+        self.phi_max, self.radius, self.z_max = _rad(phi_max_degrees), radius, z_max
+
+    def to_array(self):
+        """``CompiledShape3FCache.toCone3F``: phiMax, radius, zMax, 0."""
+        return np.array([self.phi_max, self.radius, self.z_max, 0.0], dtype=np.float32)
+
+    def corners(self):
+        return _box_corners((-self.radius, -self.radius, 0.0), (self.radius, self.radius, self.z_max))
+
+
+class Paraboloid(Shape):
+    """``geometry/shape/Paraboloid3F``: z = zMax (x^2 + y^2) / r^2, zMin <= z <= zMax."""
+    ID = SHAPE_PARABOLOID
+
+    def __init__(self, phi_max_degrees=360.0, radius=1.0, z_max=1.0, z_min=0.0):
+        self.phi_max, self.radius, self.z_max, self.z_min = _rad(phi_max_degrees), radius, z_max, z_min
+
+    def to_array(self):
+        """``CompiledShape3FCache.toParaboloid3F``: phiMax, radius, zMax, zMin."""
+        return np.array([self.phi_max, self.radius, self.z_max, self.z_min], dtype=np.float32)
+
+    def corners(self):
+        return _box_corners((-self.radius, -self.radius, self.z_min), (self.radius, self.radius, self.z_max))
+
+
+class Hyperboloid(Shape):
+    """``geometry/shape/Hyperboloid3F``: the surface swept by the segment a-b about z.
+    The coefficients follow the reference constructor (``Hyperboloid3F.java:144-178``),
+    evaluated in float."""
+    ID = SHAPE_HYPERBOLOID
+
+    def __init__(self, phi_max_degrees=360.0, a=(0.0001, 0.0001, 0.0), b=(1.0, 1.0, 1.0)):
+        f = np.float32
+        a, b = _v(a), _v(b)
+        pa = a if a[2] == 0 else (b if b[2] == 0 else a)
+        pb = b if a[2] == 0 else (a if b[2] == 0 else b)
+        pc = pa.copy()
+        aH = cH = f(np.inf)
+        with np.errstate(all="ignore"):
+            for _ in range(10):
+                if np.isfinite(aH):
+                    break
+                pc = (pc + (pb - pa) * f(2.0)).astype(np.float32)
+                c = f(pc[0] * pc[0] + pc[1] * pc[1])
+                d = f(pb[0] * pb[0] + pb[1] * pb[1])
+                aH = f((f(1.0) / c - (pc[2] * pc[2]) / (c * pb[2] * pb[2])) / (f(1.0) - (d * pc[2] * pc[2]) / (c * pb[2] * pb[2])))
+                cH = f((aH * d - f(1.0)) / (pb[2] * pb[2]))
+        if not np.isfinite(aH):
+            raise ValueError("degenerate hyperboloid")
+        self.phi_max, self.a, self.b, self.aH, self.cH = _rad(phi_max_degrees), pa, pb, float(aH), float(cH)
+        self.r_max = float(max(np.sqrt(f(a[0] * a[0] + a[1] * a[1])), np.sqrt(f(b[0] * b[0] + b[1] * b[1]))))
+        self.z_max, self.z_min = float(max(a[2], b[2])), float(min(a[2], b[2]))
+
+    def to_array(self):
+        """``CompiledShape3FCache.toHyperboloid3F``: 16 floats."""
+        out = np.zeros(16, dtype=np.float32)
+        out[0] = self.phi_max
+        out[1:4], out[4:7] = self.a, self.b
+        out[7], out[8], out[9], out[10], out[11] = self.aH, self.cH, self.r_max, self.z_max, self.z_min
+        return out
+
+    def corners(self):
+        return _box_corners((-self.r_max, -self.r_max, self.z_min), (self.r_max, self.r_max, self.z_max))
+
+
+class RectangularCuboid(Shape):
+    """``geometry/shape/RectangularCuboid3F``: an axis-aligned box in object space."""
+    ID = SHAPE_CUBOID
+
+    def __init__(self, minimum=(-0.5, -0.5, -0.5), maximum=(0.5, 0.5, 0.5)):
+        self.minimum, self.maximum = _v(np.minimum(minimum, maximum)), _v(np.maximum(minimum, maximum))
+
+    def to_array(self):
+        """``CompiledShape3FCache.toRectangularCuboid3F``: maximum, minimum, 0, 0."""
+        return np.concatenate([self.maximum, self.minimum, [0.0, 0.0]]).astype(np.float32)
+
+    def corners(self):
+        return _box_corners(self.minimum, self.maximum)
+
+
+class Torus(Shape):
+    """``geometry/shape/Torus3F``: tube radius ri around a circle of radius ro in z = 0."""
+    ID = SHAPE_TORUS
+
+    def __init__(self, radius_inner=0.25, radius_outer=1.0):
+        self.ri, self.ro = radius_inner, radius_outer
+
+    def to_array(self):
+        """``CompiledShape3FCache.toTorus3F``: radiusInner, radiusOuter."""
+        return np.array([self.ri, self.ro], dtype=np.float32)
+
+    def corners(self):
+        r = self.ri + self.ro  # the reference bounds it by a sphere of this radius
+        return _box_corners((-r, -r, -r), (r, r, r))
+
+
 # ------------------------------------------------------------- materials ----
 @dataclass(eq=False)
 class Material:

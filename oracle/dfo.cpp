@@ -318,6 +318,300 @@ inline Surface plane_surface(const Ray& r, float t) {
   return s;
 }
 
+// ---- quadric, disk, box and torus shapes -----------------------------------
+// The CPU shapes call org.macroing.java.lang.Floats, which is not vendored; its
+// routines are restated from the same author's utility/Floats.java.
+
+// java.lang.Math.min/max on floats: NaN propagates, -0 < +0.
+inline float jmin(float a, float b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a == 0.0f && b == 0.0f) return std::signbit(a) ? a : b;
+  return a <= b ? a : b;
+}
+inline float jmax(float a, float b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a == 0.0f && b == 0.0f) return std::signbit(a) ? b : a;
+  return a >= b ? a : b;
+}
+
+// geometry/Point3F.java:223 sphericalPhi (Floats.atan2 is Math.atan2 in double)
+inline float spherical_phi(float x, float y) {
+  float phi = (float)std::atan2((double)y, (double)x);
+  return phi < 0.0f ? phi + 2.0f * kPi : phi;
+}
+
+// utility/Floats.java:1227 solveQuadraticSystem: {NaN, NaN} without real roots.
+inline void solve_quadratic(float a, float b, float c, float* r0, float* r1) {
+  const float disc2 = b * b - 4.0f * a * c;
+  *r0 = NAN; *r1 = NAN;
+  if (disc2 == 0.0f) {
+    const float q = -0.5f * b / a;
+    *r0 = q; *r1 = q;
+  } else if (disc2 > 0.0f) {
+    const float disc = std::sqrt(disc2);
+    const float q = -0.5f * (b > 0.0f ? b + disc : b - disc);
+    const float x0 = q / a, x1 = c / q;
+    *r0 = jmin(x0, x1); *r1 = jmax(x0, x1);
+  }
+}
+
+inline V3 point_at(const Ray& r, float t) { return V3{r.o.x + r.d.x * t, r.o.y + r.d.y * t, r.o.z + r.d.z * t}; }
+inline float len2d(V3 p) { return std::sqrt(p.x * p.x + p.y * p.y); }
+
+// The quadrics share one loop: the first root in (tmin, tmax) whose point
+// passes `inside` wins; a NaN root ends the search (Cylinder3F.java:342 and
+// the same method of Cone3F, Paraboloid3F, Hyperboloid3F).
+template <typename PointF, typename InsideF>
+inline float quadric_t(float a, float b, float c, const Ray& r, float tmin, float tmax, PointF point, InsideF inside) {
+  float ts[2];
+  solve_quadratic(a, b, c, &ts[0], &ts[1]);
+  for (int i = 0; i < 2; ++i) {
+    const float t = ts[i];
+    if (t != t) return NAN;
+    if (t > tmin && t < tmax && inside(point(r, t))) return t;
+  }
+  return NAN;
+}
+
+inline ONB uv_frame(V3 u, V3 v) {
+  u = normalize(u);
+  v = normalize(v);
+  return ONB{cross(u, v), v, u};
+}
+
+inline Surface simple_surface(const Ray& r, float t, V3 p, ONB g, float tu, float tv) {
+  Surface s;
+  s.g = g; s.s = g; s.tu = tu; s.tv = tv; s.p = p; s.ray = r; s.t = t;
+  return s;
+}
+
+// geometry/shape/Disk3F.java:342 (record: phiMax, radiusInner, radiusOuter, zMax)
+inline float disk_t(const float* q, const Ray& r, float tmin, float tmax) {
+  if (r.d.z == 0.0f) return NAN;
+  const float t = (q[3] - r.o.z) / r.d.z;
+  if (t <= tmin || t >= tmax) return NAN;
+  V3 p = point_at(r, t);
+  p.z = q[3];
+  const float l2 = p.x * p.x + p.y * p.y;
+  if (l2 > q[2] * q[2] || l2 < q[1] * q[1] || spherical_phi(p.x, p.y) > q[0]) return NAN;
+  return t;
+}
+inline Surface disk_surface(const float* q, const Ray& r, float t) {
+  V3 p = point_at(r, t);
+  p.z = q[3];
+  const float l = len2d(p);
+  const ONB g = uv_frame(V3{-q[0] * p.y, q[0] * p.x, 0.0f}, V3{p.x * (q[1] - q[2]) / l, p.y * (q[1] - q[2]) / l, 0.0f});
+  return simple_surface(r, t, p, g, spherical_phi(p.x, p.y) / q[0], (q[2] - l) / (q[2] - q[1]));
+}
+
+// geometry/shape/Cylinder3F.java:342 (record: phiMax, radius, zMax, zMin)
+inline V3 cylinder_point(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const float s = q[1] / len2d(p);
+  return V3{p.x * s, p.y * s, p.z};
+}
+inline float cylinder_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const V3 o = r.o, d = r.d;
+  const float a = d.x * d.x + d.y * d.y;
+  const float b = 2.0f * (d.x * o.x + d.y * o.y);
+  const float c = o.x * o.x + o.y * o.y - q[1] * q[1];
+  return quadric_t(a, b, c, r, tmin, tmax, [&](const Ray& rr, float t) { return cylinder_point(q, rr, t); },
+                   [&](V3 p) { return p.z >= q[3] && p.z <= q[2] && spherical_phi(p.x, p.y) <= q[0]; });
+}
+inline Surface cylinder_surface(const float* q, const Ray& r, float t) {
+  const V3 p = cylinder_point(q, r, t);
+  const ONB g = uv_frame(V3{-q[0] * p.y, q[0] * p.x, 0.0f}, V3{0.0f, 0.0f, q[2] - q[3]});
+  return simple_surface(r, t, p, g, spherical_phi(p.x, p.y) / q[0], (p.z - q[3]) / (q[2] - q[3]));
+}
+
+// geometry/shape/Cone3F.java (record: phiMax, radius, zMax, 0)
+inline float cone_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const V3 o = r.o, d = r.d;
+  const float k = (q[1] / q[2]) * (q[1] / q[2]);
+  const float a = d.x * d.x + d.y * d.y - k * d.z * d.z;
+  const float b = 2.0f * (d.x * o.x + d.y * o.y - k * d.z * (o.z - q[2]));
+  const float c = o.x * o.x + o.y * o.y - k * (o.z - q[2]) * (o.z - q[2]);
+  return quadric_t(a, b, c, r, tmin, tmax, [](const Ray& rr, float t) { return point_at(rr, t); },
+                   [&](V3 p) { return p.z >= 0.0f && p.z <= q[2] && spherical_phi(p.x, p.y) <= q[0]; });
+}
+inline Surface cone_surface(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const float value = 1.0f - (p.z / q[2]);
+  const ONB g = uv_frame(V3{-q[0] * p.y, q[0] * p.x, 0.0f}, V3{-p.x / value, -p.y / value, q[2]});
+  return simple_surface(r, t, p, g, spherical_phi(p.x, p.y) / q[0], p.z / q[2]);
+}
+
+// geometry/shape/Paraboloid3F.java (record: phiMax, radius, zMax, zMin)
+inline float paraboloid_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const V3 o = r.o, d = r.d;
+  const float k = q[2] / (q[1] * q[1]);
+  const float a = k * (d.x * d.x + d.y * d.y);
+  const float b = 2.0f * k * (d.x * o.x + d.y * o.y) - d.z;
+  const float c = k * (o.x * o.x + o.y * o.y) - o.z;
+  return quadric_t(a, b, c, r, tmin, tmax, [](const Ray& rr, float t) { return point_at(rr, t); },
+                   [&](V3 p) { return p.z >= q[3] && p.z <= q[2] && spherical_phi(p.x, p.y) <= q[0]; });
+}
+inline Surface paraboloid_surface(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const float dz = q[2] - q[3];
+  const ONB g = uv_frame(V3{-q[0] * p.y, q[0] * p.x, 0.0f}, V3{dz * (p.x / (2.0f * p.z)), dz * (p.y / (2.0f * p.z)), dz});
+  return simple_surface(r, t, p, g, spherical_phi(p.x, p.y) / q[0], (p.z - q[3]) / dz);
+}
+
+// geometry/shape/Hyperboloid3F.java (record: phiMax, A xyz, B xyz, aH, cH, rMax, zMax, zMin)
+inline float hyperboloid_phi(const float* q, V3 p, float v) {
+  // Point3F.lerp with Floats.lerp: (1 - t) * a + t * b
+  const float ax = (1.0f - v) * q[1] + v * q[4], ay = (1.0f - v) * q[2] + v * q[5];
+  return spherical_phi(p.x * ax + p.y * ay, p.y * ax - p.x * ay);
+}
+inline float hyperboloid_phi(const float* q, V3 p) { return hyperboloid_phi(q, p, (p.z - q[3]) / (q[6] - q[3])); }
+inline float hyperboloid_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const V3 o = r.o, d = r.d;
+  const float aH = q[7], cH = q[8];
+  const float a = aH * d.x * d.x + aH * d.y * d.y - cH * d.z * d.z;
+  const float b = 2.0f * (aH * d.x * o.x + aH * d.y * o.y - cH * d.z * o.z);
+  const float c = aH * o.x * o.x + aH * o.y * o.y - cH * o.z * o.z - 1.0f;
+  return quadric_t(a, b, c, r, tmin, tmax, [](const Ray& rr, float t) { return point_at(rr, t); },
+                   [&](V3 p) { return p.z >= q[11] && p.z <= q[10] && hyperboloid_phi(q, p) <= q[0]; });
+}
+inline Surface hyperboloid_surface(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const float phi = hyperboloid_phi(q, p);
+  const float c = (float)std::cos((double)phi), sn = (float)std::sin((double)phi);
+  const V3 v = {(q[4] - q[1]) * c - (q[5] - q[2]) * sn, (q[4] - q[1]) * sn + (q[5] - q[2]) * c, q[6] - q[3]};
+  const ONB g = uv_frame(V3{-q[0] * p.y, q[0] * p.x, 0.0f}, v);
+  const float tv = (p.z - q[3]) / (q[6] - q[3]);
+  return simple_surface(r, t, p, g, hyperboloid_phi(q, p, tv) / q[0], tv);
+}
+
+// geometry/shape/RectangularCuboid3F.java (record: maximum xyz, minimum xyz, 0, 0)
+inline float cuboid_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const V3 rd = {1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
+  const V3 da = {(q[3] - r.o.x) * rd.x, (q[4] - r.o.y) * rd.y, (q[5] - r.o.z) * rd.z};
+  const V3 db = {(q[0] - r.o.x) * rd.x, (q[1] - r.o.y) * rd.y, (q[2] - r.o.z) * rd.z};
+  const float t0 = jmax(jmax(jmin(da.x, db.x), jmin(da.y, db.y)), jmin(da.z, db.z));
+  const float t1 = jmin(jmin(jmax(da.x, db.x), jmax(da.y, db.y)), jmax(da.z, db.z));
+  if (t0 > t1) return NAN;
+  if (t0 > tmin && t0 < tmax) return t0;
+  if (t1 > tmin && t1 < tmax) return t1;
+  return NAN;
+}
+inline Surface cuboid_surface(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const V3 mid = {(q[0] + q[3]) * 0.5f, (q[1] + q[4]) * 0.5f, (q[2] + q[5]) * 0.5f};
+  const V3 half = {(q[0] - q[3]) * 0.5f, (q[1] - q[4]) * 0.5f, (q[2] - q[5]) * 0.5f};
+  const bool x0 = p.x + half.x - 0.0001f < mid.x, x1 = p.x - half.x + 0.0001f > mid.x;
+  const bool y0 = p.y + half.y - 0.0001f < mid.y, y1 = p.y - half.y + 0.0001f > mid.y;
+  const bool z0 = p.z + half.z - 0.0001f < mid.z, z1 = p.z - half.z + 0.0001f > mid.z;
+  ONB g = ONB{V3{0, 0, 1}, V3{0, 1, 0}, V3{1, 0, 0}};
+  if (x0) g = onb_from_w(V3{-1, 0, 0});
+  else if (x1) g = onb_from_w(V3{1, 0, 0});
+  else if (y0) g = onb_from_w(V3{0, -1, 0});
+  else if (y1) g = onb_from_w(V3{0, 1, 0});
+  else if (z0) g = onb_from_w(V3{0, 0, -1});
+  else if (z1) g = onb_from_w(V3{0, 0, 1});
+  auto nrm = [](float v, float a, float b) { const float mx = jmax(a, b), mn = jmin(a, b); return (v - mn) / (mx - mn); };
+  float tu = 0.0f, tv = 0.0f;
+  if (x0 || x1) { tu = nrm(p.z, q[5], q[2]); tv = nrm(p.y, q[4], q[1]); }
+  else if (y0 || y1) { tu = nrm(p.x, q[3], q[0]); tv = nrm(p.z, q[5], q[2]); }
+  else if (z0 || z1) { tu = nrm(p.x, q[3], q[0]); tv = nrm(p.y, q[4], q[1]); }
+  return simple_surface(r, t, p, g, tu, tv);
+}
+
+// geometry/shape/Torus3F.java (record: radiusInner, radiusOuter): a quartic in
+// double precision, solved by the reference's own resolvent-cubic method.
+inline double torus_cubic(double p, double q, double r) {
+  const double p2 = p * p;
+  const double q0 = (p2 - 3.0 * q) / 9.0;
+  const double q0c = q0 * q0 * q0;
+  const double r0 = (p * (p2 - 4.5 * q) + 13.5 * r) / 27.0;
+  const double r02 = r0 * r0;
+  const double d = q0c - r02;
+  const double e = p / 3.0;
+  if (d >= 0.0) {
+    const double d0 = r0 / std::sqrt(q0c);
+    const double theta = std::acos(d0) / 3.0;
+    const double q1 = -2.0 * std::sqrt(q0);
+    return q1 * std::cos(theta) - e;
+  }
+  const double q1 = std::pow(std::sqrt(r02 - q0c) + std::fabs(r0), 1.0 / 3.0);
+  return r0 < 0.0 ? (q1 + q0 / q1) - e : -(q1 + q0 / q1) - e;
+}
+inline int torus_quartic(double a, double b, double c, double d, double e, double* out) {
+  const double ar = 1.0 / a;
+  const double bA = b * ar, bA2 = bA * bA, cA = c * ar, dA = d * ar, eA = e * ar;
+  const double p = -0.375 * bA2 + cA;
+  const double q = 0.125 * bA2 * bA - 0.5 * bA * cA + dA;
+  const double r = -0.01171875 * bA2 * bA2 + 0.0625 * bA2 * cA - 0.25 * bA * dA + eA;
+  const double z = torus_cubic(-0.5 * p, -r, 0.5 * r * p - 0.125 * q * q);
+  double d1 = 2.0 * z - p, d2;
+  if (d1 < 0.0) return 0;
+  if (d1 < 1.0e-10) {
+    d2 = z * z - r;
+    if (d2 < 0.0) return 0;
+    d2 = std::sqrt(d2);
+  } else {
+    d1 = std::sqrt(d1);
+    d2 = 0.5 * q / d1;
+  }
+  const double q1 = d1 * d1, q2 = -0.25 * bA;
+  const double pm = q1 - 4.0 * (z - d2), pp = q1 - 4.0 * (z + d2);
+  if (pm >= 0.0 && pp >= 0.0) {
+    const double pms = std::sqrt(pm), pps = std::sqrt(pp);
+    out[0] = -0.5 * (d1 + pms) + q2;
+    out[1] = -0.5 * (d1 - pms) + q2;
+    out[2] = 0.5 * (d1 + pps) + q2;
+    out[3] = 0.5 * (d1 - pps) + q2;
+    for (int i = 1; i < 4; ++i)
+      for (int j = i; j > 0 && out[j - 1] > out[j]; --j) std::swap(out[j], out[j - 1]);
+    return 4;
+  }
+  if (pm >= 0.0) {
+    const double pms = std::sqrt(pm);
+    out[0] = -0.5 * (d1 + pms) + q2;
+    out[1] = -0.5 * (d1 - pms) + q2;
+    return 2;
+  }
+  if (pp >= 0.0) {
+    const double pps = std::sqrt(pp);
+    out[0] = 0.5 * (d1 - pps) + q2;
+    out[1] = 0.5 * (d1 + pps) + q2;
+    return 2;
+  }
+  return 0;
+}
+inline float torus_t(const float* q, const Ray& r, float tmin, float tmax) {
+  const float ri2 = q[0] * q[0], ro2 = q[1] * q[1];
+  const double f0 = (double)dot(r.d, r.d);
+  const double f1 = (double)dot(r.o, r.d) * 2.0;
+  const double f2 = ri2, f3 = ro2;
+  const double f4 = (double)dot(r.o, r.o) - f2 - f3;
+  const double f5 = r.d.z, f6 = r.o.z;
+  const double a = f0 * f0;
+  const double b = f0 * 2.0 * f1;
+  const double c = f1 * f1 + 2.0 * f0 * f4 + 4.0 * f3 * f5 * f5;
+  const double d = f1 * 2.0 * f4 + 8.0 * f3 * f6 * f5;
+  const double e = f4 * f4 + 4.0 * f3 * f6 * f6 - 4.0 * f3 * f2;
+  double ts[4];
+  const int n = torus_quartic(a, b, c, d, e, ts);
+  if (n == 0) return NAN;
+  if (ts[0] >= tmax || ts[n - 1] <= tmin) return NAN;
+  for (int i = 0; i < n; ++i)
+    if (ts[i] > tmin) return (float)ts[i];
+  return NAN;
+}
+inline Surface torus_surface(const float* q, const Ray& r, float t) {
+  const V3 p = point_at(r, t);
+  const float ri2 = q[0] * q[0], ro2 = q[1] * q[1];
+  const float der = dot(p, p) - ri2 - ro2;
+  const ONB g = onb_from_w(normalize(V3{p.x * der, p.y * der, p.z * der + 2.0f * ro2 * p.z}));
+  const float phi = (float)std::asin((double)saturate(p.z / q[0], -1.0f, 1.0f));
+  const float theta = spherical_phi(p.x, p.y);
+  return simple_surface(r, t, p, g, theta * (1.0f / (2.0f * kPi)), (phi + kPi / 2.0f) * (1.0f / kPi));
+}
+
 // renderer/gpu/AbstractShape3FKernel.java:3735 threaded mesh BVH stream, walked
 // with TriangleMesh3F's closest-hit rule (geometry/boundingvolume/hierarchy/*BVHNode3F.java).
 inline float mesh_t(const Scene& sc, int mesh_off, const Ray& r, float tmin, float tmax, int* tri_out) {
@@ -356,6 +650,13 @@ inline float shape_t(const Scene& sc, int sid, int soff, const Ray& r, float tmi
     case kShapeSphere: { SphereHit h; return sphere_hit(r, tmin, tmax, &h) ? h.t : NAN; }
     case kShapeRectangle: return rect_t(load_rect(sc.F("shape3FRectangle3FArray"), soff), r, tmin, tmax);
     case kShapePlane: return plane_t(r, tmin, tmax);
+    case kShapeDisk: return disk_t(sc.F("shape3FDisk3FArray").data() + soff, r, tmin, tmax);
+    case kShapeCylinder: return cylinder_t(sc.F("shape3FCylinder3FArray").data() + soff, r, tmin, tmax);
+    case kShapeCone: return cone_t(sc.F("shape3FCone3FArray").data() + soff, r, tmin, tmax);
+    case kShapeParaboloid: return paraboloid_t(sc.F("shape3FParaboloid3FArray").data() + soff, r, tmin, tmax);
+    case kShapeHyperboloid: return hyperboloid_t(sc.F("shape3FHyperboloid3FArray").data() + soff, r, tmin, tmax);
+    case kShapeCuboid: return cuboid_t(sc.F("shape3FRectangularCuboid3FArray").data() + soff, r, tmin, tmax);
+    case kShapeTorus: return torus_t(sc.F("shape3FTorus3FArray").data() + soff, r, tmin, tmax);
     default: return NAN;
   }
 }
@@ -383,6 +684,21 @@ inline bool shape_surface(const Scene& sc, int sid, int soff, const Ray& r, floa
       *s = rect_surface(q, r, t); *tri_out = -1; return true;
     }
     case kShapePlane: { float t = plane_t(r, tmin, tmax); if (std::isnan(t)) return false; *s = plane_surface(r, t); *tri_out = -1; return true; }
+#define DFO_SIMPLE_SHAPE(ID, ARR, TF, SF)                       \
+    case ID: {                                                  \
+      const float* q = sc.F(ARR).data() + soff;                 \
+      const float t = TF(q, r, tmin, tmax);                     \
+      if (std::isnan(t)) return false;                          \
+      *s = SF(q, r, t); *tri_out = -1; return true;             \
+    }
+    DFO_SIMPLE_SHAPE(kShapeDisk, "shape3FDisk3FArray", disk_t, disk_surface)
+    DFO_SIMPLE_SHAPE(kShapeCylinder, "shape3FCylinder3FArray", cylinder_t, cylinder_surface)
+    DFO_SIMPLE_SHAPE(kShapeCone, "shape3FCone3FArray", cone_t, cone_surface)
+    DFO_SIMPLE_SHAPE(kShapeParaboloid, "shape3FParaboloid3FArray", paraboloid_t, paraboloid_surface)
+    DFO_SIMPLE_SHAPE(kShapeHyperboloid, "shape3FHyperboloid3FArray", hyperboloid_t, hyperboloid_surface)
+    DFO_SIMPLE_SHAPE(kShapeCuboid, "shape3FRectangularCuboid3FArray", cuboid_t, cuboid_surface)
+    DFO_SIMPLE_SHAPE(kShapeTorus, "shape3FTorus3FArray", torus_t, torus_surface)
+#undef DFO_SIMPLE_SHAPE
     default: return false;
   }
 }
@@ -1492,6 +1808,17 @@ int dfo_scene_commit(void* s, int layout) {
   if ((int)mats.size() < sc->prim_count * 32) return -2;
   sc->o2w.resize(sc->prim_count); sc->w2o.resize(sc->prim_count);
   for (int p = 0; p < sc->prim_count; ++p) { sc->o2w[p] = load_m44(mats.data() + p * 32); sc->w2o[p] = load_m44(mats.data() + p * 32 + 16); }
+  // record-sized shapes: the offset must leave a whole record in its array
+  struct { int id; const char* arr; size_t len; } recs[] = {
+      {kShapeDisk, "shape3FDisk3FArray", 4}, {kShapeCylinder, "shape3FCylinder3FArray", 4}, {kShapeCone, "shape3FCone3FArray", 4},
+      {kShapeParaboloid, "shape3FParaboloid3FArray", 4}, {kShapeHyperboloid, "shape3FHyperboloid3FArray", 12},
+      {kShapeCuboid, "shape3FRectangularCuboid3FArray", 6}, {kShapeTorus, "shape3FTorus3FArray", 2},
+      {kShapeRectangle, "shape3FRectangle3FArray", 12}, {kShapeTriangle, "shape3FTriangle3FArray", 24}};
+  for (int p = 0; p < sc->prim_count; ++p) {
+    const int sid = sc->prims[p * 8 + 6], soff = sc->prims[p * 8 + 7];
+    for (const auto& rc : recs)
+      if (rc.id == sid && (soff < 0 || (size_t)soff + rc.len > sc->F(rc.arr).size())) return -4;
+  }
   sc->lights = sc->I("lightIDAndOffsetArray");
   const auto& cam = sc->F("cameraArray");
   if (cam.size() < 19) return -3;

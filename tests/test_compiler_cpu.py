@@ -114,3 +114,47 @@ def test_oracle_render_counts_and_guard(oracle):
     assert r["count"].max() <= 3 and r["count"].min() >= 0
     assert np.all(np.isfinite(r["sum"]))
     assert r["rays"] > 16 * 16 * 3
+
+
+def test_record_shapes_layout_and_oracle():
+    """Disk ... torus compile into their reference records (CompiledShape3FCache.to*3F)
+    and every one of them is hit by the oracle's primary rays."""
+    import numpy as np
+
+    from dayflower_b200.scene import generators as G
+    from dayflower_b200.scene import model as M
+    from dayflower_b200.scene.compiler import compile_scene
+    from oracle import dfo
+
+    cs = compile_scene(G.quadrics_scene(resolution=(64, 48)))
+    a = cs.arrays
+    assert a["shape3FDisk3FArray"].size == 4 and a["shape3FCylinder3FArray"].size == 8
+    assert a["shape3FCone3FArray"].size == 4 and a["shape3FCone3FArray"][3] == 0.0
+    assert a["shape3FHyperboloid3FArray"].size == 16 and a["shape3FRectangularCuboid3FArray"].size == 8
+    assert a["shape3FTorus3FArray"].tolist() == [0.35, 1.0, 0.25, 0.800000011920929] or np.allclose(a["shape3FTorus3FArray"], [0.35, 1.0, 0.25, 0.8])
+    assert np.float32(a["shape3FDisk3FArray"][0]) == np.float32(np.radians(300.0))
+    prims = a["primitiveArray"].reshape(-1, 8)
+    offsets = {int(sid): sorted(set(prims[prims[:, 6] == sid, 7].tolist())) for sid in np.unique(prims[:, 6])}
+    assert offsets[M.SHAPE_CYLINDER] == [0, 4] and offsets[M.SHAPE_TORUS] == [0, 2]
+    o = dfo.OracleScene(cs)
+    res = o.render(3, spp=1, threads=4)
+    hit = set(res["prim"].ravel().tolist())
+    record_prims = [i for i, p in enumerate(prims) if p[6] in (M.SHAPE_DISK, M.SHAPE_CYLINDER, M.SHAPE_CONE, M.SHAPE_PARABOLOID,
+                                                             M.SHAPE_HYPERBOLOID, M.SHAPE_CUBOID, M.SHAPE_TORUS)]
+    assert len(record_prims) == 9
+    assert set(record_prims) <= hit
+
+
+def test_hyperboloid_coefficients_match_reference_constructor():
+    """Hyperboloid3F(phiMax, a, b) solves aH and cH so that b and c = a + 2 (b - a)
+    (the constructor's first probe point) lie on aH (x^2 + y^2) - cH z^2 = 1
+    (Hyperboloid3F.java:144-178)."""
+    import numpy as np
+
+    from dayflower_b200.scene import model as M
+
+    h = M.Hyperboloid(360.0, (0.3, 0.3, 0.0), (1.0, 0.2, 2.0))
+    c = h.a + 2.0 * (h.b - h.a)
+    for p in (h.b, c):
+        assert abs(h.aH * (p[0] ** 2 + p[1] ** 2) - h.cH * p[2] ** 2 - 1.0) < 1e-4
+    assert h.z_min == 0.0 and h.z_max == 2.0 and np.isclose(h.r_max, np.sqrt(1.04))
