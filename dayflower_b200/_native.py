@@ -45,6 +45,27 @@ SIGNATURES = [
     ("dfc_read_counters", _c_int, [_c_p, _c_p]),
     ("dfc_read_stage_times", _c_int, [_c_p, _c_p]),
     ("dfc_trace_rays_noalloc", _c_int, [_c_p, _c_p, _c_p, _c_p, _c_i64]),
+    # batch and serving engine
+    ("dfc_engine_create", _c_int, [_c_int, _c_i64, ctypes.POINTER(_c_p)]),
+    ("dfc_engine_destroy", _c_int, [_c_p]),
+    ("dfc_engine_last_error", ctypes.c_char_p, [_c_p]),
+    ("dfc_engine_scene_put", _c_int, [_c_p, ctypes.c_char_p, _c_p, _c_i64, _c_int]),
+    ("dfc_engine_scene_commit", _c_int, [_c_p, _c_int, ctypes.POINTER(ctypes.c_int32)]),
+    ("dfc_engine_scene_release", _c_int, [_c_p, ctypes.c_int32]),
+    ("dfc_engine_configure", _c_int, [_c_p, _c_p]),
+    ("dfc_engine_get_config", _c_int, [_c_p, _c_p]),
+    ("dfc_engine_autotune", _c_int, [_c_p, _c_p, _c_int, ctypes.c_char_p, ctypes.c_char_p, _c_p]),
+    ("dfc_job_submit", _c_int, [_c_p, _c_p, ctypes.POINTER(_c_i64)]),
+    ("dfc_job_get_info", _c_int, [_c_p, _c_i64, _c_p]),
+    ("dfc_job_wait", _c_int, [_c_p, _c_i64, ctypes.c_double]),
+    ("dfc_job_cancel", _c_int, [_c_p, _c_i64]),
+    ("dfc_job_read_film", _c_int, [_c_p, _c_i64, _c_p, _c_i64]),
+    ("dfc_job_read_image_rgba8", _c_int, [_c_p, _c_i64, _c_int, _c_p, _c_i64]),
+    ("dfc_job_release", _c_int, [_c_p, _c_i64]),
+    ("dfc_engine_run", _c_int, [_c_p, ctypes.c_double]),
+    ("dfc_engine_start", _c_int, [_c_p]),
+    ("dfc_engine_stop", _c_int, [_c_p]),
+    ("dfc_engine_get_stats", _c_int, [_c_p, _c_p]),
 ]
 
 

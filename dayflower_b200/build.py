@@ -7,6 +7,7 @@ Each library is rebuilt only when one of its sources is newer than it.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -17,8 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 ROOT = os.path.dirname(HERE)
 
-CUDA_SOURCES = ["dfc_api.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp"]
-CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h"]
+CUDA_SOURCES = ["dfc_api.cu", "dfc_engine.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp", "dfc_devscene.cpp"]
+CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h", "dfc_devscene.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -59,8 +60,7 @@ def build_cuda(force: bool = False, verbose: bool = False, extra=()) -> str:
         return out
     obj_dir = os.path.join(LIB, "_obj")
     os.makedirs(obj_dir, exist_ok=True)
-    objs = []
-    for s in CUDA_SOURCES:
+    def compile_one(s):
         o = os.path.join(obj_dir, s + ".o")
         # -fmad=false: every float operation is rounded on its own, as in the
         # reference (Java float arithmetic has no contraction); the traversal's
@@ -69,10 +69,15 @@ def build_cuda(force: bool = False, verbose: bool = False, extra=()) -> str:
                "-Xptxas", "-O3", "--expt-relaxed-constexpr", "-fmad=false"] + GENCODE + list(extra)
         if verbose and s.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
-        log = _run(cmd)
-        if verbose:
+        return o, _run(cmd)
+
+    # the sources compile independently: one nvcc process each
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(CUDA_SOURCES), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, CUDA_SOURCES))
+    objs = [o for o, _ in results]
+    if verbose:
+        for _, log in results:
             sys.stdout.write(log)
-        objs.append(o)
     _run([_nvcc(), "-shared", "-o", out] + objs + GENCODE + ["-cudart", "static"])
     return out
 

@@ -17,29 +17,11 @@
 #include <vector>
 
 #include "../../include/dayflower_cuda.h"
+#include "dfc_devscene.h"
 #include "dfc_ingest.h"
 #include "dfc_kernels.h"
 
 using namespace dfc;
-
-namespace {
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DevBuf() { release(); }
-  void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
-  cudaError_t ensure(size_t n) {
-    if (n <= bytes && p) return cudaSuccess;
-    release();
-    cudaError_t e = cudaMalloc(&p, n ? n : 16);
-    if (e == cudaSuccess) bytes = n;
-    return e;
-  }
-  template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
-}  // namespace
 
 struct dfc_renderer {
   int device = 0;
@@ -58,10 +40,7 @@ struct dfc_renderer {
   // scene
   Staged staged;
   bool have_scene = false;
-  HostScene host;
-  DevBuf d_prims, d_mats, d_lights, d_nodes, d_tlas_items, d_tlas_bound, d_unbounded, d_tri_pos, d_tri_attr, d_rects, d_perez, d_camera;
-  DevBuf d_shapes;
-  SceneView view{};
+  DeviceScene scene;
   // film and wavefront
   bool set_up = false;
   unsigned pixels = 0, paths = 0;
@@ -96,13 +75,6 @@ int cuda_fail(dfc_renderer* r, cudaError_t e, const char* what) {
     cudaError_t e_ = (expr);                           \
     if (e_ != cudaSuccess) return cuda_fail(r, e_, what); \
   } while (0)
-
-template <typename T>
-cudaError_t upload(dfc_renderer* r, DevBuf& b, const std::vector<T>& v) {
-  cudaError_t e = b.ensure(v.size() * sizeof(T));
-  if (e != cudaSuccess) return e;
-  return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, r->stream);
-}
 
 __global__ void k_sum_counts(const unsigned* counts, int steps, unsigned long long* total) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -183,7 +155,7 @@ int clear_film(dfc_renderer* r) {
 
 ShadeArgs shade_args(dfc_renderer* r, int step) {
   ShadeArgs a{};
-  a.scene = r->view;
+  a.scene = r->scene.view;
   a.paths = r->paths;
   a.pixels = r->pixels;
   a.max_bounce = r->max_bounce;
@@ -219,11 +191,11 @@ ShadeArgs shade_args(dfc_renderer* r, int step) {
 // The traversal kernel for the committed scene: the one with the disk ... torus
 // tests only when the scene has such primitives.
 using TraceKernel = void (*)(TraceArgs);
-TraceKernel trace_kernel(const dfc_renderer* r) { return r->host.record_shapes ? k_trace_records : k_trace; }
+TraceKernel trace_kernel(const dfc_renderer* r) { return r->scene.host.record_shapes ? k_trace_records : k_trace; }
 
 TraceArgs trace_args(dfc_renderer* r, int step) {
   TraceArgs t{};
-  t.scene = r->view;
+  t.scene = r->scene.view;
   unsigned* counts = r->d_counts.as<unsigned>();
   t.ray_list = r->d_ray_list[step & 1].as<unsigned>();
   t.ray_count = counts + 4 * step;
@@ -245,7 +217,7 @@ int enqueue_pass(dfc_renderer* r) {
   DFC_CK(cudaMemsetAsync(r->d_counts.p, 0, counts_bytes, r->stream), "counters");
   unsigned* counts = r->d_counts.as<unsigned>();
   RaygenArgs g{};
-  g.scene = r->view;
+  g.scene = r->scene.view;
   g.paths = r->paths;
   g.pixels = r->pixels;
   g.width = (unsigned)r->width;
@@ -277,7 +249,7 @@ int enqueue_pass(dfc_renderer* r) {
       ShadeArgs a = shade_args(r, s);
       a.last_step = s == steps - 1;
       SortArgs so{};
-      so.scene = r->view;
+      so.scene = r->scene.view;
       so.paths = r->paths;
       so.work_list = a.work_list;
       so.work_count = a.work_count;
@@ -290,7 +262,7 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
       a.work_list = so.sorted;
-      (r->host.record_shapes ? k_shade_path_records : k_shade_path)<<<shade_grid, 256, 0, r->stream>>>(a);
+      (r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)<<<shade_grid, 256, 0, r->stream>>>(a);
       stage_end(r, ev);
       r->launches += 4;
     }
@@ -302,7 +274,7 @@ int enqueue_pass(dfc_renderer* r) {
     r->launches += 2;
     if (kind == DFC_ALGO_AO) {
       AoArgs o{};
-      o.scene = r->view;
+      o.scene = r->scene.view;
       o.paths = r->paths;
       o.samples = r->ao_samples;
       o.max_distance = r->max_distance;
@@ -400,46 +372,12 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   std::string err;
   int rc = ingest_scene(r->staged, layout_version, &hs, &err);
   if (rc != DFC_OK) return fail(r, rc, err);
-  DFC_CK(cudaStreamSynchronize(r->stream), "sync");
-  DFC_CK(upload(r, r->d_prims, hs.prims), "scene upload");
-  DFC_CK(upload(r, r->d_mats, hs.materials), "scene upload");
-  DFC_CK(upload(r, r->d_lights, hs.lights), "scene upload");
-  DFC_CK(upload(r, r->d_nodes, hs.nodes), "scene upload");
-  DFC_CK(upload(r, r->d_tlas_items, hs.tlas_items), "scene upload");
-  DFC_CK(upload(r, r->d_tlas_bound, hs.tlas_bound), "scene upload");
-  DFC_CK(upload(r, r->d_unbounded, hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded), "scene upload");
-  DFC_CK(upload(r, r->d_tri_pos, hs.tri_pos), "scene upload");
-  DFC_CK(upload(r, r->d_tri_attr, hs.tri_attr), "scene upload");
-  DFC_CK(upload(r, r->d_rects, hs.rects), "scene upload");
-  DFC_CK(upload(r, r->d_shapes, hs.shapes), "scene upload");
-  DFC_CK(upload(r, r->d_perez, hs.perez), "scene upload");
-  std::vector<float> cam(hs.camera, hs.camera + 19);
-  DFC_CK(upload(r, r->d_camera, cam), "scene upload");
-  DFC_CK(cudaStreamSynchronize(r->stream), "sync");
-  SceneView& v = r->view;
-  v.prims = r->d_prims.as<DPrim>();
-  v.prim_count = (int)hs.prims.size();
-  v.materials = r->d_mats.as<DMaterial>();
-  v.lights = r->d_lights.as<DLight>();
-  v.light_count = hs.lights_storage_pad ? 0 : (int)hs.lights.size();
-  v.nodes = r->d_nodes.as<BVH4Node>();
-  v.tlas_root = hs.tlas_root;
-  v.tlas_items = r->d_tlas_items.as<int>();
-  v.tlas_bound = r->d_tlas_bound.as<F4>();
-  v.unbounded = r->d_unbounded.as<int>();
-  v.unbounded_count = (int)hs.unbounded.size();
-  v.tri_pos = r->d_tri_pos.as<F4>();
-  v.tri_attr = r->d_tri_attr.as<float>();
-  v.rects = r->d_rects.as<float>();
-  v.shapes = r->d_shapes.as<float>();
-  v.perez = r->d_perez.as<float>();
-  v.camera = r->d_camera.as<float>();
-  r->host = std::move(hs);
+  DFC_CK(upload_scene(std::move(hs), r->stream, &r->scene), "scene upload");
   r->have_scene = true;
   r->staged = Staged();
   if (r->image_from_camera) {
-    r->width = (int)r->host.camera[17];
-    r->height = (int)r->host.camera[18];
+    r->width = (int)r->scene.host.camera[17];
+    r->height = (int)r->scene.host.camera[18];
   }
   r->set_up = false;
   return DFC_OK;
@@ -450,7 +388,7 @@ int dfc_set_image(dfc_renderer* r, int width, int height) {
   std::lock_guard<std::mutex> lk(r->mu);
   if (width == 0 && height == 0) {
     r->image_from_camera = 1;
-    if (r->have_scene) { r->width = (int)r->host.camera[17]; r->height = (int)r->host.camera[18]; }
+    if (r->have_scene) { r->width = (int)r->scene.host.camera[17]; r->height = (int)r->scene.host.camera[18]; }
   } else {
     if (width < 1 || height < 1 || (int64_t)width * height > (1LL << 27)) return fail(r, DFC_E_INVALID_ARG, "resolution out of range");
     r->image_from_camera = 0;
@@ -567,8 +505,8 @@ int dfc_update_camera(dfc_renderer* r, const float* camera19) {
   if (!valid(r) || !camera19) return fail(r, DFC_E_INVALID_ARG, "camera == null");
   std::lock_guard<std::mutex> lk(r->mu);
   if (!r->have_scene) return fail(r, DFC_E_STATE, "updateCamera() before setScene()");
-  std::memcpy(r->host.camera, camera19, 19 * sizeof(float));
-  DFC_CK(cudaMemcpyAsync(r->d_camera.p, camera19, 19 * sizeof(float), cudaMemcpyHostToDevice, r->stream), "camera");
+  std::memcpy(r->scene.host.camera, camera19, 19 * sizeof(float));
+  DFC_CK(cudaMemcpyAsync(r->scene.camera.p, camera19, 19 * sizeof(float), cudaMemcpyHostToDevice, r->stream), "camera");
   DFC_CK(cudaStreamSynchronize(r->stream), "camera");
   return DFC_OK;
 }
@@ -577,11 +515,11 @@ int dfc_update_matrices(dfc_renderer* r, const float* m, int64_t n) {
   if (!valid(r) || !m) return fail(r, DFC_E_INVALID_ARG, "matrices == null");
   std::lock_guard<std::mutex> lk(r->mu);
   if (!r->have_scene) return fail(r, DFC_E_STATE, "updateMatrix44Fs() before setScene()");
-  if (n != (int64_t)r->host.prims.size()) return fail(r, DFC_E_INVALID_ARG, "matrix count differs from the primitive count");
+  if (n != (int64_t)r->scene.host.prims.size()) return fail(r, DFC_E_INVALID_ARG, "matrix count differs from the primitive count");
   // The top level is built over compiled bounding volumes; moving primitives
   // requires a new setScene so that the hierarchy sees their new boxes.
   for (int64_t p = 0; p < n; ++p) {
-    DPrim& pr = r->host.prims[p];
+    DPrim& pr = r->scene.host.prims[p];
     const float* q = m + p * 32;
     std::memcpy(pr.o2w, q, 12 * sizeof(float));
     std::memcpy(pr.w2o, q + 16, 12 * sizeof(float));
@@ -589,9 +527,8 @@ int dfc_update_matrices(dfc_renderer* r, const float* m, int64_t n) {
     for (int k = 0; k < 16; ++k) id = id && q[k] == ((k % 5) == 0 ? 1.0f : 0.0f) && q[16 + k] == ((k % 5) == 0 ? 1.0f : 0.0f);
     pr.identity = id;
   }
-  DFC_CK(upload(r, r->d_prims, r->host.prims), "matrices");
+  DFC_CK(cudaMemcpyAsync(r->scene.prims.p, r->scene.host.prims.data(), n * sizeof(DPrim), cudaMemcpyHostToDevice, r->stream), "matrices");
   DFC_CK(cudaStreamSynchronize(r->stream), "matrices");
-  r->view.prims = r->d_prims.as<DPrim>();
   return DFC_OK;
 }
 
@@ -745,7 +682,7 @@ extern "C" int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, c
   const unsigned n = (unsigned)count;
   k_noalloc_prepare<<<(n + 255u) / 256u, 256, 0, r->stream>>>(scratch, n);
   TraceArgs t{};
-  t.scene = r->view;
+  t.scene = r->scene.view;
   t.ray_list = scratch + kNoAllocHeader;
   t.ray_count = scratch;
   t.fetch = scratch + 1;

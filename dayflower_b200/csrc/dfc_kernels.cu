@@ -405,7 +405,15 @@ constexpr bool kSpeculate = DFC_SPECULATE != 0;  // lanes holding a leaf keep wa
 #ifndef DFC_TRACE_MIN_BLOCKS
 #define DFC_TRACE_MIN_BLOCKS 6
 #endif
-template <bool kRecords>
+// The scene a kernel works on: the launch's own (per-job renderer) or, in
+// the batch engine, the table entry of the ray's or path's job.
+template <bool kMulti, typename Args>
+DFC_D const SceneView& scene_at(const Args& a, int si) {
+  if constexpr (kMulti) return a.scenes[si];
+  else return a.scene;
+}
+
+template <bool kRecords, bool kMulti>
 __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
   __shared__ int stack_smem[kStack * kTraceBlock];
   int* stack = stack_smem + threadIdx.x;
@@ -415,6 +423,7 @@ __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
   T.sp = 0;
   unsigned cur = kNoRay;
   unsigned slot = 0;
+  int si = 0;  // scene of this lane's ray (batch engine)
   int lf_first = 0, lf_cnt = 0;
   bool pool_empty = false;  // warp-uniform
   while (true) {
@@ -433,8 +442,9 @@ __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
           const unsigned ref = a.ray_list[i];
           const unsigned p = ref >> 3, type = ref & 3u;
           slot = type * a.paths + p;
+          if constexpr (kMulti) si = a.jobs[a.slot_job[p]].scene;
           const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
-          trav_init<kRecords>(a.scene, T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
+          trav_init<kRecords>(scene_at<kMulti>(a, si), T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
           lf_cnt = 0;
         }
       }
@@ -446,11 +456,12 @@ __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
     for (int k = 0; k < kNodeSteps; ++k) {
       const bool searching = act && T.sp > 0 && lf_cnt == 0;
       if (!__any_sync(0xffffffffu, searching)) break;
-      if (kSpeculate ? (act && T.sp > 0 && !blocked) : searching) blocked = node_step(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
+      if (kSpeculate ? (act && T.sp > 0 && !blocked) : searching)
+        blocked = node_step(scene_at<kMulti>(a, si), T, stack, a.overflow, lf_first, lf_cnt);
     }
     // leaf phase
     while (__any_sync(0xffffffffu, lf_cnt > 0)) {
-      if (lf_cnt > 0) leaf_step<kRecords>(a.scene, T, stack, a.overflow, lf_first, lf_cnt);
+      if (lf_cnt > 0) leaf_step<kRecords>(scene_at<kMulti>(a, si), T, stack, a.overflow, lf_first, lf_cnt);
     }
     if (act && T.sp == 0) {
       a.hits[slot] = make_float4(T.cbest, __int_as_float(T.prim), __int_as_float(T.aux), T.t_obj);
@@ -459,8 +470,10 @@ __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
   }
 }
 
-__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) { trace_rays<false>(a); }
-__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace_records(TraceArgs a) { trace_rays<true>(a); }
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace(TraceArgs a) { trace_rays<false, false>(a); }
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace_records(TraceArgs a) { trace_rays<true, false>(a); }
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace_batch(TraceArgs a) { trace_rays<false, true>(a); }
+__global__ void __launch_bounds__(kTraceBlock, DFC_TRACE_MIN_BLOCKS) k_trace_batch_records(TraceArgs a) { trace_rays<true, true>(a); }
 
 __global__ void k_raygen(RaygenArgs a) {
   // No early return: every lane of the warp takes part in warp_append's ballot.
@@ -543,27 +556,36 @@ DFC_D float area_light_pdf(const SceneView& S, const DLight& lt, V3 p, V3 wi) {
   return 0.0f;
 }
 
-DFC_D void film_add(const ShadeArgs& a, unsigned pix, V3 L) {
+DFC_D void film_add_to(float4* film_sum, float4* film_sq, unsigned pix, V3 L) {
   if (!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z))) return;  // AbstractCPURenderer.java:231
   if (luminance(L) < -1.0e-5f) return;
-  float* f = reinterpret_cast<float*>(a.film_sum + pix);
+  float* f = reinterpret_cast<float*>(film_sum + pix);
   atomicAdd(f + 0, L.x); atomicAdd(f + 1, L.y); atomicAdd(f + 2, L.z); atomicAdd(f + 3, 1.0f);
-  float* g = reinterpret_cast<float*>(a.film_sq + pix);
+  float* g = reinterpret_cast<float*>(film_sq + pix);
   atomicAdd(g + 0, L.x * L.x); atomicAdd(g + 1, L.y * L.y); atomicAdd(g + 2, L.z * L.z);
 }
+DFC_D void film_add(const ShadeArgs& a, unsigned pix, V3 L) { film_add_to(a.film_sum, a.film_sq, pix, L); }
 
-// One shade step of the path tracer for every path on the work list.
-template <bool kRecords>
+// One shade step of the path tracer for every path on the work list.  In
+// the batch engine (kMulti) the scene, film and bounce limits come from the
+// path's job, a path ends at its own step max_bounce + 3 (the step count of
+// a render pass of the per-job renderer), and a retired path's slot goes back
+// on the free stack.
+template <bool kRecords, bool kMulti>
 __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
   const unsigned n = *a.work_count;
   const unsigned stride = gridDim.x * blockDim.x;
-  const SceneView& S = a.scene;
   for (unsigned base = blockIdx.x * blockDim.x; base < n; base += stride) {
     const unsigned i = base + threadIdx.x;
-    bool spawn_ext = false, spawn_shadow = false, spawn_mis = false, keep = false, shadow_any = false;
-    unsigned p = 0;
+    bool spawn_ext = false, spawn_shadow = false, spawn_mis = false, keep = false, shadow_any = false, retire = false;
+    unsigned p = 0, job = 0;
     if (i < n) {
       p = a.work_list[i];
+      const DJob* J = nullptr;
+      if constexpr (kMulti) { job = a.slot_job[p]; J = a.jobs + job; }
+      const SceneView& S = scene_at<kMulti>(a, kMulti ? J->scene : 0);
+      const int max_bounce = kMulti ? J->max_bounce : a.max_bounce;
+      const int min_rr = kMulti ? J->min_rr : a.min_rr;
       uint4 meta = a.meta[p];
       float4 b4 = a.beta[p];
       float4 l4 = a.radiance[p];
@@ -606,16 +628,18 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
       }
       flags &= ~(kPendShadow | kPendMis | kShadowAny);
       bool alive = (flags & kAlive) != 0u;
+      const int step = (int)l4.w;  // shade steps this path has had
+      const bool last_step = kMulti ? step >= max_bounce + 3 : a.last_step != 0;
       if (alive) {
         const float4 h = a.hits[p];
         const float4 ro = a.ray_o[p], rd = a.ray_d[p];
         const V3 ray_o = {ro.x, ro.y, ro.z}, ray_d = {rd.x, rd.y, rd.z};
         const int hp = __float_as_int(h.y);
         const bool spec = (flags & kFlagSpecular) != 0u;
-        const bool rec = a.record_primary && bounce == 0 && dimb == 0 && p < a.pixels;
+        const bool rec = !kMulti && a.record_primary && bounce == 0 && dimb == 0 && p < a.pixels;
         if (rec && hp < 0) { a.primary_prim[p] = -1; a.primary_t[p] = __int_as_float(0x7fc00000); }
         if (hp < 0) {
-          if (bounce == 0 && a.preview) L = {1, 1, 1};
+          if (bounce == 0 && !kMulti && a.preview) L = {1, 1, 1};
           else if (bounce == 0 || spec) {
             for (int k = 0; k < S.light_count; ++k) L = L + mul(beta, light_Le_miss(S, S.lights[k], ray_d));
           }
@@ -637,7 +661,7 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
             }
             L = L + mul(beta, Le);
           }
-          if (bounce >= a.max_bounce) {
+          if (bounce >= max_bounce) {
             alive = false;
           } else {
             const DMaterial& m = S.materials[pr.material];
@@ -714,7 +738,7 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
                 a.ray_d[p] = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, kFltMax);
                 V3 rr = beta * eta_scale;
                 float mx = fmaxf(rr.x, fmaxf(rr.y, rr.z));
-                if (mx < 1.0f && bounce >= a.min_rr) {
+                if (mx < 1.0f && bounce >= min_rr) {
                   float q = fmaxf(0.05f, 1.0f - mx);
                   if (rng_uniform(key, bounce_dim(dimb, kDimRoulette)) < q) cont = false;
                   else beta = beta * (1.0f / (1.0f - q));
@@ -727,13 +751,17 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
         }
       }
       if (alive && !spawn_ext) alive = false;
-      if (a.last_step && alive) { alive = false; spawn_ext = false; }
+      if (last_step && alive) { alive = false; spawn_ext = false; }
       flags = alive ? (flags | kAlive) : (flags & ~kAlive);
       keep = alive || spawn_shadow || spawn_mis;
-      if (a.last_step) { keep = false; spawn_shadow = spawn_mis = false; }
-      if (!keep && !(flags & kNoSample)) film_add(a, meta.x, L);
+      if (last_step) { keep = false; spawn_shadow = spawn_mis = false; }
+      if (!keep && !(flags & kNoSample)) {
+        if constexpr (kMulti) film_add_to(J->film_sum, J->film_sq, meta.x, L);
+        else film_add(a, meta.x, L);
+      }
+      retire = kMulti && !keep;
       a.beta[p] = make_float4(beta.x, beta.y, beta.z, eta_scale);
-      a.radiance[p] = make_float4(L.x, L.y, L.z, 0.0f);
+      a.radiance[p] = make_float4(L.x, L.y, L.z, (float)(step + 1));
       a.meta[p] = make_uint4(meta.x, meta.y, ((unsigned)bounce & 0xffffu) | ((unsigned)dimb << 16), flags);
     }
     // appends (all lanes of the warp take part)
@@ -745,17 +773,30 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
     if (spawn_mis) a.next_ray_list[r2] = (p << 3) | 2u;
     const unsigned w = warp_append(a.next_work_count, keep);
     if (keep) a.next_work_list[w] = p;
+    if constexpr (kMulti) {
+      // retired slots back on the free stack; per-job retire counts, one atomic per job in the warp
+      const unsigned f = warp_append(a.free_top, retire);
+      if (retire) a.free_stack[f] = p;
+      const unsigned peers = __match_any_sync(0xffffffffu, retire ? job : 0xffffffffu);
+      const unsigned lane = threadIdx.x & 31u;
+      if (retire && (int)lane == __ffs(peers) - 1) atomicAdd(a.job_done + job, (unsigned long long)__popc(peers));
+      const unsigned rmask = __ballot_sync(0xffffffffu, retire);
+      if (lane == 0 && rmask) atomicAdd(&a.state->retired, (unsigned long long)__popc(rmask));
+    }
   }
 }
 
-__global__ void k_shade_path(ShadeArgs a) { shade_path<false>(a); }
-__global__ void k_shade_path_records(ShadeArgs a) { shade_path<true>(a); }
+__global__ void k_shade_path(ShadeArgs a) { shade_path<false, false>(a); }
+__global__ void k_shade_path_records(ShadeArgs a) { shade_path<true, false>(a); }
+__global__ void k_shade_path_batch(ShadeArgs a) { shade_path<false, true>(a); }
+__global__ void k_shade_path_batch_records(ShadeArgs a) { shade_path<true, true>(a); }
 
 // ---- material sort of the shade work list -----------------------------------
 // Shading diverges badly when one warp holds paths on different materials (each
 // material is a different BSDF routine), so the work list of every step is
 // counting-sorted by material kind before shading.
-__global__ void k_sort_count(SortArgs a) {
+template <bool kMulti>
+__device__ __forceinline__ void sort_count(const SortArgs& a) {
   __shared__ unsigned cnt[kSortBins];
   if (threadIdx.x < kSortBins) cnt[threadIdx.x] = 0;
   __syncthreads();
@@ -765,7 +806,8 @@ __global__ void k_sort_count(SortArgs a) {
     int key = kMatKinds + 1;
     if (a.meta[p].w & kFlagAlive) {
       const int hp = __float_as_int(a.hits[p].y);
-      key = hp < 0 ? kMatKinds : a.scene.materials[a.scene.prims[hp].material].kind;
+      const SceneView& S = scene_at<kMulti>(a, kMulti ? a.jobs[a.slot_job[p]].scene : 0);
+      key = hp < 0 ? kMatKinds : S.materials[S.prims[hp].material].kind;
     }
     a.keys[i] = (unsigned char)key;
     atomicAdd(&cnt[key], 1u);
@@ -773,6 +815,8 @@ __global__ void k_sort_count(SortArgs a) {
   __syncthreads();
   if (threadIdx.x < kSortBins && cnt[threadIdx.x]) atomicAdd(&a.bins[threadIdx.x], cnt[threadIdx.x]);
 }
+__global__ void k_sort_count(SortArgs a) { sort_count<false>(a); }
+__global__ void k_sort_count_batch(SortArgs a) { sort_count<true>(a); }
 
 __global__ void k_sort_scatter(SortArgs a) {
   __shared__ unsigned start[kSortBins];
@@ -913,6 +957,102 @@ __global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_map
     return (unsigned char)(clampf(v, 0.0f, 1.0f) * 255.0f + 0.5f);
   };
   out[i] = make_uchar4(enc(c.x), enc(c.y), enc(c.z), 255);
+}
+
+// ---- batch engine: path slots refilled every iteration ------------------------
+// The engine keeps `capacity` path slots.  Retired slots go on a free stack
+// (shade pushes them); each iteration's plan takes as many as there are
+// unstarted paths of admitted jobs, and regen starts those paths in them, so
+// new jobs join the running wavefront at every bounce iteration.
+
+__global__ void k_batch_init(BatchArgs a) {
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < a.capacity; i += stride) a.free_stack[i] = a.capacity - 1u - i;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.state->free_top = a.capacity;
+}
+
+// Job ring index of the admitted job that owns global path index g.
+DFC_D unsigned job_of(const BatchArgs& a, unsigned long long g) {
+  unsigned lo = a.ctl->job_lo, hi = a.ctl->job_hi;
+  while (hi - lo > 1u) {
+    const unsigned mid = lo + (hi - lo) / 2u;
+    if (a.jobs[mid & a.job_mask].start <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo & a.job_mask;
+}
+
+// One thread: the previous iteration's counters are final (its rays are
+// added up, then they are zeroed for the lists this iteration's shade fills),
+// the unstarted paths of cancelled jobs at the cursor are skipped (counted as
+// done), and the number of paths to start is fixed for regen.
+__global__ void k_batch_plan(BatchArgs a) {
+  if (threadIdx.x < 2 * kSortBins) a.sort_bins[threadIdx.x] = 0u;
+  if (threadIdx.x != 0) return;
+  BatchState* st = a.state;
+  st->rays += a.counts_next[0];
+  a.counts_next[0] = 0u;
+  a.counts_next[1] = 0u;
+  a.counts_next[2] = 0u;
+  const unsigned long long admitted = a.ctl->admitted;
+  for (int guard = 0; guard < 16 && st->cursor < admitted; ++guard) {
+    const unsigned jr = job_of(a, st->cursor);
+    const DJob& J = a.jobs[jr];
+    if (!J.cancelled) break;
+    const unsigned long long end = J.start + J.paths;
+    a.job_done[jr] += end - st->cursor;
+    st->cursor = end;
+  }
+  const unsigned long long rem = admitted - st->cursor;
+  const unsigned top = st->free_top;
+  const unsigned k = rem < (unsigned long long)top ? (unsigned)rem : top;
+  st->regen_k = k;
+  st->regen_base = top - k;
+  st->regen_cursor = st->cursor;
+  st->free_top = top - k;
+  st->cursor += k;
+  st->iterations += 1u;
+}
+
+// Starts the planned paths: global path index -> job (binary search over the
+// admitted window by first path index) -> pixel and sample -> camera ray, in
+// the same form as k_raygen so that a job's samples are those the per-job
+// renderer draws for the same seed.
+__global__ void k_batch_regen(BatchArgs a) {
+  const BatchState* st = a.state;
+  const unsigned k = st->regen_k, sbase = st->regen_base;
+  const unsigned long long g0 = st->regen_cursor;
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < k; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool ok = false, valid = i < k;
+    unsigned slot = 0;
+    if (valid) {
+      slot = a.free_stack[sbase + i];
+      const unsigned long long g = g0 + i;
+      const unsigned jr = job_of(a, g);
+      const DJob& J = a.jobs[jr];
+      const unsigned long long q = g - J.start;
+      const unsigned pix = (unsigned)(q % J.pixels);
+      const unsigned sample = (unsigned)(q / J.pixels);
+      const unsigned x = pix % J.width, y = pix / J.width;
+      const uint32_t key = rng_path_key(J.seed, pix, sample);
+      V3 o = {0, 0, 0}, d = {0, 0, 1};
+      if (!J.cancelled)
+        ok = camera_ray(J.camera, (float)x, (float)y, rng_uniform(key, kDimPixelX), rng_uniform(key, kDimPixelY),
+                        rng_uniform(key, kDimLensU), rng_uniform(key, kDimLensV), &o, &d);
+      a.slot_job[slot] = jr;
+      a.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+      a.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      a.meta[slot] = make_uint4(pix, key, 0u, ok ? kAlive : kNoSample);
+      a.ray_o[slot] = make_float4(o.x, o.y, o.z, kTMin);
+      a.ray_d[slot] = make_float4(d.x, d.y, d.z, kFltMax);
+    }
+    const unsigned r = warp_append(a.counts_cur + 0, ok);
+    if (ok) a.ray_list[r] = slot << 3;
+    const unsigned w = warp_append(a.counts_cur + 1, valid);
+    if (valid) a.work_list[w] = slot;
+  }
 }
 
 }  // namespace dfc

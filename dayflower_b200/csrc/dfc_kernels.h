@@ -12,8 +12,49 @@ enum { DFC_ALGO_AO = 0, DFC_ALGO_DEPTH = 1, DFC_ALGO_PATH = 2, DFC_ALGO_RAY_CAST
 // Path flags (PathMeta.w)
 enum : unsigned { kFlagAlive = 1u, kFlagSpecular = 2u, kFlagPendShadow = 4u, kFlagPendMis = 8u, kFlagShadowAny = 16u, kFlagNoSample = 32u };
 
+// One render job of the batch/serving engine as the kernels read it.  Jobs
+// live in a ring of power-of-two capacity indexed by sequence number & mask;
+// the paths of all admitted jobs form one global sequence in which job j owns
+// [start, start + paths), sample-major (path q of the job is pixel q % pixels
+// of sample q / pixels).
+struct DJob {
+  float camera[19];          // the scene's compiled camera with the job's resolution in [17], [18]
+  int scene;                 // index into the engine's scene table
+  unsigned width, pixels;
+  int max_bounce, min_rr;
+  uint32_t seed;
+  unsigned cancelled;        // 1: hand out no more paths of this job (they retire unsampled)
+  unsigned long long start;  // first global path index
+  unsigned long long paths;  // pixels * samples
+  float4* film_sum;          // per pixel: sum of accepted samples (xyz), count (w)
+  float4* film_sq;           // per pixel: sum of squares (xyz)
+};
+
+// Words the host writes between wavefront iterations (stream-ordered copies).
+struct BatchControl {
+  unsigned long long admitted;  // total paths of all admitted jobs
+  unsigned job_lo, job_hi;      // sequence numbers of the jobs that may still hand out paths
+};
+
+// Words the wavefront iterations keep on the device.
+struct BatchState {
+  unsigned long long cursor;    // next global path index to hand out
+  unsigned long long rays;      // rays traced (all iterations)
+  unsigned long long retired;   // paths retired
+  unsigned free_top;            // slots on the free stack
+  unsigned regen_k;             // plan -> regen: paths to start this iteration
+  unsigned regen_base;          //                first free-stack entry they take
+  unsigned iterations;
+  unsigned long long regen_cursor;  //            global index of the first of them
+};
+
 struct TraceArgs {
   SceneView scene;
+  // batch engine only: per-slot job, job ring and scene table (the scene of
+  // a ray is scenes[jobs[slot_job[slot]].scene])
+  const SceneView* scenes;
+  const DJob* jobs;
+  const unsigned* slot_job;
   const unsigned* ray_list;
   const unsigned* ray_count;
   const float4* ray_o;  // 3 slots per path: [type * paths + p]
@@ -41,6 +82,14 @@ struct RaygenArgs {
 
 struct ShadeArgs {
   SceneView scene;
+  // batch engine only (see TraceArgs); retired slots go back on the free stack
+  const SceneView* scenes;
+  const DJob* jobs;
+  const unsigned* slot_job;
+  unsigned* free_stack;
+  unsigned* free_top;
+  unsigned long long* job_done;  // per job ring entry: paths retired
+  BatchState* state;
   unsigned paths, pixels;
   int max_bounce, min_rr, preview, last_step, record_primary, ao_samples;
   const unsigned* work_list;
@@ -83,6 +132,9 @@ struct AoArgs {
 constexpr int kSortBins = kMatKinds + 2;
 struct SortArgs {
   SceneView scene;
+  const SceneView* scenes;  // batch engine only (see TraceArgs)
+  const DJob* jobs;
+  const unsigned* slot_job;
   unsigned paths;
   const unsigned* work_list;
   const unsigned* work_count;
@@ -93,7 +145,35 @@ struct SortArgs {
   unsigned* sorted;        // the work list in key order
 };
 __global__ void k_sort_count(SortArgs a);
+__global__ void k_sort_count_batch(SortArgs a);
 __global__ void k_sort_scatter(SortArgs a);
+
+// Batch engine: one wavefront iteration is
+//   plan -> regen -> trace -> sort count -> sort scatter -> shade
+// with the lists and counters of parity (iteration & 1).
+struct BatchArgs {
+  const DJob* jobs;
+  unsigned job_mask;
+  const BatchControl* ctl;
+  BatchState* state;
+  unsigned long long* job_done;  // per job ring entry: paths retired (or skipped by a cancel)
+  unsigned* free_stack;
+  unsigned* slot_job;
+  unsigned capacity;
+  unsigned* counts_cur;    // {ray count, work count, fetch, -} of this iteration
+  unsigned* counts_next;   // of the next one (zeroed by plan)
+  unsigned* sort_bins;     // 2 * kSortBins of this iteration (zeroed by plan)
+  float4* beta;
+  float4* radiance;
+  uint4* meta;
+  float4* ray_o;
+  float4* ray_d;
+  unsigned* ray_list;      // of this iteration
+  unsigned* work_list;
+};
+__global__ void k_batch_init(BatchArgs a);
+__global__ void k_batch_plan(BatchArgs a);
+__global__ void k_batch_regen(BatchArgs a);
 
 __global__ void k_raygen(RaygenArgs a);
 // Closest/any hit of the listed rays.  k_trace_records also tests disk,
@@ -101,8 +181,12 @@ __global__ void k_raygen(RaygenArgs a);
 // it when the scene has any (SceneView has no flag for it: the host knows).
 __global__ void k_trace(TraceArgs a);
 __global__ void k_trace_records(TraceArgs a);
+__global__ void k_trace_batch(TraceArgs a);          // batch engine: scene per ray from the job table
+__global__ void k_trace_batch_records(TraceArgs a);
 __global__ void k_shade_path(ShadeArgs a);
 __global__ void k_shade_path_records(ShadeArgs a);  // with the disk ... torus surfaces
+__global__ void k_shade_path_batch(ShadeArgs a);     // batch engine: scene, film and limits per path from the job table
+__global__ void k_shade_path_batch_records(ShadeArgs a);
 __global__ void k_shade_primary(ShadeArgs a, int algorithm);
 __global__ void k_trace_ao(AoArgs a);
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);

@@ -206,3 +206,55 @@ def quadrics_scene(resolution=(128, 96), with_lights=True) -> M.Scene:
         sc.lights.append(sl)
         sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((-4.0, 7.0, 4.0), 0.8), area_light=sl))
     return sc
+
+
+# ---- batched-job mix: eight seeded scenes and a job list over them --------------
+# Sphere counts 10 .. 10k and heightfield sizes 10k .. 2M triangles, each spaced
+# evenly in log scale over the eight scenes and paired in a shuffled order.
+JOB_MIX_SPHERES = [10, 27, 72, 193, 518, 1389, 3728, 10000]
+JOB_MIX_CELLS = [71, 103, 151, 220, 321, 468, 684, 1000]  # 2 * cells^2 = 10,082 .. 2,000,000 triangles
+JOB_MIX_CELL_ORDER = [3, 7, 0, 5, 1, 6, 2, 4]
+
+
+def job_mix_scene(index: int, seed: int = 300, resolution=(512, 512), kinds=(0, 1, 2, 3)) -> M.Scene:
+    """Scene `index` (0..7) of the batched-job mix: a fractal heightfield and
+    log-uniform spheres of random matte/plastic/metal/glass materials, lit by a
+    point light, a spot light and a rectangular area light made of two
+    triangles (the CPU renderer samples area lights on triangles and spheres
+    only)."""
+    extent = 100.0
+    cells = JOB_MIX_CELLS[JOB_MIX_CELL_ORDER[index]]
+    sc = terrain_spheres(cells=cells, n_spheres=JOB_MIX_SPHERES[index], resolution=resolution, seed=seed + 17 * index,
+                         extent=extent, kinds=kinds)
+    sc.name = "job_mix_%d" % index
+    sc.lights = []
+    rng = np.random.default_rng(seed + 31 * index)
+    px, pz = rng.uniform(-0.3 * extent, 0.3 * extent, size=2)
+    sc.lights.append(M.PointLight((float(px), 0.45 * extent, float(pz)), (4000.0, 3800.0, 3500.0)))
+    sx, sz = rng.uniform(-0.3 * extent, 0.3 * extent, size=2)
+    sc.lights.append(M.SpotLight((float(sx), 0.5 * extent, float(sz)), (0.0, 0.0, 0.0), (9000.0, 8000.0, 7000.0), 35.0, 8.0))
+    y, h = 0.42 * extent, 0.08 * extent
+    a, b, c, d = (-h, y, -h), (h, y, -h), (h, y, h), (-h, y, h)
+    for tri in (M.Triangle(a, c, b), M.Triangle(a, d, c)):  # facing down
+        al = M.DiffuseAreaLight(tri, (25.0, 25.0, 25.0))
+        sc.lights.append(al)
+        sc.add(M.Primitive(tri, M.Matte(kd=(0.0, 0.0, 0.0)), area_light=al))
+    return sc
+
+
+def job_mix(n_jobs: int = 256, seed: int = 301, n_scenes: int = 8, min_side: int = 64, max_side: int = 1024,
+            spp_choices=(1, 4, 16, 64), bounce_choices=(4, 8, 20)):
+    """The batched workload: n_jobs jobs with square resolutions log-uniform
+    from min_side^2 to max_side^2, spp uniform over spp_choices, maximum bounce
+    uniform over bounce_choices, a uniformly drawn scene and a per-job seed.
+    Returns a list of dicts with keys scene, width, height, samples,
+    maximum_bounce, seed."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n_jobs):
+        side = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        jobs.append({"scene": int(rng.integers(0, n_scenes)), "width": side, "height": side,
+                     "samples": int(spp_choices[rng.integers(0, len(spp_choices))]),
+                     "maximum_bounce": int(bounce_choices[rng.integers(0, len(bounce_choices))]),
+                     "seed": int(rng.integers(1, 2 ** 31))})
+    return jobs

@@ -190,6 +190,120 @@ int dfc_read_stage_times(dfc_renderer* r, float* out5);
 int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, const float* d_directions, float* d_hits,
                            int64_t count);
 
+/* ------------------------------------------------------------------------
+ * Batch and serving engine.  The reference renders one image per
+ * GPURenderer, one pass per execute() (AbstractGPURenderer.java:231-297), so
+ * these entry points have no single counterpart: each render job is what a
+ * GPURenderer would do for setScene(scene) + setImage(w, h) +
+ * setMaximumBounce(b) + setMinimumBounceRussianRoulette(r) + setup() +
+ * render(spp) with PATH_TRACING, and the engine runs many such jobs at once in
+ * one wavefront of path slots.  A job's samples are those the per-job renderer
+ * draws for the same seed, so its image is the same alone, in a mix, or on a
+ * GPURenderer handle, up to the order of the film's float additions.
+ *
+ * Scenes are committed once and stay resident, reference-counted by the
+ * caller and by every unfinished job on them.  Jobs are admitted against a
+ * device-memory budget (wavefront + resident scenes + per-job films) and
+ * start their paths in the running wavefront at the next bounce iteration.
+ * Films can be read while a job runs (a progressive image).
+ *
+ * Threading: every dfc_engine_* / dfc_job_* call is thread-safe.  Either call
+ * dfc_engine_run() (the wavefront runs in the calling thread until every
+ * submitted job is finished) or dfc_engine_start()/dfc_engine_stop() (it runs
+ * on an engine thread; jobs may be submitted from any thread meanwhile).
+ * ------------------------------------------------------------------------ */
+typedef struct dfc_engine dfc_engine;
+
+enum { DFC_JOB_QUEUED = 0, DFC_JOB_RUNNING = 1, DFC_JOB_DONE = 2, DFC_JOB_CANCELLED = 3, DFC_JOB_FAILED = 4 };
+
+typedef struct dfc_job_desc {
+  int32_t scene;                            /* id from dfc_engine_scene_commit */
+  int32_t width, height;                    /* film resolution (the camera's field of view is kept) */
+  int32_t samples;                          /* samples per pixel: render(samples) on a GPURenderer */
+  int32_t maximum_bounce;                   /* setMaximumBounce */
+  int32_t minimum_bounce_russian_roulette;  /* setMinimumBounceRussianRoulette */
+  uint32_t seed;                            /* seed of the counter-based random numbers (dfc_set_seed) */
+  int32_t reserved;                         /* 0 */
+} dfc_job_desc;
+
+typedef struct dfc_job_info {
+  int32_t state;                 /* DFC_JOB_* */
+  int32_t scene;
+  int64_t paths_total;           /* width * height * samples */
+  int64_t paths_done;            /* retired paths as of the engine's last progress read */
+  double submit_s, admit_s, done_s;  /* engine clock in seconds (0 until reached) */
+} dfc_job_info;
+
+typedef struct dfc_engine_config {
+  int64_t capacity;              /* path slots of the wavefront (0: default 2^21) */
+  int32_t trace_blocks_per_sm;   /* resident blocks per SM of the traversal kernel (0: occupancy maximum) */
+  int32_t shade_blocks_per_sm;   /* blocks per SM of the sort and shade kernels (0: 8) */
+  int32_t shade_threads;         /* threads per shade block: 128 or 256 (0: 256) */
+  int32_t iterations_per_launch; /* bounce iterations per CUDA-graph launch, even (0: 4) */
+} dfc_engine_config;
+
+typedef struct dfc_engine_stats {
+  int64_t iterations, graph_launches, kernel_launches;
+  int64_t paths_retired, rays;
+  int64_t jobs_submitted, jobs_done;
+  int64_t device_bytes_used, device_bytes_budget;
+  int64_t overflow;              /* traversal stack bound hits (0 in a correct run) */
+  double busy_s;                 /* engine-clock seconds with work on the device */
+} dfc_engine_stats;
+
+/* Creates an engine on CUDA device `device` that admits work while its
+ * device memory (wavefront, resident scenes, job films) stays within
+ * `memory_budget_bytes` (0: 90% of the device's free memory). */
+int dfc_engine_create(int device, int64_t memory_budget_bytes, dfc_engine** out);
+/* Stops the engine thread if running, frees all device memory. */
+int dfc_engine_destroy(dfc_engine* e);
+const char* dfc_engine_last_error(const dfc_engine* e);
+
+/* Scene staging and commit, as dfc_scene_put/dfc_scene_commit; the committed
+ * scene gets an id and one caller reference.  DFC_E_OOM if it would exceed the
+ * budget. */
+int dfc_engine_scene_put(dfc_engine* e, const char* name, const void* data, int64_t count, int type);
+int dfc_engine_scene_commit(dfc_engine* e, int layout_version, int32_t* scene_id);
+/* Drops the caller's reference; the scene is freed once no unfinished job uses it. */
+int dfc_engine_scene_release(dfc_engine* e, int32_t scene_id);
+
+/* Wavefront shape (see dfc_engine_config); takes effect at the next run. */
+int dfc_engine_configure(dfc_engine* e, const dfc_engine_config* cfg);
+int dfc_engine_get_config(dfc_engine* e, dfc_engine_config* out);
+/* Picks capacity, block shapes and iterations per launch by timing
+ * candidates on `n` sample jobs (each candidate renders all of them), keeps
+ * the fastest and writes it to *out (may be NULL).  With `cache_path` set, a
+ * result stored there under `key` for this GPU is used instead of timing, and
+ * a new result is stored.  Only while the engine has no other jobs. */
+int dfc_engine_autotune(dfc_engine* e, const dfc_job_desc* jobs, int n, const char* cache_path, const char* key,
+                        dfc_engine_config* out);
+
+/* Queues a job; *job_id receives its id.  DFC_E_INVALID_ARG for a bad
+ * descriptor or unknown scene. */
+int dfc_job_submit(dfc_engine* e, const dfc_job_desc* desc, int64_t* job_id);
+int dfc_job_get_info(dfc_engine* e, int64_t job_id, dfc_job_info* out);
+/* Blocks until the job is done, cancelled or failed, or `timeout_s` passed
+ * (DFC_E_TIMEOUT).  Needs a running engine (dfc_engine_start) or another
+ * thread in dfc_engine_run. */
+int dfc_job_wait(dfc_engine* e, int64_t job_id, double timeout_s);
+/* Stops handing out the job's remaining paths; it ends as DFC_JOB_CANCELLED. */
+int dfc_job_cancel(dfc_engine* e, int64_t job_id);
+/* The job's film as dfc_read_film lays it out (width*height*7 floats), read
+ * while it runs (a progressive image) or after it finished. */
+int dfc_job_read_film(dfc_engine* e, int64_t job_id, float* dst, int64_t capacity_floats);
+/* Tone-mapped sRGB RGBA8 of the job's film, width*height*4 bytes. */
+int dfc_job_read_image_rgba8(dfc_engine* e, int64_t job_id, int tone_mapper, uint8_t* dst, int64_t capacity_bytes);
+/* Frees the job's film and forgets it (a running job is cancelled first). */
+int dfc_job_release(dfc_engine* e, int64_t job_id);
+
+/* Runs the wavefront in the calling thread until every submitted job is
+ * finished (DFC_E_TIMEOUT after `timeout_s` seconds, <= 0: no limit). */
+int dfc_engine_run(dfc_engine* e, double timeout_s);
+/* Runs the wavefront on an engine thread until dfc_engine_stop. */
+int dfc_engine_start(dfc_engine* e);
+int dfc_engine_stop(dfc_engine* e);
+int dfc_engine_get_stats(dfc_engine* e, dfc_engine_stats* out);
+
 #ifdef __cplusplus
 }
 #endif
