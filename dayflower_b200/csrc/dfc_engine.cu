@@ -44,8 +44,10 @@ using namespace dfc;
 namespace {
 
 constexpr int kMaxScenes = 64;
-constexpr unsigned kJobRing = 4096;  // job records on the device (power of two)
-constexpr int64_t kDefaultCapacity = int64_t(1) << 21;
+constexpr unsigned kJobRing = 4096;    // job records on the device (power of two)
+constexpr unsigned kSegRing = 65536;   // segment records on the device (power of two)
+constexpr int64_t kDefaultCapacity = int64_t(1) << 20;
+constexpr int64_t kDefaultSegment = 65536;
 constexpr int64_t kMaxCapacity = int64_t(1) << 26;
 // Device bytes per path slot: state 3 x 16, three ray slots (origin, direction,
 // hit) 3 x 48, pending light terms 2 x 16, ray lists 2 x 3 x 4, work lists 2 x 4,
@@ -66,7 +68,7 @@ struct JobRec {
   int state = DFC_JOB_QUEUED;
   bool cancel_req = false, cancel_sent = false;
   unsigned seq = 0;
-  unsigned long long start = 0, paths = 0, done = 0;
+  unsigned long long paths = 0, appended = 0, done = 0;  // total, handed to the device in segments, retired
   float4* film = nullptr;  // sum (pixels float4), then sum of squares (pixels float4)
   size_t film_bytes = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
@@ -98,8 +100,12 @@ struct dfc_engine {
   std::map<int64_t, JobRec> jobs;
   std::deque<int64_t> queue;
   std::vector<int64_t> ring_id = std::vector<int64_t>(kJobRing, 0);
-  unsigned seq_next = 0, seq_oldest = 0, job_lo = 0;
-  unsigned long long admitted_paths = 0;
+  unsigned seq_next = 0, seq_oldest = 0;
+  std::vector<int64_t> sched;    // admitted jobs with paths left to append, in admission order
+  size_t rr = 0;                 // round-robin position in `sched`
+  unsigned seg_next = 0, seg_lo = 0;
+  unsigned long long admitted_paths = 0;  // end of the last appended segment
+  unsigned long long cursor_seen = 0;     // the device's path cursor at the last progress read
   bool ctl_dirty = true;
   size_t film_bytes = 0;
   int64_t jobs_submitted = 0, jobs_done = 0;
@@ -108,7 +114,7 @@ struct dfc_engine {
   dfc_engine_config active{};
   bool built = false;
   size_t wave_bytes = 0;
-  DevBuf d_scene_table, d_jobs, d_job_done, d_ctl, d_state;
+  DevBuf d_scene_table, d_jobs, d_segs, d_job_done, d_ctl, d_state;
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_sort_keys, d_sort_bins, d_sorted, d_free_stack, d_slot_job, d_overflow;
   cudaGraphExec_t graph = nullptr;
@@ -118,6 +124,8 @@ struct dfc_engine {
   unsigned long long* h_done[2] = {nullptr, nullptr};
   unsigned* h_overflow[2] = {nullptr, nullptr};
   unsigned read_seq[2] = {0, 0};  // seq_next when the read-back was enqueued
+  unsigned read_seg[2] = {0, 0};  // seg_next when the read-back was enqueued
+  std::vector<unsigned long long> seg_end = std::vector<unsigned long long>(kSegRing, 0);  // end of each ring segment
   cudaEvent_t ev_read[2] = {nullptr, nullptr};
   // stats
   int64_t iterations = 0, graph_launches = 0, kernel_launches = 0, paths_retired = 0, rays = 0, overflow = 0;
@@ -167,12 +175,17 @@ dfc_engine_config resolved(const dfc_engine* e, dfc_engine_config c) {
   if (c.shade_threads != 128) c.shade_threads = 256;
   if (c.iterations_per_launch <= 0) c.iterations_per_launch = 4;
   c.iterations_per_launch += c.iterations_per_launch & 1;  // even: the graph ends on the parity it started with
+  if (c.policy != DFC_SCHEDULE_FIFO) c.policy = DFC_SCHEDULE_ROUND_ROBIN;
+  c.reserved = 0;
+  if (c.segment_paths <= 0) c.segment_paths = kDefaultSegment;
+  if (c.lookahead_paths <= 0) c.lookahead_paths = 8 * c.capacity;
   return c;
 }
 
 bool same_config(const dfc_engine_config& a, const dfc_engine_config& b) {
   return a.capacity == b.capacity && a.trace_blocks_per_sm == b.trace_blocks_per_sm && a.shade_blocks_per_sm == b.shade_blocks_per_sm &&
-         a.shade_threads == b.shade_threads && a.iterations_per_launch == b.iterations_per_launch;
+         a.shade_threads == b.shade_threads && a.iterations_per_launch == b.iterations_per_launch && a.policy == b.policy &&
+         a.segment_paths == b.segment_paths && a.lookahead_paths == b.lookahead_paths;
 }
 
 // Kernel arguments of one iteration of parity b.
@@ -184,7 +197,8 @@ void iteration_args(dfc_engine* e, int b, BatchArgs* ba, TraceArgs* ta, SortArgs
   const DJob* jobs = e->d_jobs.as<DJob>();
   *ba = BatchArgs{};
   ba->jobs = jobs;
-  ba->job_mask = kJobRing - 1;
+  ba->segs = e->d_segs.as<DSegment>();
+  ba->seg_mask = kSegRing - 1;
   ba->ctl = e->d_ctl.as<BatchControl>();
   ba->state = st;
   ba->job_done = e->d_job_done.as<unsigned long long>();
@@ -333,10 +347,11 @@ int build_wavefront(dfc_engine* e) {
   DFC_ECK(cudaMemsetAsync(e->d_state.p, 0, sizeof(BatchState), e->stream), "wavefront");
   DFC_ECK(cudaMemsetAsync(e->d_overflow.p, 0, 16, e->stream), "wavefront");
   // no job is running: the global path sequence restarts at 0, and the
-  // search window starts at the next job admitted (older ring records hold
-  // starts of the previous sequence)
+  // search window starts at the next segment appended (older ring records
+  // hold starts of the previous sequence)
   e->admitted_paths = 0;
-  e->job_lo = e->seq_next;
+  e->cursor_seen = 0;
+  e->seg_lo = e->seg_next;
   e->ctl_dirty = true;
   BatchArgs ba;
   TraceArgs ta;
@@ -388,7 +403,9 @@ int service(dfc_engine* e, bool idle_device) {
   }
   // cancellations of running jobs
   for (unsigned s = e->seq_oldest; s != e->seq_next; ++s) {
-    JobRec& J = e->jobs[e->ring_id[s & (kJobRing - 1)]];
+    auto it = e->jobs.find(e->ring_id[s & (kJobRing - 1)]);
+    if (it == e->jobs.end()) continue;
+    JobRec& J = it->second;
     if (J.cancel_req && !J.cancel_sent && J.state == DFC_JOB_RUNNING) {
       static const unsigned one = 1u;
       DJob* dj = e->d_jobs.as<DJob>() + (s & (kJobRing - 1));
@@ -396,7 +413,7 @@ int service(dfc_engine* e, bool idle_device) {
       J.cancel_sent = true;
     }
   }
-  // admission
+  // admission: film, job record
   while (!e->queue.empty()) {
     const int64_t id = e->queue.front();
     auto it = e->jobs.find(id);
@@ -437,8 +454,6 @@ int service(dfc_engine* e, bool idle_device) {
     dj.min_rr = J.d.minimum_bounce_russian_roulette;
     dj.seed = J.d.seed;
     dj.cancelled = 0;
-    dj.start = e->admitted_paths;
-    dj.paths = (unsigned long long)pixels * (unsigned long long)J.d.samples;
     dj.film_sum = static_cast<float4*>(film);
     dj.film_sq = static_cast<float4*>(film) + pixels;
     // pageable source: the copy has taken the bytes when the call returns
@@ -447,31 +462,76 @@ int service(dfc_engine* e, bool idle_device) {
     J.film = static_cast<float4*>(film);
     J.film_bytes = fb;
     J.seq = seq;
-    J.start = dj.start;
-    J.paths = dj.paths;
+    J.paths = (unsigned long long)pixels * (unsigned long long)J.d.samples;
+    J.appended = 0;
     J.done = 0;
     J.state = DFC_JOB_RUNNING;
     J.t_admit = now_s(e);
     e->film_bytes += fb;
-    e->admitted_paths += dj.paths;
     e->ring_id[r] = id;
     e->seq_next = seq + 1;
-    e->ctl_dirty = true;
+    e->sched.push_back(id);
     e->queue.pop_front();
+  }
+  // scheduling: append segments of admitted jobs while fewer than
+  // lookahead_paths appended paths are unstarted
+  {
+    const dfc_engine_config& c = e->active;
+    std::vector<DSegment> add;
+    unsigned long long backlog = e->admitted_paths - std::min(e->cursor_seen, e->admitted_paths);
+    while (backlog < (unsigned long long)c.lookahead_paths && !e->sched.empty() &&
+           e->seg_next + (unsigned)add.size() - e->seg_lo < kSegRing) {
+      if (e->rr >= e->sched.size()) e->rr = 0;
+      const size_t pick = c.policy == DFC_SCHEDULE_FIFO ? 0 : e->rr;
+      const int64_t id = e->sched[pick];
+      auto it = e->jobs.find(id);
+      if (it == e->jobs.end() || it->second.state != DFC_JOB_RUNNING || it->second.cancel_req ||
+          it->second.appended >= it->second.paths) {
+        e->sched.erase(e->sched.begin() + (long)pick);
+        continue;
+      }
+      JobRec& J = it->second;
+      const unsigned long long n = std::min((unsigned long long)c.segment_paths, J.paths - J.appended);
+      DSegment sg{};
+      sg.start = e->admitted_paths;
+      sg.q0 = J.appended;
+      sg.count = n;
+      sg.job = J.seq & (kJobRing - 1);
+      add.push_back(sg);
+      J.appended += n;
+      e->admitted_paths += n;
+      backlog += n;
+      if (J.appended >= J.paths) e->sched.erase(e->sched.begin() + (long)pick);
+      else if (c.policy != DFC_SCHEDULE_FIFO) e->rr = pick + 1;
+    }
+    // one copy per contiguous run of ring slots
+    size_t k = 0;
+    while (k < add.size()) {
+      const unsigned first = (e->seg_next + (unsigned)k) & (kSegRing - 1);
+      const size_t run = std::min(add.size() - k, (size_t)(kSegRing - first));
+      DFC_ECK(cudaMemcpyAsync(e->d_segs.as<DSegment>() + first, add.data() + k, run * sizeof(DSegment), cudaMemcpyHostToDevice,
+                              e->stream), "segments");
+      k += run;
+    }
+    for (size_t q = 0; q < add.size(); ++q) e->seg_end[(e->seg_next + (unsigned)q) & (kSegRing - 1)] = add[q].start + add[q].count;
+    if (!add.empty()) {
+      e->seg_next += (unsigned)add.size();
+      e->ctl_dirty = true;
+    }
   }
   if (e->ctl_dirty) {
     BatchControl c{};
     c.admitted = e->admitted_paths;
-    c.job_lo = e->job_lo;
-    c.job_hi = e->seq_next;
+    c.seg_lo = e->seg_lo;
+    c.seg_hi = e->seg_next;
     DFC_ECK(cudaMemcpyAsync(e->d_ctl.p, &c, sizeof c, cudaMemcpyHostToDevice, e->stream), "control");
     e->ctl_dirty = false;
   }
   return DFC_OK;
 }
 
-// Reads one progress record (holding mu): job completions, the admission
-// window's lower end, counters.
+// Reads one progress record (holding mu): job completions, the lower end of
+// the segment window, counters.
 void process(dfc_engine* e, int b) {
   const BatchState& st = *e->h_state[b];
   const unsigned long long* done = e->h_done[b];
@@ -481,14 +541,17 @@ void process(dfc_engine* e, int b) {
   e->overflow = e->base_overflow + *e->h_overflow[b];
   const double t = now_s(e);
   bool changed = false;
+  // jobs admitted after this read-back was enqueued have fresh counters on the device: skip them
   for (unsigned s = e->seq_oldest; s != e->read_seq[b]; ++s) {
     auto it = e->jobs.find(e->ring_id[s & (kJobRing - 1)]);
     if (it == e->jobs.end()) continue;
     JobRec& J = it->second;
     if (J.state != DFC_JOB_RUNNING) continue;
+    // a cancelled job ends once the paths it was given are done; no more are appended after the request
+    const unsigned long long target = J.cancel_req ? J.appended : J.paths;
     J.done = std::min(done[s & (kJobRing - 1)], J.paths);
-    if (J.done >= J.paths) {
-      J.state = J.cancel_sent ? DFC_JOB_CANCELLED : DFC_JOB_DONE;
+    if (J.done >= target) {
+      J.state = J.cancel_req ? DFC_JOB_CANCELLED : DFC_JOB_DONE;
       J.t_done = t;
       e->scenes[J.d.scene].job_refs--;
       e->jobs_done++;
@@ -502,15 +565,15 @@ void process(dfc_engine* e, int b) {
     e->ring_id[r] = 0;
     e->seq_oldest++;
   }
-  // lowest job that may still hand out paths: the one holding the cursor
-  unsigned lo = e->seq_oldest;
-  while (lo != e->read_seq[b]) {
-    auto it = e->jobs.find(e->ring_id[lo & (kJobRing - 1)]);
-    if (it != e->jobs.end() && it->second.start + it->second.paths > st.cursor) break;
-    ++lo;
-  }
-  if (lo != e->job_lo) {
-    e->job_lo = lo;
+  // segments wholly behind the cursor hand out nothing more: the window
+  // starts at the one holding the cursor, and their ring slots can be reused
+  e->cursor_seen = st.cursor;
+  // (the device copy of the segments is only read inside [seg_lo, seg_hi))
+  unsigned lo = e->seg_lo;
+  const unsigned hi = e->read_seg[b];
+  while (lo != hi && e->seg_end[lo & (kSegRing - 1)] <= st.cursor) ++lo;
+  if (lo != e->seg_lo) {
+    e->seg_lo = lo;
     e->ctl_dirty = true;
   }
   if (changed) e->cv.notify_all();
@@ -567,6 +630,7 @@ int drive(dfc_engine* e, bool until_idle, double timeout_s) {
             break;
           }
           e->read_seq[b] = e->seq_next;
+          e->read_seg[b] = e->seg_next;
           pending[b] = true;
           launched = true;
           e->graph_launches++;
@@ -689,11 +753,13 @@ int dfc_engine_create(int device, int64_t budget, dfc_engine** out) {
   }
   cudaGetLastError();
   if (e->d_scene_table.ensure(kMaxScenes * sizeof(SceneView)) != cudaSuccess || e->d_jobs.ensure(kJobRing * sizeof(DJob)) != cudaSuccess ||
+      e->d_segs.ensure(kSegRing * sizeof(DSegment)) != cudaSuccess ||
       e->d_job_done.ensure(kJobRing * sizeof(unsigned long long)) != cudaSuccess || e->d_ctl.ensure(sizeof(BatchControl)) != cudaSuccess ||
       e->d_state.ensure(sizeof(BatchState)) != cudaSuccess)
     return DFC_E_OOM;
   cudaMemsetAsync(e->d_scene_table.p, 0, kMaxScenes * sizeof(SceneView), e->stream);
   cudaMemsetAsync(e->d_jobs.p, 0, kJobRing * sizeof(DJob), e->stream);
+  cudaMemsetAsync(e->d_segs.p, 0, kSegRing * sizeof(DSegment), e->stream);
   cudaMemsetAsync(e->d_job_done.p, 0, kJobRing * sizeof(unsigned long long), e->stream);
   cudaMemsetAsync(e->d_ctl.p, 0, sizeof(BatchControl), e->stream);
   cudaMemsetAsync(e->d_state.p, 0, sizeof(BatchState), e->stream);

@@ -971,15 +971,15 @@ __global__ void k_batch_init(BatchArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) a.state->free_top = a.capacity;
 }
 
-// Job ring index of the admitted job that owns global path index g.
-DFC_D unsigned job_of(const BatchArgs& a, unsigned long long g) {
-  unsigned lo = a.ctl->job_lo, hi = a.ctl->job_hi;
+// Segment ring index of the appended segment that holds global path index g.
+DFC_D unsigned seg_of(const BatchArgs& a, unsigned long long g) {
+  unsigned lo = a.ctl->seg_lo, hi = a.ctl->seg_hi;
   while (hi - lo > 1u) {
     const unsigned mid = lo + (hi - lo) / 2u;
-    if (a.jobs[mid & a.job_mask].start <= g) lo = mid;
+    if (a.segs[mid & a.seg_mask].start <= g) lo = mid;
     else hi = mid;
   }
-  return lo & a.job_mask;
+  return lo & a.seg_mask;
 }
 
 // One thread: the previous iteration's counters are final (its rays are
@@ -995,12 +995,11 @@ __global__ void k_batch_plan(BatchArgs a) {
   a.counts_next[1] = 0u;
   a.counts_next[2] = 0u;
   const unsigned long long admitted = a.ctl->admitted;
-  for (int guard = 0; guard < 16 && st->cursor < admitted; ++guard) {
-    const unsigned jr = job_of(a, st->cursor);
-    const DJob& J = a.jobs[jr];
-    if (!J.cancelled) break;
-    const unsigned long long end = J.start + J.paths;
-    a.job_done[jr] += end - st->cursor;
+  for (int guard = 0; guard < 64 && st->cursor < admitted; ++guard) {
+    const DSegment& S = a.segs[seg_of(a, st->cursor)];
+    if (!a.jobs[S.job].cancelled) break;
+    const unsigned long long end = S.start + S.count;
+    a.job_done[S.job] += end - st->cursor;
     st->cursor = end;
   }
   const unsigned long long rem = admitted - st->cursor;
@@ -1014,8 +1013,9 @@ __global__ void k_batch_plan(BatchArgs a) {
   st->iterations += 1u;
 }
 
-// Starts the planned paths: global path index -> job (binary search over the
-// admitted window by first path index) -> pixel and sample -> camera ray, in
+// Starts the planned paths: global path index -> segment (binary search over
+// the appended window by first path index) -> job path -> pixel and sample ->
+// camera ray, in
 // the same form as k_raygen so that a job's samples are those the per-job
 // renderer draws for the same seed.
 __global__ void k_batch_regen(BatchArgs a) {
@@ -1030,9 +1030,10 @@ __global__ void k_batch_regen(BatchArgs a) {
     if (valid) {
       slot = a.free_stack[sbase + i];
       const unsigned long long g = g0 + i;
-      const unsigned jr = job_of(a, g);
+      const DSegment& S = a.segs[seg_of(a, g)];
+      const unsigned jr = S.job;
       const DJob& J = a.jobs[jr];
-      const unsigned long long q = g - J.start;
+      const unsigned long long q = S.q0 + (g - S.start);
       const unsigned pix = (unsigned)(q % J.pixels);
       const unsigned sample = (unsigned)(q / J.pixels);
       const unsigned x = pix % J.width, y = pix / J.width;

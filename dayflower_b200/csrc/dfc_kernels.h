@@ -12,28 +12,38 @@ enum { DFC_ALGO_AO = 0, DFC_ALGO_DEPTH = 1, DFC_ALGO_PATH = 2, DFC_ALGO_RAY_CAST
 // Path flags (PathMeta.w)
 enum : unsigned { kFlagAlive = 1u, kFlagSpecular = 2u, kFlagPendShadow = 4u, kFlagPendMis = 8u, kFlagShadowAny = 16u, kFlagNoSample = 32u };
 
-// One render job of the batch/serving engine as the kernels read it.  Jobs
-// live in a ring of power-of-two capacity indexed by sequence number & mask;
-// the paths of all admitted jobs form one global sequence in which job j owns
-// [start, start + paths), sample-major (path q of the job is pixel q % pixels
-// of sample q / pixels).
+// One render job of the batch/serving engine as the kernels read it (a ring
+// of power-of-two capacity indexed by sequence number & mask).  Path q of a
+// job is pixel q % pixels of sample q / pixels (sample-major, so a partial
+// film is a progressive image).
 struct DJob {
   float camera[19];          // the scene's compiled camera with the job's resolution in [17], [18]
   int scene;                 // index into the engine's scene table
   unsigned width, pixels;
   int max_bounce, min_rr;
   uint32_t seed;
-  unsigned cancelled;        // 1: hand out no more paths of this job (they retire unsampled)
-  unsigned long long start;  // first global path index
-  unsigned long long paths;  // pixels * samples
+  unsigned cancelled;        // 1: start no more paths of this job (the plan skips them)
   float4* film_sum;          // per pixel: sum of accepted samples (xyz), count (w)
   float4* film_sq;           // per pixel: sum of squares (xyz)
 };
 
+// A run of consecutive paths of one job in the engine's global path sequence:
+// global indices [start, start + count) are the job's paths [q0, q0 + count).
+// The host appends segments (its scheduling policy decides whose) into a ring
+// indexed by segment sequence number & mask; starts increase with the
+// sequence number.
+struct DSegment {
+  unsigned long long start;
+  unsigned long long q0;
+  unsigned long long count;
+  unsigned job;              // job ring index
+  unsigned pad;
+};
+
 // Words the host writes between wavefront iterations (stream-ordered copies).
 struct BatchControl {
-  unsigned long long admitted;  // total paths of all admitted jobs
-  unsigned job_lo, job_hi;      // sequence numbers of the jobs that may still hand out paths
+  unsigned long long admitted;  // end of the last appended segment
+  unsigned seg_lo, seg_hi;      // sequence numbers of the segments that may still hand out paths
 };
 
 // Words the wavefront iterations keep on the device.
@@ -153,7 +163,8 @@ __global__ void k_sort_scatter(SortArgs a);
 // with the lists and counters of parity (iteration & 1).
 struct BatchArgs {
   const DJob* jobs;
-  unsigned job_mask;
+  const DSegment* segs;
+  unsigned seg_mask;
   const BatchControl* ctl;
   BatchState* state;
   unsigned long long* job_done;  // per job ring entry: paths retired (or skipped by a cancel)

@@ -44,9 +44,13 @@ class JobInfo(ctypes.Structure):
                 ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
 
 
+SCHEDULE_ROUND_ROBIN, SCHEDULE_FIFO = 0, 1
+
+
 class EngineConfig(ctypes.Structure):
     _fields_ = [("capacity", ctypes.c_int64), ("trace_blocks_per_sm", ctypes.c_int32), ("shade_blocks_per_sm", ctypes.c_int32),
-                ("shade_threads", ctypes.c_int32), ("iterations_per_launch", ctypes.c_int32)]
+                ("shade_threads", ctypes.c_int32), ("iterations_per_launch", ctypes.c_int32), ("policy", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("segment_paths", ctypes.c_int64), ("lookahead_paths", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -128,8 +132,11 @@ class RenderEngine:
         self._check(self._lib.dfc_engine_scene_release(self._h, int(scene_id)))
 
     # -- configuration -------------------------------------------------------------
-    def configure(self, capacity=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, shade_threads=0, iterations_per_launch=0):
-        c = EngineConfig(int(capacity), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(shade_threads), int(iterations_per_launch))
+    def configure(self, capacity=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, shade_threads=0, iterations_per_launch=0,
+                  policy=SCHEDULE_ROUND_ROBIN, segment_paths=0, lookahead_paths=0):
+        """Wavefront shape and scheduling (0 keeps a field's default); takes effect at the next run."""
+        c = EngineConfig(int(capacity), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(shade_threads), int(iterations_per_launch),
+                         int(policy), 0, int(segment_paths), int(lookahead_paths))
         self._check(self._lib.dfc_engine_configure(self._h, ctypes.byref(c)))
 
     def config(self) -> dict:

@@ -234,12 +234,23 @@ typedef struct dfc_job_info {
   double submit_s, admit_s, done_s;  /* engine clock in seconds (0 until reached) */
 } dfc_job_info;
 
+/* Scheduling policies: the host hands the device runs ("segments") of
+ * consecutive paths of one job, at most `lookahead_paths` ahead of the paths
+ * started so far.  ROUND_ROBIN gives every admitted job one segment in turn
+ * (processor sharing: small jobs finish early while large ones run); FIFO
+ * finishes jobs in admission order. */
+enum { DFC_SCHEDULE_ROUND_ROBIN = 0, DFC_SCHEDULE_FIFO = 1 };
+
 typedef struct dfc_engine_config {
-  int64_t capacity;              /* path slots of the wavefront (0: default 2^21) */
+  int64_t capacity;              /* path slots of the wavefront (0: default 2^20) */
   int32_t trace_blocks_per_sm;   /* resident blocks per SM of the traversal kernel (0: occupancy maximum) */
   int32_t shade_blocks_per_sm;   /* blocks per SM of the sort and shade kernels (0: 8) */
   int32_t shade_threads;         /* threads per shade block: 128 or 256 (0: 256) */
   int32_t iterations_per_launch; /* bounce iterations per CUDA-graph launch, even (0: 4) */
+  int32_t policy;                /* DFC_SCHEDULE_* */
+  int32_t reserved;              /* 0 */
+  int64_t segment_paths;         /* paths per segment (0: 65536) */
+  int64_t lookahead_paths;       /* appended but unstarted paths the host keeps queued (0: 8 x capacity) */
 } dfc_engine_config;
 
 typedef struct dfc_engine_stats {
