@@ -16,6 +16,10 @@ the wavefront buffers (several hundred MB) exceed the 126 MB L2 between steps.
 Multi-GPU: the passes are independent, so N ranks render N independent
 replicas of the job (weak scaling, no collective on the data path).
 
+At N=1 the line also carries the job-mix measurements (``batched``: 256 jobs
+through the batch engine against the per-job renderer; ``served``: Poisson
+arrival sweeps with p50/p99 latency), see :func:`batched_and_served`.
+
 ``--impl reference`` times the CPU restatement of the reference CPURenderer
 (the oracle) on all host threads on a bounded row sample of the same job.
 """
@@ -60,6 +64,12 @@ def parse():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and served job-mix measurements")
+    ap.add_argument("--jobs", type=int, default=256, help="jobs of the batched mix")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the batched job mix (per-job arm and engine arm) and print its JSON object")
+    ap.add_argument("--engine-only", action="store_true", help="with --batch-only: skip the per-job arm and the served sweep")
+    ap.add_argument("--no-autotune", action="store_true", help="engine arm with the default wavefront shape")
     return ap.parse_args()
 
 
@@ -150,6 +160,121 @@ def cpu_baseline(compiled, spp_sample=1, rows=12, threads=None):
             "sample": "%d rows x %d px x %d spp of the same job (%d paths, %.1f s, %d rays)" % (rows, o.width, spp_sample, paths, dt, res["rays"])}
 
 
+def batched_and_served(args, device=0):
+    """The job-mix workloads on one GPU.
+
+    Batched: 256 path-tracing jobs (square resolutions log-uniform 64^2 ..
+    1024^2, spp in {1, 4, 16, 64}, maximum bounce in {4, 8, 20}) over eight
+    seeded scenes (10 .. 10k spheres, 10k .. 2M-triangle heightfields, point,
+    spot and area lights), rendered (a) one job at a time through the per-job
+    GPURenderer, each scene resident on its own handle, and (b) all submitted
+    at once to the RenderEngine (FIFO segments) after its autotuner picked the
+    wavefront shape on 32 of the jobs.  Both arms end with every job's RGBA8
+    image read back to the host.
+
+    Served: Poisson arrival streams of the same jobs at rates 10 .. 500 jobs/s
+    into the running engine (round-robin segments); latency is submit to done
+    at the job's own spp.  The per-job comparison is the latency of one
+    renderer serving the same arrivals one job at a time in arrival order,
+    from the measured per-job render times of (a).
+    """
+    import numpy as np
+    from dayflower_b200 import GPURenderer, RenderEngine
+    from dayflower_b200 import serve as SV
+    from dayflower_b200.scene import generators as G
+    from dayflower_b200.scene.compiler import compile_scene
+
+    scenes = [compile_scene(G.job_mix_scene(i), layout_version=2) for i in range(8)]
+    jobs = G.job_mix(args.jobs)
+    paths = float(sum(j["width"] * j["height"] * j["samples"] for j in jobs))
+
+    # (a) per-job renderer
+    handles = []
+    for cs in scenes:
+        h = GPURenderer(device=device)
+        h.setScene(cs)
+        handles.append(h)
+    cams = [np.array(cs.arrays["cameraArray"], dtype=np.float32) for cs in scenes]
+
+    def plain(js):
+        times = []
+        for j in js:
+            t0 = time.perf_counter()
+            h = handles[j["scene"]]
+            c = cams[j["scene"]].copy()
+            c[17], c[18] = j["width"], j["height"]
+            h.updateCamera(c)
+            h.setImage(j["width"], j["height"])
+            h.setMaximumBounce(j["maximum_bounce"])
+            h.setSeed(j["seed"])
+            h.setup()
+            h.render(j["samples"])
+            h.getImage()
+            times.append(time.perf_counter() - t0)
+        return times
+
+    service, t_plain, plain_launches = None, None, None
+    if not args.engine_only:
+        plain(jobs[:4])
+        t0 = time.perf_counter()
+        service = plain(jobs)
+        t_plain = time.perf_counter() - t0
+        plain_launches = sum(h.getCounters()["launches"] for h in handles)
+    for h in handles:
+        h.dispose()
+
+    # (b) engine
+    eng = RenderEngine(device=device)
+    try:
+        ids = [eng.add_scene(cs) for cs in scenes]
+        del ids
+        tuned = eng.config() if args.no_autotune else eng.autotune(jobs[:32])
+        eng.configure(**dict(tuned, policy=1))
+        warm = [eng.submit(**j) for j in jobs[:4]]
+        eng.run()
+        for k in warm:
+            eng.release(k)
+        s0 = eng.stats()
+        t0 = time.perf_counter()
+        ks = [eng.submit(**j) for j in jobs]
+        eng.run()
+        imgs = [eng.image(k) for k in ks]
+        t_eng = time.perf_counter() - t0
+        s1 = eng.stats()
+        for k in ks:
+            eng.release(k)
+        batched = {
+            "workload": "job mix: %d PT jobs over 8 seeded scenes, 64^2..1024^2, spp {1,4,16,64}, bounce {4,8,20}" % len(jobs),
+            "jobs": len(jobs), "paths": paths, "engine_paths_per_s": paths / t_eng, "engine_s": t_eng,
+            "engine_rays_per_s": (s1["rays"] - s0["rays"]) / t_eng,
+            "plain_per_job_paths_per_s": paths / t_plain if t_plain else None, "plain_per_job_s": t_plain,
+            "speedup_vs_plain_per_job": t_plain / t_eng if t_plain else None,
+            "engine_config": eng.config(), "engine_gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
+            "plain_gpu_launches": plain_launches, "image_bytes_read": int(sum(x.nbytes for x in imgs)),
+            "timing": "wall clock over submit -> all RGBA8 images on the host, both arms",
+        }
+        if args.engine_only or args.batch_only:
+            return batched, None
+        # served
+        eng.configure(**dict(tuned, policy=0))
+        eng.start()
+        served = []
+        for lam in (10, 25, 50, 100, 250, 500):
+            n = min(len(jobs), max(16, int(4 * lam)))
+            arr = SV.poisson_arrivals(lam, n, seed=lam)
+            sub = [jobs[i % len(jobs)] for i in range(n)]
+            r = SV.run_served(eng, sub, arr)
+            p = SV.percentiles(r["latency_s"])
+            f = SV.percentiles(SV.fifo_latencies([service[i % len(jobs)] for i in range(n)], arr))
+            served.append({"lambda_per_s": lam, "jobs": n, "p50_s": p["p50_s"], "p99_s": p["p99_s"], "paths_per_s": r["paths_per_s"],
+                           "plain_per_job_p50_s": f["p50_s"], "plain_per_job_p99_s": f["p99_s"], "states": r["states"]})
+        eng.stop()
+    finally:
+        eng.close()
+    return batched, {"policy": "round_robin", "latency": "submit -> done at the job's spp (engine clock)",
+                     "plain_per_job": "one job at a time in arrival order, measured per-job render times", "sweep": served}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -175,6 +300,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps(batched_and_served(args, 0)[0]), flush=True)
         return
     import torch
     import torch.distributed as dist
@@ -282,8 +411,11 @@ def main():
         }
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(compiled, rows=144)
-        print(json.dumps(line), flush=True)
     r.dispose()
+    if rank == 0:
+        if world == 1 and not args.no_batch:
+            line["batched"], line["served"] = batched_and_served(args, local)
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 

@@ -133,7 +133,7 @@ class RenderEngine:
 
     # -- configuration -------------------------------------------------------------
     def configure(self, capacity=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, shade_threads=0, iterations_per_launch=0,
-                  policy=SCHEDULE_ROUND_ROBIN, segment_paths=0, lookahead_paths=0):
+                  policy=SCHEDULE_ROUND_ROBIN, segment_paths=0, lookahead_paths=0, reserved=0):
         """Wavefront shape and scheduling (0 keeps a field's default); takes effect at the next run."""
         c = EngineConfig(int(capacity), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(shade_threads), int(iterations_per_launch),
                          int(policy), 0, int(segment_paths), int(lookahead_paths))
