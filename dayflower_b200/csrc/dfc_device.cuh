@@ -397,22 +397,29 @@ DFC_D void surface_to_world(const DPrim& pr, Surface& s) {
 
 // ---------------------------------------------------------------- BSDFs --
 enum { kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossy = 8, kSpecular = 16, kAll = 31, kAllButSpecular = 15 };
-enum : int { kLambert = 0, kOrenNayar = 1, kSpecBRDF = 2, kFresnelSpec = 3, kSpecBTDF = 4, kTSBRDF = 5, kTSBTDF = 6 };
-enum : int { kFresConst = 0, kFresDielectric = 1, kFresConductor = 2 };
+enum : int {
+  kLambert = 0, kOrenNayar = 1, kSpecBRDF = 2, kFresnelSpec = 3, kSpecBTDF = 4, kTSBRDF = 5, kTSBTDF = 6,
+  kLambertBTDF = 7,                                                                   // scene/bxdf/LambertianBTDF.java
+  kDisneyDiffuse = 8, kDisneyFakeSS = 9, kDisneyRetro = 10, kDisneySheen = 11, kDisneyClearCoat = 12  // scene/bxdf/Disney*.java
+};
+enum : int { kFresConst = 0, kFresDielectric = 1, kFresConductor = 2, kFresDisney = 3 };
+constexpr int kMaxLobes = 8;  // DisneyMaterial, thin: diffuse, fake subsurface, retro, sheen, specular, clear coat, two transmissions
 
+// One BxDF of a BSDF: 24 bytes.  Parameters every lobe of one material shares
+// (Fresnel and refraction indices, conductor or Disney colours) live in the Bsdf.
 struct Lobe {
-  int kind, type, fresnel;
-  V3 scale, scale2;          // scale2: FresnelSpecular transmittance
-  float a, b;                // Oren-Nayar
-  float etaI, etaT;          // dielectric Fresnel
-  V3 cEta, cK;               // conductor Fresnel (etaI = 1)
-  float ax, ay;
-  float etaA, etaB;
+  unsigned char kind, type, fresnel, separable;  // separable: G = G1(wo) G1(wi) (MicrofacetDistribution.isSeparableModel)
+  V3 scale;
+  float p0, p1;  // Oren-Nayar A, B | microfacet alpha x, y | Disney roughness | clear coat alpha, weight
 };
 struct Bsdf {
   int n;
-  Lobe l[2];
-  float eta;
+  Lobe l[kMaxLobes];
+  float eta;            // BSDF.getEta
+  float fr_i, fr_t;     // dielectric Fresnel of reflection lobes (Disney: etaT)
+  float bt_a, bt_b;     // etaA, etaB of transmission lobes
+  float metallic;       // DisneyFresnel blend
+  V3 ca, cb;            // conductor eta and k | Disney R0 | FresnelSpecular transmittance (ca)
   ONB s;
   V3 ng, wo_w, wo;
 };
@@ -440,11 +447,18 @@ DFC_D float fr_conductor1(float c, float eta, float k) {  // scene/fresnel/Condu
   float rp = rs * (t3 - t4) / (t3 + t4);
   return (rp + rs) * 0.5f;
 }
-DFC_D V3 fresnel(const Lobe& L, float cosi) {
-  if (L.fresnel == kFresDielectric) { float f = fr_dielectric(cosi, L.etaI, L.etaT); return {f, f, f}; }
+DFC_D float schlick_w(float c) { float m = clampf(1.0f - c, 0.0f, 1.0f); return (m * m) * (m * m) * m; }  // Schlick.java:104
+DFC_D float lerpf(float a, float b, float t) { return (1.0f - t) * a + t * b; }  // utility/Floats.java:591
+DFC_D V3 fresnel(const Bsdf& B, const Lobe& L, float cosi) {
+  if (L.fresnel == kFresDielectric) { float f = fr_dielectric(cosi, B.fr_i, B.fr_t); return {f, f, f}; }
   if (L.fresnel == kFresConductor) {
     float c = fabsf(cosi);
-    return {fr_conductor1(c, L.cEta.x, L.cK.x), fr_conductor1(c, L.cEta.y, L.cK.y), fr_conductor1(c, L.cEta.z, L.cK.z)};
+    return {fr_conductor1(c, B.ca.x, B.cb.x), fr_conductor1(c, B.ca.y, B.cb.y), fr_conductor1(c, B.ca.z, B.cb.z)};
+  }
+  if (L.fresnel == kFresDisney) {  // scene/fresnel/DisneyFresnel.java
+    const float d = fr_dielectric(cosi, 1.0f, B.fr_t), w = schlick_w(cosi);
+    return {lerpf(d, lerpf(B.ca.x, 1.0f, w), B.metallic), lerpf(d, lerpf(B.ca.y, 1.0f, w), B.metallic),
+            lerpf(d, lerpf(B.ca.z, 1.0f, w), B.metallic)};
   }
   return {1, 1, 1};
 }
@@ -455,24 +469,27 @@ DFC_D float cosphi(V3 v) { float s = sint(v); return s == 0.0f ? 1.0f : clampf(v
 DFC_D float sinphi(V3 v) { float s = sint(v); return s == 0.0f ? 0.0f : clampf(v.y / s, -1.0f, 1.0f); }
 DFC_D bool same_hemi(V3 a, V3 b) { return a.z * b.z > 0.0f; }
 
-// scene/microfacet/TrowbridgeReitzMicrofacetDistribution.java
+// scene/microfacet/TrowbridgeReitzMicrofacetDistribution.java (alphas in p0, p1)
 DFC_D float tr_D(const Lobe& L, V3 h) {
   float t2 = sin2t(h) / (h.z * h.z);
   if (isinf(t2)) return 0.0f;
   float cp = cosphi(h), sp = sinphi(h);
   float c4 = (h.z * h.z) * (h.z * h.z);
-  float e = (cp * cp / (L.ax * L.ax) + sp * sp / (L.ay * L.ay)) * t2;
-  return 1.0f / (kPi * L.ax * L.ay * c4 * (1.0f + e) * (1.0f + e));
+  float e = (cp * cp / (L.p0 * L.p0) + sp * sp / (L.p1 * L.p1)) * t2;
+  return 1.0f / (kPi * L.p0 * L.p1 * c4 * (1.0f + e) * (1.0f + e));
 }
 DFC_D float tr_lambda(const Lobe& L, V3 w) {
   float ta = fabsf(sint(w) / w.z);
   if (isinf(ta)) return 0.0f;
   float cp = cosphi(w), sp = sinphi(w);
-  float al = sqrtf(cp * cp * L.ax * L.ax + sp * sp * L.ay * L.ay);
+  float al = sqrtf(cp * cp * L.p0 * L.p0 + sp * sp * L.p1 * L.p1);
   float x = (al * ta) * (al * ta);
   return (-1.0f + sqrtf(1.0f + x)) / 2.0f;
 }
-DFC_D float tr_G(const Lobe& L, V3 wo, V3 wi) { return 1.0f / (1.0f + tr_lambda(L, wo) + tr_lambda(L, wi)); }
+DFC_D float tr_G(const Lobe& L, V3 wo, V3 wi) {
+  return L.separable ? (1.0f / (1.0f + tr_lambda(L, wo))) * (1.0f / (1.0f + tr_lambda(L, wi)))
+                     : 1.0f / (1.0f + tr_lambda(L, wo) + tr_lambda(L, wi));
+}
 DFC_D float tr_pdf(const Lobe& L, V3 wo, V3 h) {
   return tr_D(L, h) * (1.0f / (1.0f + tr_lambda(L, wo))) * fabsf(dot(wo, h)) / fabsf(wo.z);
 }
@@ -500,7 +517,7 @@ DFC_D V3 tr_visible(V3 w, float ax, float ay, float u, float v) {
   return normalize(V3{-((cp * sx - sp * sy) * ax), -((sp * sx + cp * sy) * ay), 1.0f});
 }
 DFC_D V3 tr_sample_h(const Lobe& L, V3 wo, float u, float v) {
-  return wo.z >= 0.0f ? tr_visible(wo, L.ax, L.ay, u, v) : -tr_visible(-wo, L.ax, L.ay, u, v);
+  return wo.z >= 0.0f ? tr_visible(wo, L.p0, L.p1, u, v) : -tr_visible(-wo, L.p0, L.p1, u, v);
 }
 DFC_D bool refract(V3 d, V3 n, float eta, V3* out) {  // geometry/Vector3F.java:454
   float ci = dot(d, n);
@@ -509,15 +526,24 @@ DFC_D bool refract(V3 d, V3 n, float eta, V3* out) {  // geometry/Vector3F.java:
   *out = (-d) * eta + n * (eta * ci - sqrtf(1.0f - st2));
   return true;
 }
+// DisneyClearCoatBRDF.java:330 doGTR1, :337 doSmithGGGX
+DFC_D float gtr1(float ct, float alpha) {
+  const float a = alpha * alpha;
+  return (a - 1.0f) / (kPi * logf(a) * (1.0f + (a - 1.0f) * ct * ct));
+}
+DFC_D float smith_ggx(float ct, float alpha) {
+  const float a = alpha * alpha, b = ct * ct;
+  return 1.0f / (ct + sqrtf(a + b - a * b));
+}
 
-DFC_D V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
+DFC_D V3 lobe_f(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
   switch (L.kind) {
-    case kLambert: return L.scale * (1.0f / kPi);
+    case kLambert: case kLambertBTDF: return L.scale * (1.0f / kPi);
     case kOrenNayar: {
       float ci = fabsf(wi.z), co = fabsf(wo.z), si = sint(wi), so = sint(wo);
       float mc = (si > 1.0e-4f && so > 1.0e-4f) ? fmaxf(0.0f, cosphi(wi) * cosphi(wo) + sinphi(wi) * sinphi(wo)) : 0.0f;
       float sa = ci > co ? so : si, tb = ci > co ? si / ci : so / co;
-      return L.scale * (1.0f / kPi) * (L.a + L.b * mc * sa * tb);
+      return L.scale * (1.0f / kPi) * (L.p0 + L.p1 * mc * sa * tb);
     }
     case kTSBRDF: {
       float co = fabsf(wo.z), ci = fabsf(wi.z);
@@ -526,28 +552,58 @@ DFC_D V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
       if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
       h = normalize(h);
       V3 hf = h.z < 0.0f ? -h : h;
-      V3 F = fresnel(L, dot(wi, hf));
+      V3 F = fresnel(B, L, dot(wi, hf));
       return mul(L.scale * (tr_D(L, h) * tr_G(L, wo, wi)), F) * (1.0f / (4.0f * ci * co));
     }
     case kTSBTDF: {
       if (same_hemi(wo, wi)) return {0, 0, 0};
       if (wi.z == 0.0f || wo.z == 0.0f) return {0, 0, 0};
-      float eta = wo.z > 0.0f ? L.etaB / L.etaA : L.etaA / L.etaB;
+      float eta = wo.z > 0.0f ? B.bt_b / B.bt_a : B.bt_a / B.bt_b;
       V3 h = normalize(wi * eta + wo);
       if (h.z < 0.0f) h = -h;
       float oh = dot(wo, h), ih = dot(wi, h);
       if (oh * ih > 0.0f) return {0, 0, 0};
-      float F = fr_dielectric(oh, L.etaA, L.etaB);
+      float F = fr_dielectric(oh, B.bt_a, B.bt_b);
       float a = oh + eta * ih, b = 1.0f / eta;
       float k = fabsf(tr_D(L, h) * tr_G(L, wo, wi) * eta * eta * fabsf(ih) * fabsf(oh) * b * b / (wi.z * wo.z * a * a));
       return L.scale * ((1.0f - F) * k);
     }
+    case kDisneyDiffuse: {  // DisneyDiffuseBRDF.java
+      const float a = 1.0f - schlick_w(fabsf(wo.z)) / 2.0f, b = 1.0f - schlick_w(fabsf(wi.z)) / 2.0f;
+      return V3{L.scale.x * (1.0f / kPi) * a * b, L.scale.y * (1.0f / kPi) * a * b, L.scale.z * (1.0f / kPi) * a * b};
+    }
+    case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen: case kDisneyClearCoat: {
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      if (L.kind == kDisneyClearCoat) {  // DisneyClearCoatBRDF.java
+        const float d = gtr1(fabsf(h.z), L.p0);
+        const float f = lerpf(0.04f, 1.0f, schlick_w(dot(wo, h)));
+        const float g = smith_ggx(fabsf(wo.z), 0.25f) * smith_ggx(fabsf(wi.z), 0.25f);
+        const float c = L.p1 * g * f * d / 4.0f;
+        return {c, c, c};
+      }
+      const float cd = dot(wi, h);
+      if (L.kind == kDisneySheen) return L.scale * schlick_w(cd);  // DisneySheenBRDF.java
+      const float co = fabsf(wo.z), ci = fabsf(wi.z), fo = schlick_w(co), fi = schlick_w(ci);
+      if (L.kind == kDisneyRetro) {  // DisneyRetroBRDF.java
+        const float a = 2.0f * L.p0 * cd * cd;
+        const float b = fo + fi + fo * fi * (a - 1.0f);
+        return V3{L.scale.x * (1.0f / kPi) * a * b, L.scale.y * (1.0f / kPi) * a * b, L.scale.z * (1.0f / kPi) * a * b};
+      }
+      const float f90 = cd * cd * L.p0;  // DisneyFakeSSBRDF.java
+      const float fss = lerpf(1.0f, f90, fo) * lerpf(1.0f, f90, fi);
+      const float ss = 1.25f * (fss * (1.0f / (co + ci) - 0.5f) + 0.5f);
+      return V3{L.scale.x * (1.0f / kPi) * ss, L.scale.y * (1.0f / kPi) * ss, L.scale.z * (1.0f / kPi) * ss};
+    }
     default: return {0, 0, 0};
   }
 }
-DFC_D float lobe_pdf(const Lobe& L, V3 wo, V3 wi) {
+DFC_D float lobe_pdf(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
   switch (L.kind) {
-    case kLambert: case kOrenNayar: return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
+    case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
+      return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
+    case kLambertBTDF: return same_hemi(wo, wi) ? 0.0f : fabsf(wi.z) * (1.0f / kPi);
     case kTSBRDF: {
       if (!same_hemi(wo, wi)) return 0.0f;
       V3 h = normalize(wo + wi);
@@ -555,46 +611,56 @@ DFC_D float lobe_pdf(const Lobe& L, V3 wo, V3 wi) {
     }
     case kTSBTDF: {
       if (same_hemi(wo, wi)) return 0.0f;
-      float eta = wo.z > 0.0f ? L.etaB / L.etaA : L.etaA / L.etaB;
+      float eta = wo.z > 0.0f ? B.bt_b / B.bt_a : B.bt_a / B.bt_b;
       V3 h = normalize(wi * eta + wo);
       float oh = dot(wo, h), ih = dot(wi, h);
       if (oh * ih > 0.0f) return 0.0f;
       float a = oh + eta * ih;
       return tr_pdf(L, wo, h) * fabsf((eta * eta * ih) / (a * a));
     }
+    case kDisneyClearCoat: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return 0.0f;
+      h = normalize(h);
+      const float ch = fabsf(h.z);
+      return gtr1(ch, L.p0) * ch / (4.0f * dot(wo, h));
+    }
     default: return 0.0f;
   }
 }
 struct LSample { V3 f, wi; float pdf; int type; };
-DFC_D bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LSample* s) {
+DFC_D bool lobe_sample(const Bsdf& B, const Lobe& L, V3 wo, float u, float v, LSample* s) {
   s->type = L.type;
   switch (L.kind) {
-    case kLambert: case kOrenNayar: {
+    case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
+    case kLambertBTDF: {
       V3 wi = cosine_hemisphere(u, v);
-      if (wo.z < 0.0f) wi.z = -wi.z;
-      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+      // faceForwardZ for reflection, faceForwardZNegated for LambertianBTDF
+      if (L.kind == kLambertBTDF ? wo.z > 0.0f : wo.z < 0.0f) wi.z = -wi.z;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
     }
     case kSpecBRDF: {
       V3 wi = {-wo.x, -wo.y, wo.z};
-      s->wi = wi; s->f = mul(fresnel(L, wi.z), L.scale) * (1.0f / fabsf(wi.z)); s->pdf = 1.0f; return true;
+      s->wi = wi; s->f = mul(fresnel(B, L, wi.z), L.scale) * (1.0f / fabsf(wi.z)); s->pdf = 1.0f; return true;
     }
     case kSpecBTDF: case kFresnelSpec: {
-      float F = L.kind == kFresnelSpec ? fr_dielectric(wo.z, L.etaA, L.etaB) : 0.0f;
+      float F = L.kind == kFresnelSpec ? fr_dielectric(wo.z, B.bt_a, B.bt_b) : 0.0f;
       if (L.kind == kFresnelSpec && u < F) {
         V3 wi = {-wo.x, -wo.y, wo.z};
         s->type = kSpecular | kRefl; s->wi = wi; s->f = L.scale * (F / fabsf(wi.z)); s->pdf = F; return true;
       }
       bool ent = wo.z > 0.0f;
-      float ei = ent ? L.etaA : L.etaB, et = ent ? L.etaB : L.etaA;
+      float ei = ent ? B.bt_a : B.bt_b, et = ent ? B.bt_b : B.bt_a;
       V3 n = wo.z < 0.0f ? V3{0, 0, -1} : V3{0, 0, 1};
       V3 wi;
       if (!refract(wo, n, ei / et, &wi)) return false;
       if (L.kind == kSpecBTDF) {
-        float Ft = fr_dielectric(wi.z, L.etaA, L.etaB);
+        float Ft = fr_dielectric(wi.z, B.bt_a, B.bt_b);
         s->wi = wi; s->f = L.scale * ((1.0f - Ft) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f; return true;
       }
       s->type = kSpecular | kTrans; s->wi = wi;
-      s->f = L.scale2 * ((1.0f - F) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f - F; return true;
+      s->f = B.ca * ((1.0f - F) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f - F; return true;
     }
     case kTSBRDF: {
       if (wo.z == 0.0f) return false;
@@ -602,16 +668,29 @@ DFC_D bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LSample* s) {
       if (dot(wo, h) < 0.0f) return false;
       V3 wi = h * (dot(wo, h) * 2.0f) - wo;
       if (!same_hemi(wo, wi)) return false;
-      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = tr_pdf(L, wo, h) / (4.0f * dot(wo, h)); return true;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = tr_pdf(L, wo, h) / (4.0f * dot(wo, h)); return true;
     }
     case kTSBTDF: {
       if (wo.z == 0.0f) return false;
       V3 h = tr_sample_h(L, wo, u, v);
       if (dot(wo, h) < 0.0f) return false;
-      float eta = wo.z > 0.0f ? L.etaA / L.etaB : L.etaB / L.etaA;
+      float eta = wo.z > 0.0f ? B.bt_a / B.bt_b : B.bt_b / B.bt_a;
       V3 wi;
       if (!refract(wo, h, eta, &wi)) return false;
-      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
+    }
+    case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
+      if (wo.z == 0.0f) return false;
+      const float a2 = L.p0 * L.p0;
+      const float ct = sqrtf(fmaxf(0.0f, (1.0f - powf(a2, 1.0f - u)) / (1.0f - a2)));
+      const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+      float sp, cp;
+      sincosf(2.0f * kPi * v, &sp, &cp);
+      V3 h = {st * cp, st * sp, ct};
+      if (!same_hemi(wo, h)) h = -h;
+      const V3 wi = h * (dot(wo, h) * 2.0f) - wo;
+      if (!same_hemi(wo, wi)) return false;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
     }
   }
   return false;
@@ -619,46 +698,88 @@ DFC_D bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LSample* s) {
 DFC_D bool type_match(int t, int flags) { return (t & flags) == t; }
 DFC_D bool is_spec(int t) { return (t & kSpecular) != 0; }
 
-DFC_D Lobe tr_lobe(int kind, int type, V3 scale, float ax, float ay) {
-  Lobe L = {};
-  L.kind = kind; L.type = type; L.scale = scale; L.ax = fmaxf(ax, 0.001f); L.ay = fmaxf(ay, 0.001f);
+DFC_D Lobe make_lobe(int kind, int type, V3 scale, float p0 = 0.0f, float p1 = 0.0f) {
+  Lobe L;
+  L.kind = (unsigned char)kind; L.type = (unsigned char)type; L.fresnel = kFresConst; L.separable = 0;
+  L.scale = scale; L.p0 = p0; L.p1 = p1;
   return L;
+}
+DFC_D Lobe tr_lobe(int kind, int type, V3 scale, float ax, float ay) { return make_lobe(kind, type, scale, fmaxf(ax, 0.001f), fmaxf(ay, 0.001f)); }
+
+// DisneyMaterial.computeScatteringFunctions (scene/material/DisneyMaterial.java:1121-1210)
+// from the per-material quantities ingest computed (DMaterial comments).
+DFC_D void build_disney(const DMaterial& m, Bsdf* B) {
+  const V3 color = ld3(m.c0);
+  const bool thin = (m.flags & kDisneyThin) != 0;
+  const float dw = m.d_dw;
+  if (dw > 0.0f) {
+    if (thin) {
+      const float flat = m.c2[0], dt = m.c2[1];
+      B->l[B->n++] = make_lobe(kDisneyDiffuse, kRefl | kDiffuse, color * (dw * (1.0f - flat) * (1.0f - dt)));
+      B->l[B->n++] = make_lobe(kDisneyFakeSS, kRefl | kDiffuse, color * (dw * (0.0f + flat) * (1.0f - dt)), m.d_rough);
+    } else if (!(m.flags & kDisneyScatter)) {
+      B->l[B->n++] = make_lobe(kDisneyDiffuse, kRefl | kDiffuse, color * dw);
+    } else {
+      B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, V3{1, 1, 1});
+    }
+    B->l[B->n++] = make_lobe(kDisneyRetro, kRefl | kDiffuse, color * dw, m.d_rough);
+    if (m.flags & kDisneyHasSheen) B->l[B->n++] = make_lobe(kDisneySheen, kRefl | kDiffuse, ld3(m.c3));
+  }
+  Lobe spec = tr_lobe(kTSBRDF, kRefl | kGlossy, V3{1, 1, 1}, m.ax, m.ay);
+  spec.fresnel = kFresDisney;
+  spec.separable = 1;
+  B->l[B->n++] = spec;
+  if (m.flags & kDisneyHasClearCoat) B->l[B->n++] = make_lobe(kDisneyClearCoat, kRefl | kGlossy, V3{0, 0, 0}, m.d_gloss, m.d_cc);
+  if (m.flags & kDisneyHasTransmission) {
+    Lobe t = thin ? tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c4), m.on_a, m.on_b) : tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c4), m.ax, m.ay);
+    t.separable = thin ? 0 : 1;
+    B->l[B->n++] = t;
+  }
+  if (thin) B->l[B->n++] = make_lobe(kLambertBTDF, kTrans | kDiffuse, color * m.c2[1]);
+  B->fr_t = m.eta;
+  B->bt_a = 1.0f; B->bt_b = m.eta;
+  B->metallic = m.d_met;
+  B->ca = ld3(m.c1);
 }
 
 // Material.computeScatteringFunctions(intersection, RADIANCE, isAllowingMultipleLobes = true)
-// for the resolved kinds (scene/material/{Matte,Mirror,Glass,Metal,Plastic}Material.java).
+// for the resolved kinds (scene/material/{Matte,Mirror,Glass,Metal,Plastic,Disney}Material.java).
 DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, Bsdf* B) {
   B->n = 0; B->eta = 1.0f;
+  B->fr_i = 1.0f; B->fr_t = 1.0f; B->bt_a = 1.0f; B->bt_b = 1.0f; B->metallic = 0.0f;
+  B->ca = V3{0, 0, 0}; B->cb = V3{0, 0, 0};
   switch (m.kind) {
-    case kMatLambert: case kMatOrenNayar: {
-      Lobe L = {};
-      L.kind = m.kind == kMatLambert ? kLambert : kOrenNayar; L.type = kRefl | kDiffuse; L.scale = ld3(m.c0); L.a = m.on_a; L.b = m.on_b;
-      B->l[B->n++] = L; break;
-    }
-    case kMatMirror: {
-      Lobe L = {}; L.kind = kSpecBRDF; L.type = kRefl | kSpecular; L.scale = ld3(m.c0); L.fresnel = kFresConst;
-      B->l[B->n++] = L; break;
-    }
-    case kMatGlassSpec: {
-      Lobe L = {}; L.kind = kFresnelSpec; L.type = kRefl | kTrans | kSpecular; L.scale = ld3(m.c0); L.scale2 = ld3(m.c1);
-      L.etaA = 1.0f; L.etaB = m.eta;
-      B->l[B->n++] = L; B->eta = m.eta; break;
-    }
+    case kMatLambert: case kMatOrenNayar:
+      B->l[B->n++] = make_lobe(m.kind == kMatLambert ? kLambert : kOrenNayar, kRefl | kDiffuse, ld3(m.c0), m.on_a, m.on_b);
+      break;
+    case kMatMirror:
+      B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0));
+      break;
+    case kMatGlassSpec:
+      B->l[B->n++] = make_lobe(kFresnelSpec, kRefl | kTrans | kSpecular, ld3(m.c0));
+      B->ca = ld3(m.c1);
+      B->bt_a = 1.0f; B->bt_b = m.eta; B->eta = m.eta;
+      break;
     case kMatGlassRough: {
-      if (m.has_kr) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay); L.fresnel = kFresDielectric; L.etaI = 1.0f; L.etaT = m.eta; B->l[B->n++] = L; }
-      if (m.has_kt) { Lobe L = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c1), m.ax, m.ay); L.etaA = 1.0f; L.etaB = m.eta; B->l[B->n++] = L; }
-      B->eta = m.eta; break;
+      if (m.has_kr) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      if (m.has_kt) B->l[B->n++] = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c1), m.ax, m.ay);
+      B->fr_i = 1.0f; B->fr_t = m.eta; B->bt_a = 1.0f; B->bt_b = m.eta; B->eta = m.eta;
+      break;
     }
     case kMatMetal: {
       Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, V3{1, 1, 1}, m.ax, m.ay);
-      L.fresnel = kFresConductor; L.cEta = ld3(m.c1); L.cK = ld3(m.c2);
-      B->l[B->n++] = L; break;
-    }
-    case kMatPlastic: {
-      if (m.has_kr) { Lobe L = {}; L.kind = kLambert; L.type = kRefl | kDiffuse; L.scale = ld3(m.c0); B->l[B->n++] = L; }
-      if (m.has_kt) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; L.etaI = 1.5f; L.etaT = 1.0f; B->l[B->n++] = L; }
+      L.fresnel = kFresConductor;
+      B->l[B->n++] = L;
+      B->ca = ld3(m.c1); B->cb = ld3(m.c2);
       break;
     }
+    case kMatPlastic: {
+      if (m.has_kr) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
+      if (m.has_kt) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      B->fr_i = 1.5f; B->fr_t = 1.0f;
+      break;
+    }
+    case kMatDisney: build_disney(m, B); break;
     default: return false;
   }
   B->s = sf.s;
@@ -673,7 +794,7 @@ DFC_D V3 bsdf_f(const Bsdf& B, int flags, V3 wi_w) {
   V3 r = {0, 0, 0};
   for (int k = 0; k < B.n; ++k) {
     const Lobe& L = B.l[k];
-    if (type_match(L.type, flags) && ((refl && (L.type & kRefl)) || (!refl && (L.type & kTrans)))) r = r + lobe_f(L, B.wo, wi);
+    if (type_match(L.type, flags) && ((refl && (L.type & kRefl)) || (!refl && (L.type & kTrans)))) r = r + lobe_f(B, L, B.wo, wi);
   }
   return r;
 }
@@ -682,30 +803,35 @@ DFC_D float bsdf_pdf(const Bsdf& B, int flags, V3 wi_w) {
   V3 wi = normalize(to_local(wi_w, B.s));
   float p = 0.0f;
   int m = 0;
-  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) { ++m; p += lobe_pdf(B.l[k], B.wo, wi); }
+  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) { ++m; p += lobe_pdf(B, B.l[k], B.wo, wi); }
   return m > 1 ? p / m : p;
 }
 struct BSample { V3 f, wi; float pdf; int type; };
 // scene/BSDF.java:323 sampleDistributionFunction
 DFC_D bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BSample* out) {
   if (B.wo.z == 0.0f) return false;
-  int idx[2], m = 0;
-  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) idx[m++] = k;
+  int m = 0, match_k = -1;
+  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) ++m;
   if (m == 0) return false;
-  int match = min((int)floorf(u * m), m - 1);
-  const Lobe& L = B.l[idx[match]];
+  const int match = min((int)floorf(u * m), m - 1);
+  for (int k = 0, j = 0; k < B.n; ++k) {
+    if (!type_match(B.l[k].type, flags)) continue;
+    if (j++ == match) { match_k = k; break; }
+  }
+  const Lobe& L = B.l[match_k];
   LSample s;
-  if (!lobe_sample(L, B.wo, fminf(u * m - match, 0.99999994f), v, &s)) return false;
+  if (!lobe_sample(B, L, B.wo, fminf(u * m - match, 0.99999994f), v, &s)) return false;
   V3 wiw = normalize(to_world(s.wi, B.s));
   V3 f = s.f;
   float pdf = s.pdf;
   if (!is_spec(L.type)) {
     bool refl = dot(wiw, B.ng) * dot(B.wo_w, B.ng) > 0.0f;
     f = {0, 0, 0};
-    for (int k = 0; k < m; ++k) {
-      const Lobe& O = B.l[idx[k]];
-      if (k != match) pdf += lobe_pdf(O, B.wo, s.wi);
-      if ((refl && (O.type & kRefl)) || (!refl && (O.type & kTrans))) f = f + lobe_f(O, B.wo, s.wi);
+    for (int k = 0; k < B.n; ++k) {
+      const Lobe& O = B.l[k];
+      if (!type_match(O.type, flags)) continue;
+      if (k != match_k) pdf += lobe_pdf(B, O, B.wo, s.wi);
+      if ((refl && (O.type & kRefl)) || (!refl && (O.type & kTrans))) f = f + lobe_f(B, O, B.wo, s.wi);
     }
   }
   if (m > 1) pdf /= m;

@@ -118,6 +118,7 @@ struct Decoder {
       case kMatGlassId: name = "materialGlassMaterialArray"; break;
       case kMatMetalId: name = "materialMetalMaterialArray"; break;
       case kMatPlasticId: name = "materialPlasticMaterialArray"; break;
+      case kMatDisneyId: name = "materialDisneyMaterialArray"; break;
       default: throw Fail{DFC_E_UNSUPPORTED, "material id " + std::to_string(mid) + " is not supported"};
     }
     const auto& A = I(name);
@@ -181,6 +182,56 @@ struct Decoder {
         m.ax = m.ay = remap ? roughness_to_alpha(r) : r;
         m.has_kr = !black(m.c0); m.has_kt = !black(m.c1);
         m.kind = (m.has_kr || m.has_kt) ? kMatPlastic : kMatNone;
+        break;
+      }
+      case kMatDisneyId: {  // DisneyMaterial.java:1121-1210; record slots CompiledMaterialCache.java:2751-2759
+        int ida, offa, idb, offb;
+        auto f1 = [&](int slot, bool second) {
+          texref(A, moff, slot, &ida, &offa, &idb, &offb);
+          return second ? value(idb, offb) : value(ida, offa);
+        };
+        const float aniso = f1(1, false), cc = f1(2, false), ccg = f1(2, true);
+        texref(A, moff, 3, &ida, &offa, &idb, &offb);
+        float color[3];
+        this->color(ida, offa, color);
+        sat0(color);
+        const float dt = value(idb, offb) / 2.0f;
+        const float eta = f1(4, false), flat = f1(4, true), met = f1(5, false), rough = f1(5, true);
+        texref(A, moff, 6, &ida, &offa, &idb, &offb);
+        float sd[3];
+        this->color(ida, offa, sd);
+        const float sheen = value(idb, offb);
+        const float sheen_tint = f1(7, false), spec_tint = f1(7, true);
+        texref(A, moff, 8, &ida, &offa, &idb, &offb);
+        const float st = value(ida, offa);
+        const bool thin = idb != 0;  // second pair of slot 8: (isThin, 0)
+        auto lerp = [](float a, float b, float t) { return (1.0f - t) * a + t * b; };  // utility/Floats.java:591
+        const float lum = color[0] * 0.212671f + color[1] * 0.715160f + color[2] * 0.072169f;
+        float tint[3];
+        for (int k = 0; k < 3; ++k) tint[k] = lum > 0.0f ? color[k] / lum : 1.0f;
+        m.kind = kMatDisney;
+        m.flags = (thin ? kDisneyThin : 0) | (black(sd) ? 0 : kDisneyScatter) | (sheen > 0.0f ? kDisneyHasSheen : 0) |
+                  (cc > 0.0f ? kDisneyHasClearCoat : 0) | (st > 0.0f ? kDisneyHasTransmission : 0);
+        m.eta = eta;
+        m.d_rough = rough;
+        m.d_met = met;
+        m.d_dw = (1.0f - met) * (1.0f - st);
+        m.c2[0] = flat; m.c2[1] = dt; m.c2[2] = st;
+        const float r0 = ((eta - 1.0f) * (eta - 1.0f)) / ((eta + 1.0f) * (eta + 1.0f));
+        for (int k = 0; k < 3; ++k) {
+          m.c0[k] = color[k];
+          m.c1[k] = lerp(lerp(1.0f, tint[k], spec_tint) * r0, color[k], met);
+          m.c3[k] = sheen > 0.0f ? lerp(1.0f, tint[k], sheen_tint) * (m.d_dw * sheen) : 0.0f;
+          m.c4[k] = std::sqrt(color[k]) * st;
+        }
+        const float aspect = std::sqrt(1.0f - aniso * 0.9f);
+        m.ax = std::fmax(0.001f, rough * rough / aspect);
+        m.ay = std::fmax(0.001f, rough * rough * aspect);
+        const float rs = (0.65f * eta - 0.35f) * rough;
+        m.on_a = std::fmax(0.001f, rs * rs / aspect);
+        m.on_b = std::fmax(0.001f, rs * rs * aspect);
+        m.d_cc = cc;
+        m.d_gloss = lerp(0.1f, 0.001f, ccg);
         break;
       }
     }

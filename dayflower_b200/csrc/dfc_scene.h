@@ -43,8 +43,12 @@ enum : int {
   kMatGlassRough = 5,  // GlassMaterial, rough (TorranceSparrow BRDF + BTDF)
   kMatMetal = 6,       // MetalMaterial
   kMatPlastic = 7,     // PlasticMaterial
-  kMatKinds = 8
+  kMatDisney = 8,      // DisneyMaterial
+  kMatKinds = 9
 };
+
+// DisneyMaterial flags (DMaterial.flags)
+enum : int { kDisneyThin = 1, kDisneyScatter = 2, kDisneyHasSheen = 4, kDisneyHasClearCoat = 8, kDisneyHasTransmission = 16 };
 
 struct alignas(16) DPrim {
   float o2w[12];
@@ -60,21 +64,29 @@ struct alignas(16) DPrim {
 };
 static_assert(sizeof(DPrim) == 128, "DPrim is one 128-byte line");
 
+// One compiled material with its constant textures evaluated.  DisneyMaterial
+// keeps the per-material quantities of DisneyMaterial.computeScatteringFunctions
+// (scene/material/DisneyMaterial.java:1121-1210), computed once at ingest.
 struct alignas(16) DMaterial {
   int kind;
-  int has_kr, has_kt, pad0;
+  int has_kr, has_kt;
+  int flags;       // Disney: kDisney* bits
   float emission[3];
   float eta;
-  float c0[3];     // kd (matte/plastic), kr (mirror/glass), unused (metal)
+  float c0[3];     // kd (matte/plastic), kr (mirror/glass), unused (metal), Disney colour
   float ax;
-  float c1[3];     // ks (plastic), kt (glass), metal eta
+  float c1[3];     // ks (plastic), kt (glass), metal eta, Disney specular R0 (DisneyFresnel)
   float ay;
-  float c2[3];     // metal k
-  float on_a;
-  float on_b;
-  float pad1[3];
+  float c2[3];     // metal k; Disney (flatness, diffuse transmission / 2, specular transmission)
+  float on_a;      // Oren-Nayar A; Disney thin transmission alpha x
+  float on_b;      // Oren-Nayar B; Disney thin transmission alpha y
+  float d_rough, d_met, d_dw;  // Disney roughness, metallic, diffuse weight (1 - metallic)(1 - specular transmission)
+  float c3[3];     // Disney sheen lobe scale
+  float d_cc;      // Disney clear coat weight
+  float c4[3];     // Disney transmission scale sqrt(colour) * specular transmission
+  float d_gloss;   // Disney clear coat alpha lerp(0.1, 0.001, gloss)
 };
-static_assert(sizeof(DMaterial) == 96, "DMaterial layout");
+static_assert(sizeof(DMaterial) == 128, "DMaterial layout");
 
 struct alignas(16) DLight {
   int type;

@@ -179,6 +179,15 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
         elif isinstance(m, M.Plastic):
             rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness] * 3))) + plain(m.remap_roughness)
             name, length = "materialPlasticMaterialArray", 4
+        elif isinstance(m, M.Disney):
+            # CompiledMaterialCache.toDisneyMaterial (:2717-2760): nine packed slots of a 16-slot record
+            def ft(v):
+                return (T, tex([v] * 3))
+            rec = head + slot(ft(m.anisotropic)) + slot(ft(m.clear_coat), ft(m.clear_coat_gloss)) + \
+                slot((T, tex(m.color)), ft(m.diffuse_transmission)) + slot(ft(m.eta), ft(m.flatness)) + \
+                slot(ft(m.metallic), ft(m.roughness)) + slot((T, tex(m.scatter_distance)), ft(m.sheen)) + \
+                slot(ft(m.sheen_tint), ft(m.specular_tint)) + slot(ft(m.specular_transmission), (1 if m.thin else 0, 0))
+            name, length = "materialDisneyMaterialArray", 16
         else:
             raise ValueError("unsupported material %r" % type(m).__name__)
         off = push(name, pad_to(rec, length))

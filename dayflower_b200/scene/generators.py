@@ -114,7 +114,8 @@ def _height_at(hf, x, z):
 
 def terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2, extent=100.0, turbidity=2.5,
                     sun_elevation_deg=35.0, sun_azimuth_deg=40.0, kinds=(0, 1, 2, 3)) -> M.Scene:
-    """kinds: allowed sphere materials, 0 matte, 1 plastic, 2 metal, 3 glass (drawn uniformly)."""
+    """kinds: allowed sphere materials, 0 matte, 1 plastic, 2 metal, 3 glass, 4 Disney (base colour, metallic
+    and roughness uniform), drawn uniformly."""
     mesh, hf = heightfield_mesh(cells, extent, seed)
     rng = np.random.default_rng(seed + 1000)
     cam = M.Camera(eye=(0.0, 0.30 * extent, 0.62 * extent), look_at=(0.0, 0.0, -0.05 * extent), fov_x_deg=55.0,
@@ -135,8 +136,10 @@ def terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2,
             mat = M.Plastic(kd=col, ks=(0.5, 0.5, 0.5), roughness=rough)
         elif kinds[k] == 2:
             mat = M.Metal(roughness_u=rough, roughness_v=rough)
-        else:
+        elif kinds[k] == 3:
             mat = M.Glass(eta=1.5, roughness_u=rough, roughness_v=rough)
+        else:
+            mat = M.Disney(color=col, metallic=float(rng.uniform(0.0, 1.0)), roughness=rough)
         sc.add(M.Primitive(M.Sphere(), mat, M.Transform.translate_scale((xs[k], ys[k], zs[k]), radii[k])))
     el, az = math.radians(sun_elevation_deg), math.radians(sun_azimuth_deg)
     sun = (math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az))
@@ -165,6 +168,41 @@ def small_mixed_scene(resolution=(96, 64), seed=7, cells=24, n_spheres=24, with_
         sc.lights.append(sl)
         sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((5.0, 6.0, 1.0), 0.7), area_light=sl))
     del rng
+    return sc
+
+
+def disney_scene(resolution=(96, 72), with_lights=True) -> M.Scene:
+    """Spheres of DisneyMaterial covering every lobe combination the material
+    builds (DisneyMaterial.java:1121-1210): diffuse + retro, sheen, metallic and
+    anisotropic specular, clear coat, rough transmission, the scatter-distance
+    specular transmission, and thin sheets with flatness and diffuse
+    transmission; on a matte ground plane, lit by a point light, a spherical
+    area light and a triangle area light."""
+    cam = M.Camera(eye=(0.0, 3.0, 10.0), look_at=(0.0, 1.0, 0.0), fov_x_deg=60.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="disney")
+    mats = [
+        M.Disney(color=(0.8, 0.3, 0.2), roughness=0.5),
+        M.Disney(color=(0.2, 0.6, 0.8), roughness=0.3, sheen=1.0, sheen_tint=0.7),
+        M.Disney(color=(0.9, 0.7, 0.3), metallic=1.0, roughness=0.25, anisotropic=0.6),
+        M.Disney(color=(0.3, 0.8, 0.3), roughness=0.4, clear_coat=1.0, clear_coat_gloss=0.8, specular_tint=0.5),
+        M.Disney(color=(0.9, 0.9, 0.9), roughness=0.2, specular_transmission=0.9, eta=1.5),
+        M.Disney(color=(0.7, 0.5, 0.9), roughness=0.4, scatter_distance=(0.5, 0.5, 0.5)),
+        M.Disney(color=(0.6, 0.8, 0.4), roughness=0.6, thin=True, flatness=0.5, diffuse_transmission=0.8, sheen=0.5),
+        M.Disney(color=(0.8, 0.8, 0.6), roughness=0.3, thin=True, specular_transmission=0.5, metallic=0.2, clear_coat=0.5),
+    ]
+    for k, m in enumerate(mats):
+        x = -5.25 + 1.5 * k
+        sc.add(M.Primitive(M.Sphere(), m, M.Transform.translate_scale((x, 0.7, 0.0), 0.7)))
+    sc.add(M.Primitive(M.Plane(), M.Matte(kd=(0.5, 0.5, 0.5)), _rot_x(-90.0, (0.0, 0.0, 0.0))))
+    if with_lights:
+        sc.lights.append(M.PointLight((2.0, 6.0, 5.0), (40.0, 40.0, 40.0)))
+        sl = M.DiffuseAreaLight(M.Sphere(), (6.0, 5.0, 4.0), transform=M.Transform.translate_scale((-3.0, 5.0, 3.0), 0.6))
+        sc.lights.append(sl)
+        sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((-3.0, 5.0, 3.0), 0.6), area_light=sl))
+        tri = M.Triangle((3, 5, -2), (5, 5, -2), (4, 6, 1))
+        al = M.DiffuseAreaLight(tri, (5.0, 5.0, 5.0))
+        sc.lights.append(al)
+        sc.add(M.Primitive(tri, M.Matte(kd=(0.0, 0.0, 0.0)), area_light=al))
     return sc
 
 
@@ -216,9 +254,9 @@ JOB_MIX_CELLS = [71, 103, 151, 220, 321, 468, 684, 1000]  # 2 * cells^2 = 10,082
 JOB_MIX_CELL_ORDER = [3, 7, 0, 5, 1, 6, 2, 4]
 
 
-def job_mix_scene(index: int, seed: int = 300, resolution=(512, 512), kinds=(0, 1, 2, 3)) -> M.Scene:
+def job_mix_scene(index: int, seed: int = 300, resolution=(512, 512), kinds=(0, 1, 2, 3, 4)) -> M.Scene:
     """Scene `index` (0..7) of the batched-job mix: a fractal heightfield and
-    log-uniform spheres of random matte/plastic/metal/glass materials, lit by a
+    log-uniform spheres of random matte/plastic/metal/glass/Disney materials, lit by a
     point light, a spot light and a rectangular area light made of two
     triangles (the CPU renderer samples area lights on triangles and spheres
     only)."""

@@ -353,6 +353,28 @@ class Plastic(Material):
     ID = MAT_PLASTIC
 
 
+@dataclass(eq=False)
+class Disney(Material):
+    """``scene/material/DisneyMaterial`` with constant textures; the defaults are
+    those of its constructor chain (DisneyMaterial.java:111-520)."""
+    color: Sequence[float] = (0.5, 0.5, 0.5)
+    scatter_distance: Sequence[float] = (0.0, 0.0, 0.0)
+    anisotropic: float = 0.0
+    clear_coat: float = 0.0
+    clear_coat_gloss: float = 1.0
+    diffuse_transmission: float = 1.0
+    eta: float = 1.5
+    flatness: float = 0.0
+    metallic: float = 0.0
+    roughness: float = 0.5
+    sheen: float = 0.0
+    sheen_tint: float = 0.5
+    specular_tint: float = 0.0
+    specular_transmission: float = 0.0
+    thin: bool = False
+    ID = MAT_DISNEY
+
+
 # ---------------------------------------------------------------- lights ----
 class Light:
     ID = 0

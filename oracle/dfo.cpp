@@ -808,20 +808,33 @@ inline V3 mul(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
 // scene/BXDFType.java flags
 enum { kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossy = 8, kSpecular = 16, kAll = 31, kAllButSpecular = 15 };
 
-enum LobeKind { kLambert, kOrenNayar, kSpecBRDF, kFresnelSpec, kSpecBTDF, kTSBRDF, kTSBTDF };
-enum FresKind { kFresConst, kFresDielectric, kFresConductor };
+enum LobeKind {
+  kLambert, kOrenNayar, kSpecBRDF, kFresnelSpec, kSpecBTDF, kTSBRDF, kTSBTDF,
+  kLambertBTDF,                                                                    // scene/bxdf/LambertianBTDF.java
+  kDisneyDiffuse, kDisneyFakeSS, kDisneyRetro, kDisneySheen, kDisneyClearCoat      // scene/bxdf/Disney*BRDF.java
+};
+enum FresKind { kFresConst, kFresDielectric, kFresConductor, kFresDisney };
 struct Lobe {
   LobeKind kind; int type;
   V3 scale;            // reflectance / transmittance scale
   float a = 0, b = 0;  // Oren-Nayar A/B
   FresKind fk = kFresConst; float etaI = 1, etaT = 1; V3 cEtaI{1, 1, 1}, cEtaT{1, 1, 1}, cK{0, 0, 0};
   float ax = 0, ay = 0;  // microfacet alphas
+  bool separable = false;  // MicrofacetDistribution.isSeparableModel: G = G1(wo) G1(wi)
   float etaA = 1, etaB = 1;
+  float roughness = 0;     // Disney retro / fake subsurface
+  float gloss = 0, weight = 0;  // Disney clear coat
+  V3 r0{0, 0, 0}; float metallic = 0;  // DisneyFresnel(r0, etaT, metallic)
 };
+constexpr int kMaxLobes = 8;
 struct Bsdf {
-  int n = 0; Lobe l[2]; float eta = 1.0f; bool present = false;
+  int n = 0; Lobe l[kMaxLobes]; float eta = 1.0f; bool present = false;
   ONB s; V3 ng; V3 wo_world; V3 wo; V3 nl;
 };
+
+// scene/fresnel/Schlick.java:104 fresnelWeight
+inline float schlick_weight(float c) { float m = saturate(1.0f - c, 0.0f, 1.0f); return (m * m) * (m * m) * m; }
+inline float lerpf(float a, float b, float t) { return (1.0f - t) * a + t * b; }  // utility/Floats.java:591
 
 // scene/fresnel/DielectricFresnel.java:evaluate
 inline float fresnel_dielectric(float cosi, float etaI, float etaT) {
@@ -861,6 +874,12 @@ inline V3 fresnel_eval(const Lobe& L, float cosi) {
       float c = std::fabs(cosi);
       return {fresnel_conductor1(c, L.cEtaI.x, L.cEtaT.x, L.cK.x), fresnel_conductor1(c, L.cEtaI.y, L.cEtaT.y, L.cK.y), fresnel_conductor1(c, L.cEtaI.z, L.cEtaT.z, L.cK.z)};
     }
+    case kFresDisney: {  // scene/fresnel/DisneyFresnel.java:evaluate
+      const float d = fresnel_dielectric(cosi, 1.0f, L.etaT);
+      const float w = schlick_weight(cosi);
+      const V3 s = {lerpf(L.r0.x, 1.0f, w), lerpf(L.r0.y, 1.0f, w), lerpf(L.r0.z, 1.0f, w)};
+      return {lerpf(d, s.x, L.metallic), lerpf(d, s.y, L.metallic), lerpf(d, s.z, L.metallic)};
+    }
   }
   return {0, 0, 0};
 }
@@ -892,7 +911,9 @@ inline float tr_lambda(const Lobe& L, V3 w) {
   return (-1.0f + std::sqrt(1.0f + x)) / 2.0f;
 }
 inline float tr_G1(const Lobe& L, V3 w) { return 1.0f / (1.0f + tr_lambda(L, w)); }
-inline float tr_G(const Lobe& L, V3 wo, V3 wi) { return 1.0f / (1.0f + tr_lambda(L, wo) + tr_lambda(L, wi)); }
+inline float tr_G(const Lobe& L, V3 wo, V3 wi) {
+  return L.separable ? (1.0f / (1.0f + tr_lambda(L, wo))) * (1.0f / (1.0f + tr_lambda(L, wi))) : 1.0f / (1.0f + tr_lambda(L, wo) + tr_lambda(L, wi));
+}
 inline float tr_pdf(const Lobe& L, V3 wo, V3 h) { return tr_D(L, h) * tr_G1(L, wo) * std::fabs(dot(wo, h)) / std::fabs(cos_t(wo)); }
 inline void tr_slope(float ct, float u, float v, float* sx, float* sy) {
   if (ct > 0.9999f) {
@@ -953,6 +974,16 @@ inline V3 uniform_hemisphere(float u, float v) {
   return {st * std::cos(phi), st * std::sin(phi), ct};
 }
 
+// DisneyClearCoatBRDF.java:330 doGTR1, :337 doSmithGGGX
+inline float gtr1(float ct, float alpha) {
+  const float a = alpha * alpha;
+  return (a - 1.0f) / (kPi * std::log(a) * (1.0f + (a - 1.0f) * ct * ct));
+}
+inline float smith_ggx(float ct, float alpha) {
+  const float a = alpha * alpha, b = ct * ct;
+  return 1.0f / (ct + std::sqrt(a + b - a * b));
+}
+
 // BXDF.evaluateDistributionFunction
 inline V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
   switch (L.kind) {
@@ -992,12 +1023,56 @@ inline V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
       float k = std::fabs(D * G * eta * eta * std::fabs(ih) * std::fabs(oh) * b * b / (cti * cto * a * a));
       return L.scale * (1.0f - F) * k;
     }
+    case kLambertBTDF: return L.scale * (1.0f / kPi);
+    case kDisneyDiffuse: {  // DisneyDiffuseBRDF.java:evaluateDistributionFunction
+      const float fo = schlick_weight(std::fabs(cos_t(wo))), fi = schlick_weight(std::fabs(cos_t(wi)));
+      const float a = 1.0f - fo / 2.0f, b = 1.0f - fi / 2.0f;
+      return {L.scale.x * (1.0f / kPi) * a * b, L.scale.y * (1.0f / kPi) * a * b, L.scale.z * (1.0f / kPi) * a * b};
+    }
+    case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen: {
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      const float cd = dot(wi, h);
+      if (L.kind == kDisneySheen) return L.scale * schlick_weight(cd);  // DisneySheenBRDF.java
+      const float co = std::fabs(cos_t(wo)), ci = std::fabs(cos_t(wi));
+      const float fo = schlick_weight(co), fi = schlick_weight(ci);
+      if (L.kind == kDisneyRetro) {  // DisneyRetroBRDF.java
+        const float a = 2.0f * L.roughness * cd * cd;
+        const float b = fo + fi + fo * fi * (a - 1.0f);
+        return {L.scale.x * (1.0f / kPi) * a * b, L.scale.y * (1.0f / kPi) * a * b, L.scale.z * (1.0f / kPi) * a * b};
+      }
+      const float f90 = cd * cd * L.roughness;  // DisneyFakeSSBRDF.java
+      const float fss = lerpf(1.0f, f90, fo) * lerpf(1.0f, f90, fi);
+      const float ss = 1.25f * (fss * (1.0f / (co + ci) - 0.5f) + 0.5f);
+      return {L.scale.x * (1.0f / kPi) * ss, L.scale.y * (1.0f / kPi) * ss, L.scale.z * (1.0f / kPi) * ss};
+    }
+    case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      const float d = gtr1(std::fabs(cos_t(h)), L.gloss);
+      const float f = lerpf(0.04f, 1.0f, schlick_weight(dot(wo, h)));
+      const float g = smith_ggx(std::fabs(cos_t(wo)), 0.25f) * smith_ggx(std::fabs(cos_t(wi)), 0.25f);
+      const float c = L.weight * g * f * d / 4.0f;
+      return {c, c, c};
+    }
     default: return {0, 0, 0};  // specular lobes
   }
 }
 inline float lobe_pdf(const Lobe& L, V3 wo, V3 wi) {
   switch (L.kind) {
-    case kLambert: case kOrenNayar: return same_hemi(wo, wi) ? std::fabs(cos_t(wi)) * (1.0f / kPi) : 0.0f;
+    case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
+      return same_hemi(wo, wi) ? std::fabs(cos_t(wi)) * (1.0f / kPi) : 0.0f;
+    case kLambertBTDF: return same_hemi(wo, wi) ? 0.0f : std::fabs(cos_t(wi)) * (1.0f / kPi);
+    case kDisneyClearCoat: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return 0.0f;
+      h = normalize(h);
+      const float ch = std::fabs(cos_t(h));
+      return gtr1(ch, L.gloss) * ch / (4.0f * dot(wo, h));
+    }
     case kTSBRDF: {
       if (!same_hemi(wo, wi)) return 0.0f;
       V3 h = normalize(wo + wi);
@@ -1020,9 +1095,26 @@ struct LobeSample { V3 f; V3 wi; float pdf; int type; };
 inline bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LobeSample* s) {
   s->type = L.type;
   switch (L.kind) {
-    case kLambert: case kOrenNayar: {
+    case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen: {
       V3 wi = cosine_hemisphere(u, v);
       if (wo.z < 0.0f) wi.z = -wi.z;  // faceForwardZ
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+    }
+    case kLambertBTDF: {
+      V3 wi = cosine_hemisphere(u, v);
+      if (wo.z > 0.0f) wi.z = -wi.z;  // faceForwardZNegated
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+    }
+    case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
+      if (wo.z == 0.0f) return false;
+      const float a2 = L.gloss * L.gloss;
+      const float ct = std::sqrt(std::fmax(0.0f, (1.0f - std::pow(a2, 1.0f - u)) / (1.0f - a2)));
+      const float st = std::sqrt(std::fmax(0.0f, 1.0f - ct * ct));
+      const float phi = 2.0f * kPi * v;
+      V3 h = {st * std::cos(phi), st * std::sin(phi), ct};
+      if (!same_hemi(wo, h)) h = -h;
+      const V3 wi = reflect_about(wo, h);
+      if (!same_hemi(wo, wi)) return false;
       s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
     }
     case kSpecBRDF: {
@@ -1166,6 +1258,74 @@ inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool mu
       if (B->n == 0) return false;
       break;
     }
+    case kMatDisney: {  // scene/material/DisneyMaterial.java:1121-1210 (ConstantTexture values)
+      const auto& M = sc.I("materialDisneyMaterialArray");
+      TexRef t_aniso, t_z, t_cc, t_ccg, t_color, t_dt, t_eta, t_flat, t_met, t_rough, t_sd, t_sheen, t_sheen_tint, t_spec_tint, t_st, t_thin;
+      material_slot(sc, M, moff, 1, &t_aniso, &t_z);  // CompiledMaterialCache.java:2751-2759
+      material_slot(sc, M, moff, 2, &t_cc, &t_ccg);
+      material_slot(sc, M, moff, 3, &t_color, &t_dt);
+      material_slot(sc, M, moff, 4, &t_eta, &t_flat);
+      material_slot(sc, M, moff, 5, &t_met, &t_rough);
+      material_slot(sc, M, moff, 6, &t_sd, &t_sheen);
+      material_slot(sc, M, moff, 7, &t_sheen_tint, &t_spec_tint);
+      material_slot(sc, M, moff, 8, &t_st, &t_thin);  // second pair: (isThin, 0)
+      const bool thin = t_thin.id != 0;
+      const float aniso = tex_float(sc, t_aniso), cc = tex_float(sc, t_cc), dt = tex_float(sc, t_dt) / 2.0f;
+      const float eta = tex_float(sc, t_eta), met = tex_float(sc, t_met), rough = tex_float(sc, t_rough);
+      const float sheen = tex_float(sc, t_sheen), spec_tint = tex_float(sc, t_spec_tint), st = tex_float(sc, t_st);
+      const V3 color = sat0(tex_color(sc, t_color));
+      const float lum = color.x * 0.212671f + color.y * 0.715160f + color.z * 0.072169f;  // Color3F.relativeLuminance
+      const V3 tint = lum > 0.0f ? V3{color.x / lum, color.y / lum, color.z / lum} : V3{1, 1, 1};
+      const float sht = tex_float(sc, t_sheen_tint);
+      const V3 sheen_c = sheen > 0.0f ? V3{lerpf(1.0f, tint.x, sht), lerpf(1.0f, tint.y, sht), lerpf(1.0f, tint.z, sht)} : V3{0, 0, 0};
+      const float dw = (1.0f - met) * (1.0f - st);
+      auto add = [&](Lobe L) { B->l[B->n++] = L; };
+      auto diffuse_lobe = [](LobeKind k, V3 scale, float r) { Lobe L{}; L.kind = k; L.type = kRefl | kDiffuse; L.scale = scale; L.roughness = r; return L; };
+      if (dw > 0.0f) {
+        if (thin) {
+          const float flat = tex_float(sc, t_flat);
+          add(diffuse_lobe(kDisneyDiffuse, color * (dw * (1.0f - flat) * (1.0f - dt)), 0.0f));
+          add(diffuse_lobe(kDisneyFakeSS, color * (dw * (0.0f + flat) * (1.0f - dt)), rough));
+        } else if (black(tex_color(sc, t_sd))) {
+          add(diffuse_lobe(kDisneyDiffuse, color * dw, 0.0f));
+        } else {
+          Lobe L{}; L.kind = kSpecBTDF; L.type = kTrans | kSpecular; L.scale = {1, 1, 1}; L.etaA = 1.0f; L.etaB = eta; add(L);
+        }
+        add(diffuse_lobe(kDisneyRetro, color * dw, rough));
+        if (sheen > 0.0f) add(diffuse_lobe(kDisneySheen, sheen_c * (dw * sheen), 0.0f));
+      }
+      const float aspect = std::sqrt(1.0f - aniso * 0.9f);
+      const float ax = std::fmax(0.001f, rough * rough / aspect), ay = std::fmax(0.001f, rough * rough * aspect);
+      const float r0 = ((eta - 1.0f) * (eta - 1.0f)) / ((eta + 1.0f) * (eta + 1.0f));
+      const V3 tinted = V3{lerpf(1.0f, tint.x, spec_tint), lerpf(1.0f, tint.y, spec_tint), lerpf(1.0f, tint.z, spec_tint)} * r0;
+      {
+        Lobe L = make_tr_lobe(kTSBRDF, kRefl | kGlossy, V3{1, 1, 1}, ax, ay);
+        L.separable = true;
+        L.fk = kFresDisney; L.etaT = eta; L.metallic = met;
+        L.r0 = {lerpf(tinted.x, color.x, met), lerpf(tinted.y, color.y, met), lerpf(tinted.z, color.z, met)};
+        add(L);
+      }
+      if (cc > 0.0f) {
+        Lobe L{}; L.kind = kDisneyClearCoat; L.type = kRefl | kGlossy; L.gloss = lerpf(0.1f, 0.001f, tex_float(sc, t_ccg)); L.weight = cc;
+        add(L);
+      }
+      if (st > 0.0f) {
+        const V3 ts = V3{std::sqrt(color.x), std::sqrt(color.y), std::sqrt(color.z)} * st;
+        Lobe L;
+        if (thin) {
+          const float rs = (0.65f * eta - 0.35f) * rough;
+          L = make_tr_lobe(kTSBTDF, kTrans | kGlossy, ts, std::fmax(0.001f, rs * rs / aspect), std::fmax(0.001f, rs * rs * aspect));
+          L.separable = false;
+        } else {
+          L = make_tr_lobe(kTSBTDF, kTrans | kGlossy, ts, ax, ay);
+          L.separable = true;
+        }
+        L.etaA = 1.0f; L.etaB = eta;
+        add(L);
+      }
+      if (thin) { Lobe L{}; L.kind = kLambertBTDF; L.type = kTrans | kDiffuse; L.scale = color * dt; add(L); }
+      break;
+    }
     default: *supported = false; return false;
   }
   B->present = true;
@@ -1185,6 +1345,7 @@ inline V3 material_emission(const Scene& sc, int mid, int moff) {
     case kMatGlass: name = "materialGlassMaterialArray"; break;
     case kMatMetal: name = "materialMetalMaterialArray"; break;
     case kMatPlastic: name = "materialPlasticMaterialArray"; break;
+    case kMatDisney: name = "materialDisneyMaterialArray"; break;
     default: return {0, 0, 0};
   }
   TexRef a, b;
@@ -1216,7 +1377,7 @@ inline float bsdf_pdf(const Bsdf& B, int flags, V3 wi_world) {
 struct BsdfSample { V3 f; V3 wi; float pdf; int type; };
 inline bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BsdfSample* out) {
   if (B.wo.z == 0.0f) return false;
-  int idx[2]; int m = 0;
+  int idx[kMaxLobes]; int m = 0;
   for (int k = 0; k < B.n; ++k) if (type_matches(B.l[k].type, flags)) idx[m++] = k;
   if (m == 0) return false;
   int match = std::min((int)std::floor(u * m), m - 1);

@@ -27,11 +27,16 @@ def quadrics():
 
 
 @pytest.fixture(scope="module")
+def disney():
+    return compile_scene(G.disney_scene(resolution=(128, 72)))
+
+
+@pytest.fixture(scope="module")
 def terrain():
     return compile_scene(G.terrain_spheres(cells=128, n_spheres=300, resolution=(160, 90), seed=11), layout_version=2)
 
 
-@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics"])
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney"])
 def test_ray_casting_hit_ids(scene_name, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.RAY_CASTING)
@@ -55,7 +60,7 @@ def test_depth_camera(scene_name, request):
     assert np.mean(np.all(np.abs(mg - mo) <= 1e-4 + 1e-4 * np.abs(mo), axis=-1)) >= 0.999
 
 
-@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16)])
+@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16)])
 def test_path_tracing_sigma(scene_name, spp, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.PATH_TRACING, spp=spp, max_bounce=8)
