@@ -80,7 +80,7 @@ DFC_D float rng_uniform(uint32_t key, uint32_t dim) {
 enum : uint32_t {
   kDimPixelX = 0, kDimPixelY = 1, kDimLensU = 2, kDimLensV = 3, kDimBounceBase = 8, kDimBounceStride = 16,
   kDimLightPick = 0, kDimLightSampleU = 1, kDimLightSampleV = 2, kDimMisSampleU = 3, kDimMisSampleV = 4,
-  kDimSunPick = 5, kDimBsdfU = 6, kDimBsdfV = 7, kDimRoulette = 8,
+  kDimSunPick = 5, kDimBsdfU = 6, kDimBsdfV = 7, kDimRoulette = 8, kDimMaterial = 9,
 };
 DFC_D uint32_t bounce_dim(int b, uint32_t w) { return kDimBounceBase + (uint32_t)b * kDimBounceStride + w; }
 
@@ -400,6 +400,7 @@ enum { kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossy = 8, kSpecular = 16, kAll = 
 enum : int {
   kLambert = 0, kOrenNayar = 1, kSpecBRDF = 2, kFresnelSpec = 3, kSpecBTDF = 4, kTSBRDF = 5, kTSBTDF = 6,
   kLambertBTDF = 7,                                                                   // scene/bxdf/LambertianBTDF.java
+  kFresnelBlend = 13,                                                                 // scene/bxdf/FresnelBlendBRDF.java
   kDisneyDiffuse = 8, kDisneyFakeSS = 9, kDisneyRetro = 10, kDisneySheen = 11, kDisneyClearCoat = 12  // scene/bxdf/Disney*.java
 };
 enum : int { kFresConst = 0, kFresDielectric = 1, kFresConductor = 2, kFresDisney = 3 };
@@ -410,7 +411,7 @@ constexpr int kMaxLobes = 8;  // DisneyMaterial, thin: diffuse, fake subsurface,
 struct Lobe {
   unsigned char kind, type, fresnel, separable;  // separable: G = G1(wo) G1(wi) (MicrofacetDistribution.isSeparableModel)
   V3 scale;
-  float p0, p1;  // Oren-Nayar A, B | microfacet alpha x, y | Disney roughness | clear coat alpha, weight
+  float p0, p1;  // Oren-Nayar A, B | microfacet alpha x, y | Disney roughness | clear coat alpha, weight | specular BTDF etaA, etaB
 };
 struct Bsdf {
   int n;
@@ -419,7 +420,7 @@ struct Bsdf {
   float fr_i, fr_t;     // dielectric Fresnel of reflection lobes (Disney: etaT)
   float bt_a, bt_b;     // etaA, etaB of transmission lobes
   float metallic;       // DisneyFresnel blend
-  V3 ca, cb;            // conductor eta and k | Disney R0 | FresnelSpecular transmittance (ca)
+  V3 ca, cb;            // conductor eta and k | Disney R0 | FresnelSpecular transmittance (ca) | FresnelBlend specular (ca)
   ONB s;
   V3 ng, wo_w, wo;
 };
@@ -568,6 +569,20 @@ DFC_D V3 lobe_f(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
       float k = fabsf(tr_D(L, h) * tr_G(L, wo, wi) * eta * eta * fabsf(ih) * fabsf(oh) * b * b / (wi.z * wo.z * a * a));
       return L.scale * ((1.0f - F) * k);
     }
+    case kFresnelBlend: {  // FresnelBlendBRDF.java (scale: diffuse, Bsdf.ca: specular)
+      V3 h = wo + wi;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      auto pow5 = [](float x) { return x * x * x * x * x; };
+      const float a = 28.0f / (23.0f * kPi);
+      const float b = 1.0f - pow5(1.0f - 0.5f * fabsf(wi.z));
+      const float c = 1.0f - pow5(1.0f - 0.5f * fabsf(wo.z));
+      const float f = tr_D(L, h) / (4.0f * fabsf(dot(wi, h)) * fmaxf(fabsf(wi.z), fabsf(wo.z)));
+      const float w = pow5(1.0f - dot(wi, h));
+      const V3 ks = B.ca;
+      const V3 fr = {ks.x + (1.0f - ks.x) * w, ks.y + (1.0f - ks.y) * w, ks.z + (1.0f - ks.z) * w};
+      return mul(L.scale * a, V3{1.0f - ks.x, 1.0f - ks.y, 1.0f - ks.z}) * b * c + fr * f;
+    }
     case kDisneyDiffuse: {  // DisneyDiffuseBRDF.java
       const float a = 1.0f - schlick_w(fabsf(wo.z)) / 2.0f, b = 1.0f - schlick_w(fabsf(wi.z)) / 2.0f;
       return V3{L.scale.x * (1.0f / kPi) * a * b, L.scale.y * (1.0f / kPi) * a * b, L.scale.z * (1.0f / kPi) * a * b};
@@ -604,6 +619,11 @@ DFC_D float lobe_pdf(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
     case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
       return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
     case kLambertBTDF: return same_hemi(wo, wi) ? 0.0f : fabsf(wi.z) * (1.0f / kPi);
+    case kFresnelBlend: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      const V3 h = normalize(wo + wi);
+      return 0.5f * (fabsf(wi.z) * (1.0f / kPi) + tr_pdf(L, wo, h) / (4.0f * dot(wo, h)));
+    }
     case kTSBRDF: {
       if (!same_hemi(wo, wi)) return 0.0f;
       V3 h = normalize(wo + wi);
@@ -645,18 +665,20 @@ DFC_D bool lobe_sample(const Bsdf& B, const Lobe& L, V3 wo, float u, float v, LS
       s->wi = wi; s->f = mul(fresnel(B, L, wi.z), L.scale) * (1.0f / fabsf(wi.z)); s->pdf = 1.0f; return true;
     }
     case kSpecBTDF: case kFresnelSpec: {
-      float F = L.kind == kFresnelSpec ? fr_dielectric(wo.z, B.bt_a, B.bt_b) : 0.0f;
+      // SpecularBTDF carries its own etas (UberMaterial has two with different ones)
+      const float ea = L.kind == kSpecBTDF ? L.p0 : B.bt_a, eb = L.kind == kSpecBTDF ? L.p1 : B.bt_b;
+      float F = L.kind == kFresnelSpec ? fr_dielectric(wo.z, ea, eb) : 0.0f;
       if (L.kind == kFresnelSpec && u < F) {
         V3 wi = {-wo.x, -wo.y, wo.z};
         s->type = kSpecular | kRefl; s->wi = wi; s->f = L.scale * (F / fabsf(wi.z)); s->pdf = F; return true;
       }
       bool ent = wo.z > 0.0f;
-      float ei = ent ? B.bt_a : B.bt_b, et = ent ? B.bt_b : B.bt_a;
+      float ei = ent ? ea : eb, et = ent ? eb : ea;
       V3 n = wo.z < 0.0f ? V3{0, 0, -1} : V3{0, 0, 1};
       V3 wi;
       if (!refract(wo, n, ei / et, &wi)) return false;
       if (L.kind == kSpecBTDF) {
-        float Ft = fr_dielectric(wi.z, B.bt_a, B.bt_b);
+        float Ft = fr_dielectric(wi.z, ea, eb);
         s->wi = wi; s->f = L.scale * ((1.0f - Ft) * ((ei * ei) / (et * et)) / fabsf(wi.z)); s->pdf = 1.0f; return true;
       }
       s->type = kSpecular | kTrans; s->wi = wi;
@@ -677,6 +699,18 @@ DFC_D bool lobe_sample(const Bsdf& B, const Lobe& L, V3 wo, float u, float v, LS
       float eta = wo.z > 0.0f ? B.bt_a / B.bt_b : B.bt_b / B.bt_a;
       V3 wi;
       if (!refract(wo, h, eta, &wi)) return false;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
+    }
+    case kFresnelBlend: {  // FresnelBlendBRDF.java:sampleDistributionFunction
+      V3 wi;
+      if (u < 0.5f) {
+        wi = cosine_hemisphere(fminf(2.0f * u, 0.99999994f), v);
+        if (wo.z < 0.0f) wi.z = -wi.z;
+      } else {
+        const V3 h = tr_sample_h(L, wo, fminf(2.0f * (u - 0.5f), 0.99999994f), v);
+        wi = h * (dot(wo, h) * 2.0f) - wo;
+        if (!same_hemi(wo, wi)) return false;
+      }
       s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
     }
     case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
@@ -720,7 +754,7 @@ DFC_D void build_disney(const DMaterial& m, Bsdf* B) {
     } else if (!(m.flags & kDisneyScatter)) {
       B->l[B->n++] = make_lobe(kDisneyDiffuse, kRefl | kDiffuse, color * dw);
     } else {
-      B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, V3{1, 1, 1});
+      B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, V3{1, 1, 1}, 1.0f, m.eta);
     }
     B->l[B->n++] = make_lobe(kDisneyRetro, kRefl | kDiffuse, color * dw, m.d_rough);
     if (m.flags & kDisneyHasSheen) B->l[B->n++] = make_lobe(kDisneySheen, kRefl | kDiffuse, ld3(m.c3));
@@ -743,8 +777,10 @@ DFC_D void build_disney(const DMaterial& m, Bsdf* B) {
 }
 
 // Material.computeScatteringFunctions(intersection, RADIANCE, isAllowingMultipleLobes = true)
-// for the resolved kinds (scene/material/{Matte,Mirror,Glass,Metal,Plastic,Disney}Material.java).
-DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, Bsdf* B) {
+// for the resolved kinds (scene/material/*Material.java).  u_material is the
+// random number ClearCoatMaterial draws per hit (ClearCoatMaterial.java:323).
+// Returns false when the material gives no BSDF (the ray passes through).
+DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_material, Bsdf* B) {
   B->n = 0; B->eta = 1.0f;
   B->fr_i = 1.0f; B->fr_t = 1.0f; B->bt_a = 1.0f; B->bt_b = 1.0f; B->metallic = 0.0f;
   B->ca = V3{0, 0, 0}; B->cb = V3{0, 0, 0};
@@ -780,13 +816,59 @@ DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, Bsdf* B) 
       break;
     }
     case kMatDisney: build_disney(m, B); break;
+    case kMatClearCoat: {  // ClearCoatMaterial.java:computeScatteringFunctions
+      const V3 n = sf.s.w;
+      const V3 nco = dot(n, ray_d) > 0.0f ? -n : n;  // Intersection.getSurfaceNormalSCorrectlyOriented
+      const bool entering = dot(n, nco) > 0.0f;
+      const float etaI = entering ? 1.0f : 1.5f, etaT = entering ? 1.5f : 1.0f;
+      V3 refr;
+      if (refract(ray_d, nco, etaI / etaT, &refr)) {  // Vector3F.refraction(direction, normal, eta)
+        const float cosi = dot(ray_d, nco);
+        const float R = fr_dielectric(entering ? -cosi : dot(refr, n), 1.0f, 1.5f), T = 1.0f - R;
+        const float p = 0.25f + 0.5f * R;
+        if (u_material < p) B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1) * (R / p));
+        else B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0) * (T / (1.0f - p)));
+      } else {
+        B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1));
+      }
+      break;
+    }
+    case kMatGlossy: {
+      Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay);
+      L.fresnel = kFresConductor;
+      B->l[B->n++] = L;
+      B->ca = ld3(m.c1); B->cb = ld3(m.c2);
+      break;
+    }
+    case kMatSubstrate:
+      B->l[B->n++] = tr_lobe(kFresnelBlend, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay);
+      B->ca = ld3(m.c1);
+      break;
+    case kMatTranslucent: {
+      if (m.flags & 1) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
+      if (m.flags & 2) B->l[B->n++] = make_lobe(kLambertBTDF, kTrans | kDiffuse, ld3(m.c1));
+      if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c2), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      if (m.flags & 8) B->l[B->n++] = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c3), m.ax, m.ay);
+      B->fr_i = 1.0f; B->fr_t = 1.5f; B->bt_a = 1.0f; B->bt_b = 1.5f;
+      break;
+    }
+    case kMatUber: {
+      if (m.flags & 1) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c4), 1.0f, 1.0f);
+      if (m.flags & 2) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
+      if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      if (m.flags & 8) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c2)); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      if (m.flags & 16) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c3), 1.0f, m.eta);
+      B->fr_i = 1.0f; B->fr_t = m.eta;
+      B->eta = (m.flags & 1) ? 1.0f : m.eta;
+      break;
+    }
     default: return false;
   }
   B->s = sf.s;
   B->ng = sf.g.w;
   B->wo_w = -ray_d;
   B->wo = normalize(to_local(B->wo_w, B->s));
-  return B->n > 0;
+  return B->n > 0 || m.kind == kMatUber;  // UberMaterial gives a BSDF even without lobes: the path ends there
 }
 DFC_D V3 bsdf_f(const Bsdf& B, int flags, V3 wi_w) {
   V3 wi = normalize(to_local(wi_w, B.s));

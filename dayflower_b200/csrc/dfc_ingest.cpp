@@ -25,7 +25,10 @@
 namespace dfc {
 namespace {
 
-enum { kMatDisneyId = 4, kMatGlassId = 7, kMatMatteId = 11, kMatMetalId = 12, kMatMirrorId = 13, kMatPlasticId = 14 };
+enum {
+  kMatClearCoatId = 3, kMatDisneyId = 4, kMatGlassId = 7, kMatGlossyId = 8, kMatMatteId = 11, kMatMetalId = 12, kMatMirrorId = 13,
+  kMatPlasticId = 14, kMatSubstrateId = 16, kMatTranslucentId = 18, kMatUberId = 19
+};
 enum { kTexConstantId = 4, kModNoOpId = 2 };
 enum { kBVAabbId = 1, kBVSphereId = 2, kBVInfiniteId = 3 };
 
@@ -119,6 +122,11 @@ struct Decoder {
       case kMatMetalId: name = "materialMetalMaterialArray"; break;
       case kMatPlasticId: name = "materialPlasticMaterialArray"; break;
       case kMatDisneyId: name = "materialDisneyMaterialArray"; break;
+      case kMatClearCoatId: name = "materialClearCoatMaterialArray"; break;
+      case kMatGlossyId: name = "materialGlossyMaterialArray"; break;
+      case kMatSubstrateId: name = "materialSubstrateMaterialArray"; break;
+      case kMatTranslucentId: name = "materialTranslucentMaterialArray"; break;
+      case kMatUberId: name = "materialUberMaterialArray"; break;
       default: throw Fail{DFC_E_UNSUPPORTED, "material id " + std::to_string(mid) + " is not supported"};
     }
     const auto& A = I(name);
@@ -182,6 +190,74 @@ struct Decoder {
         m.ax = m.ay = remap ? roughness_to_alpha(r) : r;
         m.has_kr = !black(m.c0); m.has_kt = !black(m.c1);
         m.kind = (m.has_kr || m.has_kt) ? kMatPlastic : kMatNone;
+        break;
+      }
+      case kMatClearCoatId: {  // ClearCoatMaterial.java: kd, ks (the lobe is chosen per hit)
+        texref(A, moff, 1, &a, &ao, &b, &bo);
+        color(a, ao, m.c0); color(b, bo, m.c1);
+        m.kind = kMatClearCoat;
+        break;
+      }
+      case kMatGlossyId: {  // GlossyMaterial.java: TorranceSparrowBRDF(kr, ConductorFresnel(kr, 1, 1), TR(r, r))
+        texref(A, moff, 1, &a, &ao, &b, &bo);
+        color(a, ao, m.c0);
+        const float r = value(b, bo);
+        m.ax = m.ay = std::fmax(r, 0.001f);
+        // ConductorFresnel with etaI = kr, etaT = k = 1: relative eta and k are 1 / kr
+        for (int k = 0; k < 3; ++k) { m.c1[k] = 1.0f / m.c0[k]; m.c2[k] = 1.0f / m.c0[k]; }
+        m.kind = kMatGlossy;
+        break;
+      }
+      case kMatSubstrateId: {  // SubstrateMaterial.java: FresnelBlendBRDF(kd, ks, TR(ru, rv))
+        texref(A, moff, 1, &a, &ao, &b, &bo);
+        color(a, ao, m.c0); sat0(m.c0); color(b, bo, m.c1); sat0(m.c1);
+        texref(A, moff, 2, &a, &ao, &b, &bo);
+        const float ru = value(a, ao), rv = value(b, bo);
+        const bool remap = plain(A, moff, 3) != 0;
+        m.ax = std::fmax(remap ? roughness_to_alpha(ru) : ru, 0.001f);
+        m.ay = std::fmax(remap ? roughness_to_alpha(rv) : rv, 0.001f);
+        m.kind = (black(m.c0) && black(m.c1)) ? kMatNone : kMatSubstrate;
+        break;
+      }
+      case kMatTranslucentId: {  // TranslucentMaterial.java; flags: 1 Lambert BRDF, 2 Lambert BTDF, 4 TS BRDF, 8 TS BTDF
+        float kd[3], ks[3], rf[3], tr[3];
+        texref(A, moff, 1, &a, &ao, &b, &bo);
+        color(a, ao, kd); sat0(kd); color(b, bo, ks); sat0(ks);
+        texref(A, moff, 2, &a, &ao, &b, &bo);
+        color(a, ao, rf); sat0(rf); color(b, bo, tr); sat0(tr);
+        texref(A, moff, 3, &a, &ao, &b, &bo);  // roughness, (isRemappingRoughness, 0)
+        const float r = value(a, ao);
+        const float al = std::fmax(b != 0 ? roughness_to_alpha(r) : r, 0.001f);
+        m.flags = 0;
+        if (!black(rf) || !black(tr)) {
+          if (!black(kd)) m.flags |= (black(rf) ? 0 : 1) | (black(tr) ? 0 : 2);
+          if (!black(ks)) m.flags |= (black(rf) ? 0 : 4) | (black(tr) ? 0 : 8);
+        }
+        for (int k = 0; k < 3; ++k) { m.c0[k] = kd[k] * rf[k]; m.c1[k] = kd[k] * tr[k]; m.c2[k] = ks[k] * rf[k]; m.c3[k] = ks[k] * tr[k]; }
+        m.ax = m.ay = al;
+        m.kind = m.flags ? kMatTranslucent : kMatNone;  // no lobe: no BSDF, the ray passes through
+        break;
+      }
+      case kMatUberId: {  // UberMaterial.java; flags: 1 transparency BTDF, 2 Lambert, 4 TS BRDF, 8 specular BRDF, 16 specular BTDF
+        float kd[3], kr[3], ks[3], kt[3], op[3];
+        texref(A, moff, 1, &a, &ao, &b, &bo);
+        color(a, ao, kd); sat0(kd); color(b, bo, kr); sat0(kr);
+        texref(A, moff, 2, &a, &ao, &b, &bo);
+        color(a, ao, ks); sat0(ks); color(b, bo, kt); sat0(kt);
+        texref(A, moff, 3, &a, &ao, &b, &bo);
+        m.eta = value(a, ao);
+        color(b, bo, op); sat0(op);
+        texref(A, moff, 4, &a, &ao, &b, &bo);
+        const float ru = value(a, ao), rv = value(b, bo);
+        const bool remap = plain(A, moff, 5) != 0;
+        m.ax = std::fmax(remap ? roughness_to_alpha(ru) : ru, 0.001f);
+        m.ay = std::fmax(remap ? roughness_to_alpha(rv) : rv, 0.001f);
+        for (int k = 0; k < 3; ++k) {
+          m.c0[k] = op[k] * kd[k]; m.c1[k] = op[k] * ks[k]; m.c2[k] = op[k] * kr[k]; m.c3[k] = op[k] * kt[k];
+          m.c4[k] = std::fmax(1.0f - op[k], 0.0f);
+        }
+        m.flags = (black(m.c4) ? 0 : 1) | (black(m.c0) ? 0 : 2) | (black(m.c1) ? 0 : 4) | (black(m.c2) ? 0 : 8) | (black(m.c3) ? 0 : 16);
+        m.kind = kMatUber;
         break;
       }
       case kMatDisneyId: {  // DisneyMaterial.java:1121-1210; record slots CompiledMaterialCache.java:2751-2759

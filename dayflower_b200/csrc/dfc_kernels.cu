@@ -666,7 +666,7 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
           } else {
             const DMaterial& m = S.materials[pr.material];
             Bsdf B;
-            if (!build_bsdf(m, sf, ray_d, &B)) {
+            if (!build_bsdf(m, sf, ray_d, rng_uniform(key, bounce_dim(dimb, kDimMaterial)), &B)) {
               // Scene.java:494: no BSDF, continue straight through without counting a bounce
               a.ray_o[p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
               a.ray_d[p] = make_float4(ray_d.x, ray_d.y, ray_d.z, kFltMax);
@@ -987,7 +987,7 @@ DFC_D unsigned seg_of(const BatchArgs& a, unsigned long long g) {
 // the unstarted paths of cancelled jobs at the cursor are skipped (counted as
 // done), and the number of paths to start is fixed for regen.
 __global__ void k_batch_plan(BatchArgs a) {
-  if (threadIdx.x < 2 * kSortBins) a.sort_bins[threadIdx.x] = 0u;
+  for (unsigned i = threadIdx.x; i < 2u * kSortBins; i += blockDim.x) a.sort_bins[i] = 0u;
   if (threadIdx.x != 0) return;
   BatchState* st = a.state;
   st->rays += a.counts_next[0];

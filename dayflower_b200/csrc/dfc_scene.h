@@ -44,10 +44,16 @@ enum : int {
   kMatMetal = 6,       // MetalMaterial
   kMatPlastic = 7,     // PlasticMaterial
   kMatDisney = 8,      // DisneyMaterial
-  kMatKinds = 9
+  kMatClearCoat = 9,   // ClearCoatMaterial (picks its lobe with a random number per hit)
+  kMatGlossy = 10,     // GlossyMaterial
+  kMatSubstrate = 11,  // SubstrateMaterial (FresnelBlendBRDF)
+  kMatTranslucent = 12,  // TranslucentMaterial
+  kMatUber = 13,       // UberMaterial
+  kMatKinds = 14
 };
 
-// DisneyMaterial flags (DMaterial.flags)
+// DisneyMaterial flags (DMaterial.flags); TranslucentMaterial and UberMaterial
+// use DMaterial.flags as a bit set of the lobes they build (dfc_ingest.cpp).
 enum : int { kDisneyThin = 1, kDisneyScatter = 2, kDisneyHasSheen = 4, kDisneyHasClearCoat = 8, kDisneyHasTransmission = 16 };
 
 struct alignas(16) DPrim {

@@ -179,6 +179,23 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
         elif isinstance(m, M.Plastic):
             rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness] * 3))) + plain(m.remap_roughness)
             name, length = "materialPlasticMaterialArray", 4
+        elif isinstance(m, M.ClearCoat):  # CompiledMaterialCache.java:2639-2646
+            rec, name, length = head + slot((T, tex(m.kd)), (T, tex(m.ks))), "materialClearCoatMaterialArray", 2
+        elif isinstance(m, M.Glossy):  # :2932-2939
+            rec, name, length = head + slot((T, tex(m.kr)), (T, tex([m.roughness] * 3))), "materialGlossyMaterialArray", 2
+        elif isinstance(m, M.Substrate):  # :3373-3383
+            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + \
+                plain(m.remap_roughness)
+            name, length = "materialSubstrateMaterialArray", 4
+        elif isinstance(m, M.Translucent):  # :3466-3477
+            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex(m.reflectance)), (T, tex(m.transmittance))) + \
+                slot((T, tex([m.roughness] * 3)), (1 if m.remap_roughness else 0, 0))
+            name, length = "materialTranslucentMaterialArray", 4
+        elif isinstance(m, M.Uber):  # :3563-3577
+            rec = head + slot((T, tex(m.kd)), (T, tex(m.kr))) + slot((T, tex(m.ks)), (T, tex(m.kt))) + \
+                slot((T, tex([m.eta] * 3)), (T, tex(m.opacity))) + \
+                slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + plain(m.remap_roughness)
+            name, length = "materialUberMaterialArray", 8
         elif isinstance(m, M.Disney):
             # CompiledMaterialCache.toDisneyMaterial (:2717-2760): nine packed slots of a 16-slot record
             def ft(v):

@@ -206,6 +206,34 @@ def disney_scene(resolution=(96, 72), with_lights=True) -> M.Scene:
     return sc
 
 
+def materials_scene(resolution=(96, 72), with_lights=True) -> M.Scene:
+    """Spheres of ClearCoatMaterial, GlossyMaterial, SubstrateMaterial,
+    TranslucentMaterial (reflection and transmission) and UberMaterial (opaque;
+    partly transparent with specular reflection and transmission) on a matte
+    ground plane, lit by a point light and a spherical area light."""
+    cam = M.Camera(eye=(0.0, 3.0, 10.0), look_at=(0.0, 1.0, 0.0), fov_x_deg=60.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="materials")
+    mats = [
+        M.ClearCoat(kd=(0.6, 0.2, 0.2), ks=(1.0, 1.0, 1.0)),
+        M.Glossy(kr=(0.8, 0.6, 0.3), roughness=0.15),
+        M.Substrate(kd=(0.2, 0.5, 0.7), ks=(0.4, 0.4, 0.4), roughness_u=0.2, roughness_v=0.1),
+        M.Translucent(kd=(0.6, 0.7, 0.3), ks=(0.3, 0.3, 0.3), roughness=0.2),
+        M.Uber(kd=(0.5, 0.3, 0.6), ks=(0.3, 0.3, 0.3)),
+        M.Uber(kd=(0.2, 0.2, 0.2), kr=(0.5, 0.5, 0.5), kt=(0.6, 0.6, 0.6), opacity=(0.6, 0.7, 0.8), eta=1.4),
+        M.Translucent(kd=(0.8, 0.4, 0.2), ks=(0.0, 0.0, 0.0), reflectance=(0.0, 0.0, 0.0), transmittance=(0.9, 0.9, 0.9)),
+    ]
+    for k, m in enumerate(mats):
+        x = -4.5 + 1.5 * k
+        sc.add(M.Primitive(M.Sphere(), m, M.Transform.translate_scale((x, 0.7, 0.0), 0.7)))
+    sc.add(M.Primitive(M.Plane(), M.Matte(kd=(0.5, 0.5, 0.5)), _rot_x(-90.0, (0.0, 0.0, 0.0))))
+    if with_lights:
+        sc.lights.append(M.PointLight((2.0, 6.0, 5.0), (40.0, 40.0, 40.0)))
+        sl = M.DiffuseAreaLight(M.Sphere(), (6.0, 5.0, 4.0), transform=M.Transform.translate_scale((-3.0, 5.0, 3.0), 0.6))
+        sc.lights.append(sl)
+        sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((-3.0, 5.0, 3.0), 0.6), area_light=sl))
+    return sc
+
+
 def _rot_x(deg, position, scale=1.0):
     """Object-to-world: rotate about x by `deg`, scale, then translate."""
     c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))

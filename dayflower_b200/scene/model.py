@@ -20,6 +20,7 @@ SHAPE_CONE, SHAPE_CYLINDER, SHAPE_DISK, SHAPE_HYPERBOLOID = 2, 5, 6, 7
 SHAPE_PARABOLOID, SHAPE_PLANE, SHAPE_POLYGON, SHAPE_RECTANGLE = 9, 10, 11, 13
 SHAPE_CUBOID, SHAPE_SPHERE, SHAPE_TORUS, SHAPE_TRIANGLE, SHAPE_MESH = 14, 15, 16, 17, 18
 MAT_DISNEY, MAT_GLASS, MAT_MATTE, MAT_METAL, MAT_MIRROR, MAT_PLASTIC = 4, 7, 11, 12, 13, 14
+MAT_CLEAR_COAT, MAT_GLOSSY, MAT_SUBSTRATE, MAT_TRANSLUCENT, MAT_UBER = 3, 8, 16, 18, 19
 TEX_CONSTANT = 4
 MOD_NOOP = 2
 LIGHT_DIFFUSE_AREA, LIGHT_DIRECTIONAL, LIGHT_IMAGE, LIGHT_PEREZ = 1, 2, 3, 4
@@ -373,6 +374,60 @@ class Disney(Material):
     specular_transmission: float = 0.0
     thin: bool = False
     ID = MAT_DISNEY
+
+
+@dataclass(eq=False)
+class ClearCoat(Material):
+    """``scene/material/ClearCoatMaterial`` (defaults ClearCoatMaterial.java:86-146)."""
+    kd: Sequence[float] = (0.5, 0.5, 0.5)
+    ks: Sequence[float] = (1.0, 1.0, 1.0)
+    ID = MAT_CLEAR_COAT
+
+
+@dataclass(eq=False)
+class Glossy(Material):
+    """``scene/material/GlossyMaterial`` (defaults GlossyMaterial.java:81-141)."""
+    kr: Sequence[float] = (0.5, 0.5, 0.5)
+    roughness: float = 0.2
+    ID = MAT_GLOSSY
+
+
+@dataclass(eq=False)
+class Substrate(Material):
+    """``scene/material/SubstrateMaterial`` (defaults SubstrateMaterial.java:86-215)."""
+    kd: Sequence[float] = (0.5, 0.5, 0.5)
+    ks: Sequence[float] = (0.5, 0.5, 0.5)
+    roughness_u: float = 0.1
+    roughness_v: float = 0.1
+    remap_roughness: bool = True
+    ID = MAT_SUBSTRATE
+
+
+@dataclass(eq=False)
+class Translucent(Material):
+    """``scene/material/TranslucentMaterial`` (defaults TranslucentMaterial.java:94-274)."""
+    kd: Sequence[float] = (0.25, 0.25, 0.25)
+    ks: Sequence[float] = (0.25, 0.25, 0.25)
+    roughness: float = 0.1
+    reflectance: Sequence[float] = (0.5, 0.5, 0.5)
+    transmittance: Sequence[float] = (0.5, 0.5, 0.5)
+    remap_roughness: bool = True
+    ID = MAT_TRANSLUCENT
+
+
+@dataclass(eq=False)
+class Uber(Material):
+    """``scene/material/UberMaterial`` (defaults UberMaterial.java:97-332)."""
+    kd: Sequence[float] = (0.25, 0.25, 0.25)
+    kr: Sequence[float] = (0.0, 0.0, 0.0)
+    ks: Sequence[float] = (0.25, 0.25, 0.25)
+    kt: Sequence[float] = (0.0, 0.0, 0.0)
+    opacity: Sequence[float] = (1.0, 1.0, 1.0)
+    eta: float = 1.5
+    roughness_u: float = 0.1
+    roughness_v: float = 0.1
+    remap_roughness: bool = True
+    ID = MAT_UBER
 
 
 # ---------------------------------------------------------------- lights ----

@@ -36,7 +36,10 @@ enum { kBVAabb = 1, kBVSphere = 2, kBVInfinite = 3 };
 enum { kShapeCone = 2, kShapeCylinder = 5, kShapeDisk = 6, kShapeHyperboloid = 7, kShapeParaboloid = 9, kShapePlane = 10,
        kShapePolygon = 11, kShapeRectangle = 13, kShapeCuboid = 14, kShapeSphere = 15, kShapeTorus = 16, kShapeTriangle = 17,
        kShapeMesh = 18 };
-enum { kMatDisney = 4, kMatGlass = 7, kMatMatte = 11, kMatMetal = 12, kMatMirror = 13, kMatPlastic = 14 };
+enum {
+  kMatClearCoat = 3, kMatDisney = 4, kMatGlass = 7, kMatGlossy = 8, kMatMatte = 11, kMatMetal = 12, kMatMirror = 13, kMatPlastic = 14,
+  kMatSubstrate = 16, kMatTranslucent = 18, kMatUber = 19
+};
 enum { kTexConstant = 4 };
 enum { kLightDiffuseArea = 1, kLightDirectional = 2, kLightImage = 3, kLightPerez = 4, kLightPoint = 5, kLightSpot = 7 };
 enum { kAlgoAO = 0, kAlgoDepth = 1, kAlgoPath = 2, kAlgoRayCast = 3, kAlgoRayTrace = 4 };
@@ -811,6 +814,7 @@ enum { kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossy = 8, kSpecular = 16, kAll = 
 enum LobeKind {
   kLambert, kOrenNayar, kSpecBRDF, kFresnelSpec, kSpecBTDF, kTSBRDF, kTSBTDF,
   kLambertBTDF,                                                                    // scene/bxdf/LambertianBTDF.java
+  kFresnelBlend,                                                                   // scene/bxdf/FresnelBlendBRDF.java
   kDisneyDiffuse, kDisneyFakeSS, kDisneyRetro, kDisneySheen, kDisneyClearCoat      // scene/bxdf/Disney*BRDF.java
 };
 enum FresKind { kFresConst, kFresDielectric, kFresConductor, kFresDisney };
@@ -1024,6 +1028,23 @@ inline V3 lobe_f(const Lobe& L, V3 wo, V3 wi) {
       return L.scale * (1.0f - F) * k;
     }
     case kLambertBTDF: return L.scale * (1.0f / kPi);
+    case kFresnelBlend: {  // FresnelBlendBRDF.java:evaluateDistributionFunction (scale: diffuse, cK: specular)
+      V3 h = wo + wi;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
+      h = normalize(h);
+      auto pow5 = [](float x) { return x * x * x * x * x; };
+      const float a = 28.0f / (23.0f * kPi);
+      const float b = 1.0f - pow5(1.0f - 0.5f * std::fabs(cos_t(wi)));
+      const float c = 1.0f - pow5(1.0f - 0.5f * std::fabs(cos_t(wo)));
+      const float d = tr_D(L, h);
+      const float e = 4.0f * std::fabs(dot(wi, h)) * std::fmax(std::fabs(cos_t(wi)), std::fabs(cos_t(wo)));
+      const float f = d / e;
+      const float w = pow5(1.0f - dot(wi, h));
+      const V3 ks = L.cK;
+      const V3 fr = {ks.x + (1.0f - ks.x) * w, ks.y + (1.0f - ks.y) * w, ks.z + (1.0f - ks.z) * w};  // Schlick.fresnelDielectric
+      const V3 diff = mul(L.scale * a, V3{1.0f - ks.x, 1.0f - ks.y, 1.0f - ks.z}) * b * c;
+      return diff + fr * f;
+    }
     case kDisneyDiffuse: {  // DisneyDiffuseBRDF.java:evaluateDistributionFunction
       const float fo = schlick_weight(std::fabs(cos_t(wo))), fi = schlick_weight(std::fabs(cos_t(wi)));
       const float a = 1.0f - fo / 2.0f, b = 1.0f - fi / 2.0f;
@@ -1065,6 +1086,11 @@ inline float lobe_pdf(const Lobe& L, V3 wo, V3 wi) {
     case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
       return same_hemi(wo, wi) ? std::fabs(cos_t(wi)) * (1.0f / kPi) : 0.0f;
     case kLambertBTDF: return same_hemi(wo, wi) ? 0.0f : std::fabs(cos_t(wi)) * (1.0f / kPi);
+    case kFresnelBlend: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      const V3 h = normalize(wo + wi);
+      return 0.5f * (std::fabs(cos_t(wi)) * (1.0f / kPi) + tr_pdf(L, wo, h) / (4.0f * dot(wo, h)));
+    }
     case kDisneyClearCoat: {
       if (!same_hemi(wo, wi)) return 0.0f;
       V3 h = wi + wo;
@@ -1103,6 +1129,18 @@ inline bool lobe_sample(const Lobe& L, V3 wo, float u, float v, LobeSample* s) {
     case kLambertBTDF: {
       V3 wi = cosine_hemisphere(u, v);
       if (wo.z > 0.0f) wi.z = -wi.z;  // faceForwardZNegated
+      s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
+    }
+    case kFresnelBlend: {  // FresnelBlendBRDF.java:sampleDistributionFunction
+      V3 wi;
+      if (u < 0.5f) {
+        wi = cosine_hemisphere(std::fmin(2.0f * u, 0.99999994f), v);
+        if (wo.z < 0.0f) wi.z = -wi.z;
+      } else {
+        const V3 h = tr_sample_h(L, wo, std::fmin(2.0f * (u - 0.5f), 0.99999994f), v);
+        wi = reflect_about(wo, h);
+        if (!same_hemi(wo, wi)) return false;
+      }
       s->wi = wi; s->f = lobe_f(L, wo, wi); s->pdf = lobe_pdf(L, wo, wi); return true;
     }
     case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
@@ -1180,7 +1218,9 @@ inline Lobe make_tr_lobe(LobeKind k, int type, V3 scale, float ax, float ay) {
 // Material.computeScatteringFunctions for Matte/Mirror/Glass/Metal/Plastic
 // (scene/material/*Material.java) decoded from the compiled records
 // (scene/compiler/CompiledMaterialCache.java:2830-3294).
-inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool multi, Bsdf* B, bool* supported) {
+// u_material: the random number a material draws when it builds its BSDF
+// (ClearCoatMaterial.java:323, Floats.random()).
+inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool multi, float u_material, Bsdf* B, bool* supported) {
   *supported = true;
   B->n = 0; B->eta = 1.0f; B->present = false;
   TexRef a, b;
@@ -1326,6 +1366,104 @@ inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool mu
       if (thin) { Lobe L{}; L.kind = kLambertBTDF; L.type = kTrans | kDiffuse; L.scale = color * dt; add(L); }
       break;
     }
+    case kMatClearCoat: {  // scene/material/ClearCoatMaterial.java:computeScatteringFunctions
+      const auto& M = sc.I("materialClearCoatMaterialArray");
+      material_slot(sc, M, moff, 1, &a, &b);
+      const V3 kd = tex_color(sc, a), ks = tex_color(sc, b);
+      const V3 d = h.w.ray.d, n = h.w.s.w;
+      const V3 nco = dot(n, d) > 0.0f ? -n : n;  // Intersection.getSurfaceNormalSCorrectlyOriented
+      const bool entering = dot(n, nco) > 0.0f;
+      const float etaI = entering ? 1.0f : 1.5f, etaT = entering ? 1.5f : 1.0f;
+      V3 refr;
+      Lobe L{};
+      if (refract(d, nco, etaI / etaT, &refr)) {  // Vector3F.refraction(direction, normal, eta)
+        const float cosi = dot(d, nco);
+        const float cosc = entering ? -cosi : dot(refr, n);
+        const float R = fresnel_dielectric(cosc, 1.0f, 1.5f), T = 1.0f - R;
+        const float p = 0.25f + 0.5f * R;
+        if (u_material < p) { L.kind = kSpecBRDF; L.type = kRefl | kSpecular; L.scale = ks * (R / p); L.fk = kFresConst; }
+        else { L.kind = kLambert; L.type = kRefl | kDiffuse; L.scale = kd * (T / (1.0f - p)); }
+      } else {
+        L.kind = kSpecBRDF; L.type = kRefl | kSpecular; L.scale = ks; L.fk = kFresConst;
+      }
+      B->l[B->n++] = L;
+      break;
+    }
+    case kMatGlossy: {  // scene/material/GlossyMaterial.java: TorranceSparrowBRDF(kr, ConductorFresnel(kr, 1, 1), TR(r, r))
+      const auto& M = sc.I("materialGlossyMaterialArray");
+      material_slot(sc, M, moff, 1, &a, &b);
+      const V3 kr = tex_color(sc, a);
+      const float r = tex_float(sc, b);
+      Lobe L = make_tr_lobe(kTSBRDF, kRefl | kGlossy, kr, r, r);
+      L.fk = kFresConductor; L.cEtaI = kr; L.cEtaT = {1, 1, 1}; L.cK = {1, 1, 1};
+      B->l[B->n++] = L;
+      break;
+    }
+    case kMatSubstrate: {  // scene/material/SubstrateMaterial.java
+      const auto& M = sc.I("materialSubstrateMaterialArray");
+      TexRef tkd, tks, tru, trv;
+      material_slot(sc, M, moff, 1, &tkd, &tks);
+      material_slot(sc, M, moff, 2, &tru, &trv);
+      const bool remap = material_int(sc, M, moff, 3) != 0;
+      const V3 kd = sat0(tex_color(sc, tkd)), ks = sat0(tex_color(sc, tks));
+      if (black(kd) && black(ks)) return false;
+      const float ru = tex_float(sc, tru), rv = tex_float(sc, trv);
+      Lobe L = make_tr_lobe(kFresnelBlend, kRefl | kGlossy, kd, remap ? roughness_to_alpha(ru) : ru, remap ? roughness_to_alpha(rv) : rv);
+      L.cK = ks;
+      B->l[B->n++] = L;
+      break;
+    }
+    case kMatTranslucent: {  // scene/material/TranslucentMaterial.java
+      const auto& M = sc.I("materialTranslucentMaterialArray");
+      TexRef tkd, tks, trf, ttr, trg, tz;
+      material_slot(sc, M, moff, 1, &tkd, &tks);
+      material_slot(sc, M, moff, 2, &trf, &ttr);
+      material_slot(sc, M, moff, 3, &trg, &tz);  // second pair: (isRemappingRoughness, 0)
+      const V3 refl = sat0(tex_color(sc, trf)), tr = sat0(tex_color(sc, ttr));
+      if (black(refl) && black(tr)) return false;
+      const V3 kd = sat0(tex_color(sc, tkd)), ks = sat0(tex_color(sc, tks));
+      if (!black(kd)) {
+        if (!black(refl)) { Lobe L{}; L.kind = kLambert; L.type = kRefl | kDiffuse; L.scale = mul(kd, refl); B->l[B->n++] = L; }
+        if (!black(tr)) { Lobe L{}; L.kind = kLambertBTDF; L.type = kTrans | kDiffuse; L.scale = mul(kd, tr); B->l[B->n++] = L; }
+      }
+      if (!black(ks)) {
+        const float r = tex_float(sc, trg);
+        const float al = tz.id != 0 ? roughness_to_alpha(r) : r;
+        if (!black(refl)) {
+          Lobe L = make_tr_lobe(kTSBRDF, kRefl | kGlossy, mul(ks, refl), al, al);
+          L.fk = kFresDielectric; L.etaI = 1.0f; L.etaT = 1.5f; B->l[B->n++] = L;
+        }
+        if (!black(tr)) {
+          Lobe L = make_tr_lobe(kTSBTDF, kTrans | kGlossy, mul(ks, tr), al, al);
+          L.etaA = 1.0f; L.etaB = 1.5f; B->l[B->n++] = L;
+        }
+      }
+      if (B->n == 0) return false;
+      break;
+    }
+    case kMatUber: {  // scene/material/UberMaterial.java
+      const auto& M = sc.I("materialUberMaterialArray");
+      TexRef tkd, tkr, tks, tkt, teta, top, tru, trv;
+      material_slot(sc, M, moff, 1, &tkd, &tkr);
+      material_slot(sc, M, moff, 2, &tks, &tkt);
+      material_slot(sc, M, moff, 3, &teta, &top);
+      material_slot(sc, M, moff, 4, &tru, &trv);
+      const bool remap = material_int(sc, M, moff, 5) != 0;
+      const V3 op = sat0(tex_color(sc, top));
+      const V3 kd = mul(op, sat0(tex_color(sc, tkd))), kr = mul(op, sat0(tex_color(sc, tkr)));
+      const V3 ks = mul(op, sat0(tex_color(sc, tks))), kt = mul(op, sat0(tex_color(sc, tkt)));
+      const V3 ts = sat0(V3{1.0f - op.x, 1.0f - op.y, 1.0f - op.z});
+      const float eta = tex_float(sc, teta);
+      const float ru = tex_float(sc, tru), rv = tex_float(sc, trv);
+      const float au = remap ? roughness_to_alpha(ru) : ru, av = remap ? roughness_to_alpha(rv) : rv;
+      if (!black(ts)) { Lobe L{}; L.kind = kSpecBTDF; L.type = kTrans | kSpecular; L.scale = ts; L.etaA = 1.0f; L.etaB = 1.0f; B->l[B->n++] = L; }
+      if (!black(kd)) { Lobe L{}; L.kind = kLambert; L.type = kRefl | kDiffuse; L.scale = kd; B->l[B->n++] = L; }
+      if (!black(ks)) { Lobe L = make_tr_lobe(kTSBRDF, kRefl | kGlossy, ks, au, av); L.fk = kFresDielectric; L.etaI = 1.0f; L.etaT = eta; B->l[B->n++] = L; }
+      if (!black(kr)) { Lobe L{}; L.kind = kSpecBRDF; L.type = kRefl | kSpecular; L.scale = kr; L.fk = kFresDielectric; L.etaI = 1.0f; L.etaT = eta; B->l[B->n++] = L; }
+      if (!black(kt)) { Lobe L{}; L.kind = kSpecBTDF; L.type = kTrans | kSpecular; L.scale = kt; L.etaA = 1.0f; L.etaB = eta; B->l[B->n++] = L; }
+      B->eta = black(ts) ? eta : 1.0f;  // BSDF(intersection, bXDFs, false, eta)
+      break;  // a BSDF even with no lobes: the path ends there instead of passing through
+    }
     default: *supported = false; return false;
   }
   B->present = true;
@@ -1346,6 +1484,11 @@ inline V3 material_emission(const Scene& sc, int mid, int moff) {
     case kMatMetal: name = "materialMetalMaterialArray"; break;
     case kMatPlastic: name = "materialPlasticMaterialArray"; break;
     case kMatDisney: name = "materialDisneyMaterialArray"; break;
+    case kMatClearCoat: name = "materialClearCoatMaterialArray"; break;
+    case kMatGlossy: name = "materialGlossyMaterialArray"; break;
+    case kMatSubstrate: name = "materialSubstrateMaterialArray"; break;
+    case kMatTranslucent: name = "materialTranslucentMaterialArray"; break;
+    case kMatUber: name = "materialUberMaterialArray"; break;
     default: return {0, 0, 0};
   }
   TexRef a, b;
@@ -1822,7 +1965,7 @@ inline V3 radiance_path(const Scene& sc, Ray ray, const Params& P, uint32_t key,
       if (bounce >= P.max_bounce) break;
       const int32_t* pr = sc.prims.data() + h.prim * 8;
       Bsdf B; bool sup;
-      if (!build_bsdf(sc, pr[4], pr[5], h, true, &B, &sup)) {
+      if (!build_bsdf(sc, pr[4], pr[5], h, true, rng_uniform(key, bounce_dim(dimb, kDimMaterial)), &B, &sup)) {
         if (!sup) *unsupported = true;
         ray = make_ray(h.w.p, ray.d);
         --bounce;

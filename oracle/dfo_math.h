@@ -117,7 +117,7 @@ enum : uint32_t {
   kDimPixelX = 0, kDimPixelY = 1, kDimLensU = 2, kDimLensV = 3,
   kDimBounceBase = 8, kDimBounceStride = 16,
   kDimLightPick = 0, kDimLightSampleU = 1, kDimLightSampleV = 2, kDimMisSampleU = 3, kDimMisSampleV = 4,
-  kDimSunPick = 5, kDimBsdfU = 6, kDimBsdfV = 7, kDimRoulette = 8,
+  kDimSunPick = 5, kDimBsdfU = 6, kDimBsdfV = 7, kDimRoulette = 8, kDimMaterial = 9,
 };
 inline uint32_t bounce_dim(int bounce, uint32_t which) { return kDimBounceBase + (uint32_t)bounce * kDimBounceStride + which; }
 

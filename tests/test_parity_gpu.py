@@ -32,11 +32,16 @@ def disney():
 
 
 @pytest.fixture(scope="module")
+def materials():
+    return compile_scene(G.materials_scene(resolution=(128, 72)), layout_version=2)
+
+
+@pytest.fixture(scope="module")
 def terrain():
     return compile_scene(G.terrain_spheres(cells=128, n_spheres=300, resolution=(160, 90), seed=11), layout_version=2)
 
 
-@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney"])
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney", "materials"])
 def test_ray_casting_hit_ids(scene_name, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.RAY_CASTING)
@@ -60,7 +65,7 @@ def test_depth_camera(scene_name, request):
     assert np.mean(np.all(np.abs(mg - mo) <= 1e-4 + 1e-4 * np.abs(mo), axis=-1)) >= 0.999
 
 
-@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16)])
+@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16), ("materials", 16)])
 def test_path_tracing_sigma(scene_name, spp, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.PATH_TRACING, spp=spp, max_bounce=8)
