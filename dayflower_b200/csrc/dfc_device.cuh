@@ -987,6 +987,36 @@ DFC_D V3 perez_sky(const float* q, V3 dir) {
 }
 DFC_D V3 sat0(V3 c) { return {fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f)}; }
 
+// scene/light/ImageLight.java:544 doRadianceSky over the compiled record
+// (CompiledLightCache.java:1393-1460: angle +32, scale +33, resolution +36,
+// distribution +40, RGB image +2352): spherical texture coordinates, rotated
+// counterclockwise, scaled, mapped to pixels (Point2F.toImage) and read with
+// bilinear interpolation and wrap-around (ImageF.getColorRGB).
+DFC_D V3 image_sky(const float* q, V3 d) {
+  float phi = atan2f(d.y, d.x);
+  if (phi < 0.0f) phi += 2.0f * kPi;
+  const float theta = acosf(clampf(d.z, -1.0f, 1.0f));
+  const float u = phi * (1.0f / (2.0f * kPi)), v = theta * (1.0f / kPi);
+  float s, c;
+  sincosf(q[32], &s, &c);
+  const float us = (u * c - v * s) * q[33], vs = (v * c + u * s) * q[34];
+  const float rx = q[36], ry = q[37];
+  auto posmod = [](float x, float y) { return x < 0.0f ? fmodf(fmodf(x, y) + y, y) : fmodf(x, y); };
+  const float x = posmod(us * rx - 0.5f, rx), y = posmod(vs * ry - 0.5f, ry);
+  const int w = (int)rx, h = (int)ry;
+  const int x0 = (int)floorf(x), x1 = (int)ceilf(x), y0 = (int)floorf(y), y1 = (int)ceilf(y);
+  auto px = [&](int ix, int iy) {
+    ix = ((ix % w) + w) % w;
+    iy = ((iy % h) + h) % h;
+    const float* p = q + 2352 + ((size_t)iy * (size_t)w + (size_t)ix) * 3;
+    return V3{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+  };
+  if (x0 == x1 && y0 == y1) return px(x0, y0);
+  const float xf = x - (float)x0, yf = y - (float)y0;
+  auto lerp3 = [](V3 a, V3 b, float t) { return V3{lerpf(a.x, b.x, t), lerpf(a.y, b.y, t), lerpf(a.z, b.z, t)}; };
+  return lerp3(lerp3(px(x0, y0), px(x1, y0), xf), lerp3(px(x0, y1), px(x1, y1), xf), yf);
+}
+
 struct LightS { V3 L, p, wi; float pdf; };
 
 // Light.sampleRadianceIncoming for each supported light type.
@@ -1093,21 +1123,39 @@ DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf,
       *o = LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
       return true;
     }
+    case kLightImage: {  // scene/light/ImageLight.java:207 sampleRadianceIncoming
+      const float* q = S.perez + lt.perez;
+      float ru, rv;
+      d2_remap(q + 40, u, v, &ru, &rv);
+      const float pr = d2_pdf(q + 40, ru, rv);
+      if (pr == 0.0f) return false;
+      float sth, cth, sph, cph;
+      sincosf(rv * kPi, &sth, &cth);
+      sincosf(ru * 2.0f * kPi, &sph, &cph);
+      const V3 dobj = {sth * cph, sth * sph, cth};
+      const V3 dw = normalize(xf_vec(q, dobj));
+      const float st = sint(dobj);
+      if (st == 0.0f) return false;
+      *o = LightS{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
+      return true;
+    }
   }
   return false;
 }
 
 DFC_D bool light_is_delta(int type) { return type == kLightPoint || type == kLightSpot || type == kLightDirectional; }
 
-// Light.evaluateRadianceEmitted(Ray3F): only the sky emits along a missed ray.
+// Light.evaluateRadianceEmitted(Ray3F): only the sky lights (Perez, image) emit along a missed ray.
 DFC_D V3 light_Le_miss(const SceneView& S, const DLight& lt, V3 d) {
-  if (lt.type != kLightPerez) return {0, 0, 0};
+  if (lt.type != kLightPerez && lt.type != kLightImage) return {0, 0, 0};
   const float* q = S.perez + lt.perez;
-  return sat0(perez_sky(q, normalize(xf_vec(q + 16, d))));
+  const V3 dobj = normalize(xf_vec(q + 16, d));
+  return lt.type == kLightPerez ? sat0(perez_sky(q, dobj)) : image_sky(q, dobj);
 }
 
-// Perez part of Light.evaluateProbabilityDensityFunctionRadianceIncoming.
-DFC_D float perez_pdf(const SceneView& S, const DLight& lt, V3 wi) {
+// Light.evaluateProbabilityDensityFunctionRadianceIncoming of the sky lights
+// (PerezLight, ImageLight.java:348); their distribution starts at +48 and +40.
+DFC_D float sky_pdf(const SceneView& S, const DLight& lt, V3 wi) {
   const float* q = S.perez + lt.perez;
   V3 d = normalize(xf_vec(q + 16, wi));
   float th = acosf(clampf(d.z, -1.0f, 1.0f));
@@ -1115,7 +1163,7 @@ DFC_D float perez_pdf(const SceneView& S, const DLight& lt, V3 wi) {
   if (st == 0.0f) return 0.0f;
   float phi = atan2f(d.y, d.x);
   if (phi < 0.0f) phi += 2.0f * kPi;
-  return d2_pdf(q + 48, phi * (1.0f / (2.0f * kPi)), th * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
+  return d2_pdf(q + (lt.type == kLightPerez ? 48 : 40), phi * (1.0f / (2.0f * kPi)), th * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
 }
 
 }  // namespace dfc

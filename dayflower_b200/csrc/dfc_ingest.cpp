@@ -404,6 +404,21 @@ struct Decoder {
           std::memcpy(lt.radiance, A.data() + off + 32, 12);
           break;
         }
+        case kLightImage: {  // CompiledLightCache.java:1393-1460; kept after the Perez records in the sky pool
+          const auto& O = I("lightImageLightOffsetArray");
+          const auto& A = F("lightImageLightArray");
+          if (rel < 0 || (size_t)rel >= O.size()) throw Fail{DFC_E_INVALID_ARG, "image light offset out of range"};
+          const int off = O[rel];
+          if (off < 0 || (size_t)off + 2352 > A.size()) throw Fail{DFC_E_INVALID_ARG, "image light record out of range"};
+          const float rx = A[off + 36], ry = A[off + 37];
+          if (!(rx >= 1.0f && ry >= 1.0f) || rx != std::floor(rx) || ry != std::floor(ry) ||
+              (size_t)off + 2352 + (size_t)rx * (size_t)ry * 3 > A.size())
+            throw Fail{DFC_E_INVALID_ARG, "image light resolution out of range"};
+          validate_distribution2(A, (size_t)off + 40);
+          lt.perez = (int)F("lightPerezLightArray").size() + off;
+          lt.radius = A[off + 35];
+          break;
+        }
         default:
           throw Fail{DFC_E_UNSUPPORTED, "light id " + std::to_string(id) + " is not supported"};
       }
@@ -522,7 +537,11 @@ struct Decoder {
       hs.shapes.insert(hs.shapes.end(), A.begin(), A.end());
     }
     if (hs.shapes.empty()) hs.shapes.assign(4, 0.0f);
-    hs.perez = F("lightPerezLightArray");
+    hs.perez = F("lightPerezLightArray");  // the sky pool: Perez records, then image light records
+    {
+      const auto& img = F("lightImageLightArray");
+      hs.perez.insert(hs.perez.end(), img.begin(), img.end());
+    }
     if (hs.rects.empty()) hs.rects.assign(16, 0.0f);
     if (hs.perez.empty()) hs.perez.assign(64, 0.0f);
     lights();

@@ -710,7 +710,7 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
                       float w = 1.0f;
                       bool ok = true;
                       if (!is_spec(bs.type)) {
-                        float lp = lt.type == kLightDiffuseArea ? area_light_pdf(S, lt, sf.p, bs.wi) : (lt.type == kLightPerez ? perez_pdf(S, lt, bs.wi) : 0.0f);
+                        float lp = lt.type == kLightDiffuseArea ? area_light_pdf(S, lt, sf.p, bs.wi) : ((lt.type == kLightPerez || lt.type == kLightImage) ? sky_pdf(S, lt, bs.wi) : 0.0f);
                         if (lp == 0.0f) ok = false;
                         else w = (bs.pdf * bs.pdf) / (bs.pdf * bs.pdf + lp * lp);
                       }

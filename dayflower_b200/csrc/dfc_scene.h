@@ -108,7 +108,7 @@ struct alignas(16) DLight {
   float o2w[12];
   float w2o[12];
   float cos_cone_delta;
-  int perez;          // float offset of the Perez record in the Perez pool
+  int perez;          // PerezLight / ImageLight: float offset of its record in the sky pool (SceneView.perez)
   float pad[2];
 };
 
@@ -137,7 +137,7 @@ struct SceneView {
   const float* tri_attr;        // shape3FTriangle3FArray, 24 floats per triangle, original order
   const float* rects;           // shape3FRectangle3FArray
   const float* shapes;          // disk, cylinder, cone, paraboloid, hyperboloid, cuboid and torus records
-  const float* perez;           // lightPerezLightArray
+  const float* perez;           // sky pool: lightPerezLightArray, then lightImageLightArray
   const float* camera;          // 19 floats
 };
 

@@ -27,7 +27,7 @@ from typing import Dict, List
 import numpy as np
 
 from . import model as M
-from .perez import perez_record
+from .perez import image_light_record, perez_record
 
 ARRAY_NAMES_F32 = [
     "boundingVolume3FAxisAlignedBoundingBox3FArray", "boundingVolume3FBoundingSphere3FArray",
@@ -241,7 +241,7 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
 
     # ---- lights (scene order)
     light_refs: Dict[int, tuple] = {}
-    rel_count = {M.LIGHT_DIFFUSE_AREA: 0, M.LIGHT_DIRECTIONAL: 0, M.LIGHT_POINT: 0, M.LIGHT_SPOT: 0, M.LIGHT_PEREZ: 0}
+    rel_count = {M.LIGHT_DIFFUSE_AREA: 0, M.LIGHT_DIRECTIONAL: 0, M.LIGHT_POINT: 0, M.LIGHT_SPOT: 0, M.LIGHT_PEREZ: 0, M.LIGHT_IMAGE: 0}
     light_ids = []
     for L in scene.lights:
         if isinstance(L, M.DiffuseAreaLight):
@@ -272,6 +272,9 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
         elif isinstance(L, M.PerezLight):
             off = push("lightPerezLightArray", perez_record(L.turbidity, L.sun_direction_world))
             push("lightPerezLightOffsetArray", [off])
+        elif isinstance(L, M.ImageLight):
+            off = push("lightImageLightArray", image_light_record(L.image, L.angle_deg, L.scale))
+            push("lightImageLightOffsetArray", [off])
         else:
             raise ValueError("unsupported light %r" % type(L).__name__)
         rel = rel_count[L.ID]

@@ -234,6 +234,54 @@ def materials_scene(resolution=(96, 72), with_lights=True) -> M.Scene:
     return sc
 
 
+def environment_image(width=4096, height=2048, seed=5, sun_direction_world=(0.4, 0.6, -0.7), sun_radiance=5.0e4,
+                      sun_diameter_deg=0.5) -> np.ndarray:
+    """A seeded HDR environment for ImageLight, (height, width, 3) float32 in
+    the light's spherical texture layout (row y is theta = pi (y + 0.5) /
+    height, column x is phi = 2 pi (x + 0.5) / width, object space): a
+    low-frequency value-noise sky (blue-ish, brighter towards the zenith) and a
+    sun disk of the given angular diameter and radiance.  Pixels whose centre
+    lies inside the disk are set to the sun radiance; the nearest pixel always
+    is, so the sun survives at low resolutions."""
+    from .perez import SKY_WORLD_TO_OBJECT
+    rng = np.random.default_rng(seed)
+    xs = (np.arange(width) + 0.5) / width
+    ys = (np.arange(height) + 0.5) / height
+    noise = _value_noise(xs, ys, 3, rng)  # (height, width), about [-1, 1]
+    theta = np.pi * ys[:, None]
+    phi = 2.0 * np.pi * xs[None, :]
+    up = np.cos(theta) * np.ones_like(phi)  # object z; the sky transform maps object z to world y
+    base = np.stack([0.35 + 0.15 * noise, 0.45 + 0.15 * noise, 0.75 + 0.2 * noise], axis=-1)
+    img = base * (0.6 + 0.4 * np.clip(up, 0.0, 1.0))[..., None]
+    img = np.maximum(img, 0.02)
+    sw = np.asarray(sun_direction_world, dtype=np.float64)
+    so = SKY_WORLD_TO_OBJECT[:3, :3].astype(np.float64) @ (sw / np.linalg.norm(sw))
+    so /= np.linalg.norm(so)
+    d = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi)], axis=-1)
+    cosang = d @ so
+    disk = cosang >= math.cos(math.radians(sun_diameter_deg / 2.0))
+    sp = math.atan2(so[1], so[0]) % (2.0 * math.pi)
+    st = math.acos(max(-1.0, min(1.0, so[2])))
+    disk[min(int(st / np.pi * height), height - 1), min(int(sp / (2.0 * np.pi) * width), width - 1)] = True
+    img[disk] = sun_radiance
+    return img.astype(np.float32)
+
+
+def image_light_scene(resolution=(96, 72), env=(256, 128), seed=9) -> M.Scene:
+    """Spheres (matte, metal, glass, Disney) on a matte ground under an ImageLight
+    of a seeded environment with a small sun."""
+    cam = M.Camera(eye=(0.0, 2.5, 8.0), look_at=(0.0, 0.8, 0.0), fov_x_deg=60.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="image_light")
+    mats = [M.Matte(kd=(0.7, 0.6, 0.5)), M.Metal(roughness_u=0.2, roughness_v=0.2), M.Glass(eta=1.5),
+            M.Disney(color=(0.3, 0.6, 0.8), roughness=0.4, clear_coat=0.5)]
+    for k, m in enumerate(mats):
+        sc.add(M.Primitive(M.Sphere(), m, M.Transform.translate_scale((-3.0 + 2.0 * k, 0.8, 0.0), 0.8)))
+    sc.add(M.Primitive(M.Plane(), M.Matte(kd=(0.5, 0.5, 0.5)), _rot_x(-90.0, (0.0, 0.0, 0.0))))
+    img = environment_image(env[0], env[1], seed=seed, sun_radiance=200.0, sun_diameter_deg=4.0)
+    sc.lights.append(M.ImageLight(img, angle_deg=30.0))
+    return sc
+
+
 def _rot_x(deg, position, scale=1.0):
     """Object-to-world: rotate about x by `deg`, scale, then translate."""
     c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))

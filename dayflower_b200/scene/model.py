@@ -487,6 +487,21 @@ class PerezLight(Light):
         self.sun_direction_world = normalize(sun_direction_world)
 
 
+class ImageLight(Light):
+    """``scene/light/ImageLight``: an environment image (float RGB, rows from
+    theta = 0 at the top), rotated by ``angle_deg`` and scaled by ``scale`` in
+    spherical texture space (ImageLight.java:134-146)."""
+    ID = LIGHT_IMAGE
+
+    def __init__(self, image, angle_deg=0.0, scale=(1.0, 1.0)):
+        img = np.ascontiguousarray(image, dtype=np.float32)
+        if img.ndim != 3 or img.shape[2] != 3:
+            raise ValueError("image must be (height, width, 3)")
+        self.image = img
+        self.angle_deg = float(angle_deg)
+        self.scale = (float(scale[0]), float(scale[1]))
+
+
 # ------------------------------------------------------ camera, primitives ----
 class Camera:
     """``scene/Camera.java`` reduced to what ``CompiledCameraCache.toCamera`` stores."""

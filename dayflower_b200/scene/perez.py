@@ -231,3 +231,68 @@ def perez_record(turbidity: float, sun_direction_world) -> np.ndarray:
     rec = np.concatenate([head, dist])
     pad = (-len(rec)) % 8
     return np.concatenate([rec, np.zeros(pad, dtype=np.float32)]).astype(np.float32)
+
+
+# ---- ImageLight ------------------------------------------------------------------
+def image_sky_rgb(image: np.ndarray, angle_rad: float, scale, dirs: np.ndarray) -> np.ndarray:
+    """``ImageLight.doRadianceSky`` for object-space unit directions (n, 3):
+    spherical texture coordinates (Point2F.sphericalCoordinates), rotated
+    counterclockwise, scaled, mapped to pixel space (Point2F.toImage) and looked
+    up with bilinear interpolation and wrap-around (ImageF.getColorRGB)."""
+    f32 = np.float32
+    h, w = image.shape[0], image.shape[1]
+    d = dirs.astype(np.float32)
+    phi = np.arctan2(d[:, 1].astype(np.float64), d[:, 0].astype(np.float64)).astype(f32)
+    phi = np.where(phi < 0, phi + f32(2.0 * math.pi), phi).astype(f32)
+    theta = np.arccos(np.clip(d[:, 2], -1.0, 1.0)).astype(f32)
+    u = (phi * f32(1.0 / (2.0 * math.pi))).astype(f32)
+    v = (theta * f32(1.0 / math.pi)).astype(f32)
+    c, s_ = f32(math.cos(angle_rad)), f32(math.sin(angle_rad))
+    ur = (u * c - v * s_).astype(f32)
+    vr = (v * c + u * s_).astype(f32)
+    us, vs = (ur * f32(scale[0])).astype(f32), (vr * f32(scale[1])).astype(f32)
+
+    def posmod(x, y):
+        return np.where(x < 0, np.fmod(np.fmod(x, y) + y, y), np.fmod(x, y)).astype(f32)
+
+    x = posmod((us * f32(w) - f32(0.5)).astype(f32), f32(w))
+    y = posmod((vs * f32(h) - f32(0.5)).astype(f32), f32(h))
+    x0, x1 = np.floor(x).astype(np.int64), np.ceil(x).astype(np.int64)
+    y0, y1 = np.floor(y).astype(np.int64), np.ceil(y).astype(np.int64)
+    xf, yf = (x - x0).astype(f32)[:, None], (y - y0).astype(f32)[:, None]
+    c00 = image[y0 % h, x0 % w]
+    c01 = image[y0 % h, x1 % w]
+    c10 = image[y1 % h, x0 % w]
+    c11 = image[y1 % h, x1 % w]
+    top = (1 - xf) * c00 + xf * c01
+    bot = (1 - xf) * c10 + xf * c11
+    return ((1 - yf) * top + yf * bot).astype(f32)
+
+
+def image_light_record(image: np.ndarray, angle_deg: float = 0.0, scale=(1.0, 1.0)) -> np.ndarray:
+    """The compiled ImageLight record (``CompiledLightCache.toImageLight``,
+    CompiledLightCache.java:1393-1460): object-to-world and world-to-object
+    matrices, angle, scale, radius 10, resolution, the 32x32 luminance
+    distribution of ``ImageLight.doCreateDistribution`` and the RGB image."""
+    img = np.ascontiguousarray(image, dtype=np.float32)
+    h, w = img.shape[0], img.shape[1]
+    ang = math.radians(angle_deg)
+    su = (np.arange(32, dtype=np.float32) + np.float32(0.5)) * np.float32(1.0 / 32.0)
+    U, V = np.meshgrid(su, su, indexing="ij")  # functions[u][v]
+    phi, th = U * np.float32(2.0 * math.pi), V * np.float32(math.pi)
+    d = np.stack([np.sin(th) * np.cos(phi), np.sin(th) * np.sin(phi), np.cos(th)], axis=-1).reshape(-1, 3).astype(np.float32)
+    rgb = image_sky_rgb(img, ang, scale, d)
+    lum = rgb[:, 0] * np.float32(0.212671) + rgb[:, 1] * np.float32(0.715160) + rgb[:, 2] * np.float32(0.072169)
+    funcs = (lum.reshape(32, 32) * np.sin(np.float32(math.pi) * V)).astype(np.float32)
+    dist = _distribution2_uv(funcs)
+    head = np.zeros(40, dtype=np.float32)
+    head[0:16] = SKY_OBJECT_TO_WORLD.reshape(-1)
+    head[16:32] = SKY_WORLD_TO_OBJECT.reshape(-1)
+    head[32] = ang
+    head[33], head[34] = scale
+    head[35] = 10.0  # ImageLight radius
+    head[36], head[37] = w, h
+    assert len(dist) == 2312
+    rec = np.concatenate([head, dist, img.reshape(-1)])
+    pad = (-len(rec)) % 8
+    return np.concatenate([rec, np.zeros(pad, dtype=np.float32)]).astype(np.float32)

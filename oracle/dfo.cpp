@@ -1595,6 +1595,33 @@ inline float dist2_pdf_remapped(const float* a, int off, float su, float sv) {
 
 inline V3 xyz_to_srgb_linear(V3 c);  // below
 
+// scene/light/ImageLight.java:544 doRadianceSky over the compiled record
+// (CompiledLightCache.java:1393-1460: angle +32, scale +33, resolution +36,
+// image +2352): Point2F.sphericalCoordinates -> rotateCounterclockwise ->
+// scale -> toImage, then ImageF.getColorRGB(x, y, WRAP_AROUND) (bilinear).
+inline V3 image_sky(const float* q, V3 d) {
+  const float phi = spherical_phi(d.x, d.y);  // Vector3F.sphericalPhi
+  const float theta = std::acos(saturate(d.z, -1.0f, 1.0f));
+  const float u = phi * (1.0f / (2.0f * kPi)), v = theta * (1.0f / kPi);
+  const float c = std::cos(q[32]), s = std::sin(q[32]);
+  const float ur = u * c - v * s, vr = v * c + u * s;
+  const float us = ur * q[33], vs = vr * q[34];
+  const float rx = q[36], ry = q[37];
+  auto posmod = [](float x, float y) { return x < 0.0f ? std::fmod(std::fmod(x, y) + y, y) : std::fmod(x, y); };
+  const float x = posmod(us * rx - 0.5f, rx), y = posmod(vs * ry - 0.5f, ry);
+  const int w = (int)rx, h = (int)ry;
+  const int x0 = (int)std::floor(x), x1 = (int)std::ceil(x), y0 = (int)std::floor(y), y1 = (int)std::ceil(y);
+  auto px = [&](int ix, int iy) {
+    ix = ((ix % w) + w) % w; iy = ((iy % h) + h) % h;  // PixelOperation.WRAP_AROUND
+    const float* p = q + 2352 + ((size_t)iy * w + ix) * 3;
+    return V3{p[0], p[1], p[2]};
+  };
+  if (x0 == x1 && y0 == y1) return px(x0, y0);
+  const float xf = x - (float)x0, yf = y - (float)y0;
+  auto lerp3 = [](V3 a, V3 b, float t) { return V3{lerpf(a.x, b.x, t), lerpf(a.y, b.y, t), lerpf(a.z, b.z, t)}; };
+  return lerp3(lerp3(px(x0, y0), px(x1, y0), xf), lerp3(px(x0, y1), px(x1, y1), xf), yf);
+}
+
 // scene/light/PerezLight.java:doRadianceSky (GPU form: renderer/gpu/AbstractLightKernel.java:1615)
 inline V3 perez_sky(const float* q, V3 dir) {
   if (dir.z < 0.0f) return {0, 0, 0};
@@ -1673,6 +1700,7 @@ inline LightRef light_ref(const Scene& sc, int index) {
     case kLightPoint: r.abs = r.rel * 8; break;
     case kLightSpot: r.abs = r.rel * 24; break;
     case kLightPerez: r.abs = sc.I("lightPerezLightOffsetArray")[r.rel]; break;
+    case kLightImage: r.abs = sc.I("lightImageLightOffsetArray")[r.rel]; break;
     default: r.abs = 0;
   }
   return r;
@@ -1822,6 +1850,20 @@ inline bool light_sample(const Scene& sc, const LightRef& lr, const Hit& h, floa
       *out = LightSample{L, p + dw * (2.0f * radius), dw, pr / (2.0f * kPi * kPi * st)};
       return true;
     }
+    case kLightImage: {  // scene/light/ImageLight.java:207 sampleRadianceIncoming
+      const float* q = sc.F("lightImageLightArray").data() + lr.abs;
+      float ru, rv;
+      dist2_remap(q, 40, u, v, &ru, &rv);
+      const float pr = dist2_pdf_remapped(q, 40, ru, rv);
+      if (pr == 0.0f) return false;
+      const float phi = ru * 2.0f * kPi, th = rv * kPi;
+      const V3 dobj = {std::sin(th) * std::cos(phi), std::sin(th) * std::sin(phi), std::cos(th)};
+      const V3 dw = normalize(transform_vector(load_m44(q), dobj));
+      const float st = sin_t(dobj);
+      if (st == 0.0f) return false;
+      *out = LightSample{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
+      return true;
+    }
   }
   return false;
 }
@@ -1845,16 +1887,29 @@ inline float light_pdf(const Scene& sc, const LightRef& lr, const Hit& h, V3 wi)
     float su = phi * (1.0f / (2.0f * kPi)), sv = std::acos(saturate(d.z, -1.0f, 1.0f)) * (1.0f / kPi);
     return dist2_pdf_remapped(q, 48, su, sv) / (2.0f * kPi * kPi * st);
   }
+  if (lr.id == kLightImage) {  // ImageLight.java:348
+    const float* q = sc.F("lightImageLightArray").data() + lr.abs;
+    const V3 d = normalize(transform_vector(load_m44(q + 16), wi));
+    const float st = std::sin(std::acos(saturate(d.z, -1.0f, 1.0f)));
+    if (st == 0.0f) return 0.0f;
+    float phi = std::atan2(d.y, d.x); if (phi < 0.0f) phi += 2.0f * kPi;
+    const float su = phi * (1.0f / (2.0f * kPi)), sv = std::acos(saturate(d.z, -1.0f, 1.0f)) * (1.0f / kPi);
+    return dist2_pdf_remapped(q, 40, su, sv) / (2.0f * kPi * kPi * st);
+  }
   return 0.0f;
 }
 
-// Light.evaluateRadianceEmitted(Ray3F): only the Perez light emits along a missed ray.
+// Light.evaluateRadianceEmitted(Ray3F): only the Perez and image lights emit along a missed ray.
 inline V3 light_Le_ray(const Scene& sc, const LightRef& lr, const Ray& r) {
   if (lr.id == kLightPerez) {
     const float* q = sc.F("lightPerezLightArray").data() + lr.abs;
     M44 w2o = load_m44(q + 16);
     V3 d = normalize(transform_vector(w2o, r.d));
     return sat0(perez_sky(q, d));
+  }
+  if (lr.id == kLightImage) {  // ImageLight.java:165
+    const float* q = sc.F("lightImageLightArray").data() + lr.abs;
+    return image_sky(q, normalize(transform_vector(load_m44(q + 16), r.d)));
   }
   return {0, 0, 0};
 }
