@@ -70,6 +70,10 @@ def parse():
                     help="run only the batched job mix (per-job arm and engine arm) and print its JSON object")
     ap.add_argument("--engine-only", action="store_true", help="with --batch-only: skip the per-job arm and the served sweep")
     ap.add_argument("--no-autotune", action="store_true", help="engine arm with the default wavefront shape")
+    ap.add_argument("--large", action="store_true",
+                    help="also render the large scene (10M-triangle terrain, 50k blob instances, 4096x2048 image light, 3840x2160, 256 spp)")
+    ap.add_argument("--large-only", action="store_true", help="render only the large scene and print its JSON object")
+    ap.add_argument("--large-spp", type=int, default=256)
     return ap.parse_args()
 
 
@@ -275,6 +279,50 @@ def batched_and_served(args, device=0):
                      "plain_per_job": "one job at a time in arrival order, measured per-job render times", "sweep": served}
 
 
+def large_scene_run(args, device=0):
+    """The large single scene, one job through the per-job renderer: a
+    9,999,392-triangle fractal terrain plus 50,000 instances of a 5,120-triangle
+    seeded blob (Disney materials), an ImageLight of a seeded 4096x2048 HDR
+    environment with a 0.5 degree sun of radiance 5e4; 3840x2160 film,
+    PATH_TRACING, maximum bounce 20, Russian roulette from bounce 5.  Timed
+    region: render(spp) with the scene resident (device events); the scene
+    upload and acceleration build are reported separately."""
+    from dayflower_b200 import GPURenderer, RenderingAlgorithm
+    from dayflower_b200.scene import generators as G
+    from dayflower_b200.scene.compiler import compile_scene
+
+    t0 = time.perf_counter()
+    cs = compile_scene(G.large_scene(), layout_version=2)
+    t_compile = time.perf_counter() - t0
+    r = GPURenderer(device=device)
+    try:
+        t0 = time.perf_counter()
+        r.setScene(cs)
+        t_scene = time.perf_counter() - t0
+        r.setRenderingAlgorithm(RenderingAlgorithm.PATH_TRACING)
+        r.setMaximumBounce(20)
+        r.setMinimumBounceRussianRoulette(5)
+        r.setup()
+        r.render(1)  # warm-up pass
+        r.clear()
+        spp = args.large_spp
+        assert r.render(spp)
+        ms = r.lastRenderMillis()
+        c = r.getCounters()
+        W, H = r.resolution
+        img = r.getImage()
+        paths = W * H * spp
+        return {"workload": "large: 9,999,392-tri terrain + 50,000 x 5,120-tri blob instances, Disney, 4096x2048 image light, "
+                            "3840x2160, PT %d spp, bounce 20, RR 5" % spp,
+                "paths_per_s": paths / (ms / 1000.0), "rays_per_s": c["rays"] / (ms / 1000.0), "render_s": ms / 1000.0,
+                "paths": paths, "rays_per_path": c["rays"] / paths, "gpu_launches": c["launches"],
+                "triangles_total": cs.stats["triangles"], "instances": cs.stats["primitives"] - 1,
+                "host_compile_s": t_compile, "set_scene_s": t_scene, "scene_bytes": int(cs.nbytes()),
+                "image_mean": float(img[..., :3].mean()), "timing": "device events around render(spp), scene resident"}
+    finally:
+        r.dispose()
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -304,6 +352,10 @@ def main():
     if args.batch_only:
         if rank == 0:
             print(json.dumps(batched_and_served(args, 0)[0]), flush=True)
+        return
+    if args.large_only:
+        if rank == 0:
+            print(json.dumps(large_scene_run(args, 0)), flush=True)
         return
     import torch
     import torch.distributed as dist
@@ -415,6 +467,8 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_batch:
             line["batched"], line["served"] = batched_and_served(args, local)
+        if world == 1 and args.large:
+            line["large"] = large_scene_run(args, local)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

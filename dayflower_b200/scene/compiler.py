@@ -284,6 +284,7 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
     push("lightIDAndOffsetArray", light_ids)
 
     # ---- primitives
+    mesh_bounds: Dict[int, np.ndarray] = {}
     for p in scene.primitives:
         sid, soff = shape(p.shape)
         mid, moff = material(p.material)
@@ -298,7 +299,11 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
             elif isinstance(p.shape, M.Rectangle) or isinstance(p.shape, tuple(_RECORD_SHAPES)):
                 pts = p.shape.corners()
             else:
-                pts = p.shape.triangles[:, 0:9].reshape(-1, 3)
+                key = id(p.shape)
+                if key not in mesh_bounds:  # the mesh's object-space box, shared by its instances
+                    q = p.shape.triangles[:, 0:9].reshape(-1, 3)
+                    mesh_bounds[key] = np.stack([q.min(axis=0), q.max(axis=0)])
+                pts = mesh_bounds[key]
             lo, hi = _world_aabb(pts, o2w)
             bvid = M.BV_AABB
             bvoff = sizes["boundingVolume3FAxisAlignedBoundingBox3FArray"] // 8

@@ -282,6 +282,72 @@ def image_light_scene(resolution=(96, 72), env=(256, 128), seed=9) -> M.Scene:
     return sc
 
 
+def blob_mesh(subdivisions: int = 4, seed: int = 21, amplitude: float = 0.3):
+    """A seeded blob: an icosphere of 20 * 4^subdivisions triangles (5,120 for
+    4) with its vertices pushed along their directions by smooth noise."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+             (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    v = [np.asarray(x, dtype=np.float64) / np.linalg.norm(x) for x in verts]
+    f = list(faces)
+    for _ in range(subdivisions):
+        cache, nf = {}, []
+
+        def mid(a, b):
+            k = (min(a, b), max(a, b))
+            if k not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[k] = len(v) - 1
+            return cache[k]
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    V = np.array(v)
+    rng = np.random.default_rng(seed)
+    k = rng.normal(size=(6, 3))
+    ph = rng.uniform(0, 2 * np.pi, size=6)
+    disp = sum(np.sin(V @ k[i] * (1.5 + 0.5 * i) + ph[i]) / (1.0 + i) for i in range(6))
+    P = V * (1.0 + amplitude * disp / np.abs(disp).max())[:, None]
+    return M.TriangleMesh.from_positions(P.astype(np.float32), np.array(f, dtype=np.int64))
+
+
+def large_scene(cells=2236, instances=50000, blob_subdivisions=4, resolution=(3840, 2160), env=(4096, 2048), seed=4,
+                extent=400.0) -> M.Scene:
+    """The large single scene: a fractal heightfield of 2 * cells^2 triangles
+    (2236 -> 9,999,392), `instances` instanced copies of one seeded blob mesh
+    (5,120 triangles) standing on it with random scale and rotation, every
+    copy with its own DisneyMaterial (base colour, metallic and roughness
+    uniform), lit by an ImageLight of a seeded env[0] x env[1] HDR
+    environment with a 0.5 degree sun disk of radiance 5e4."""
+    terrain, hf = heightfield_mesh(cells, extent, seed)
+    blob = blob_mesh(blob_subdivisions, seed=seed + 1)
+    cam = M.Camera(eye=(0.0, 0.12 * extent, 0.45 * extent), look_at=(0.0, 0.0, 0.0), fov_x_deg=60.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="large")
+    rng = np.random.default_rng(seed + 2)
+    sc.add(M.Primitive(terrain, M.Disney(color=(0.45, 0.42, 0.35), roughness=0.7)))
+    xs = rng.uniform(-0.45 * extent, 0.45 * extent, size=instances)
+    zs = rng.uniform(-0.45 * extent, 0.45 * extent, size=instances)
+    scale = rng.uniform(0.5, 2.0, size=instances)
+    ys = _height_at(hf, xs, zs) + 0.6 * scale
+    ang = rng.uniform(0.0, 2.0 * np.pi, size=instances)
+    cols = rng.uniform(0.05, 0.95, size=(instances, 3))
+    met = rng.uniform(0.0, 1.0, size=instances)
+    rough = rng.uniform(0.05, 0.95, size=instances)
+    for k in range(instances):
+        c, s_ = math.cos(ang[k]), math.sin(ang[k])
+        m = np.eye(4)
+        m[:3, :3] = np.array([[c, 0, s_], [0, 1, 0], [-s_, 0, c]]) * scale[k]
+        m[:3, 3] = (xs[k], ys[k], zs[k])
+        mat = M.Disney(color=tuple(float(x) for x in cols[k]), metallic=float(met[k]), roughness=float(rough[k]))
+        sc.add(M.Primitive(blob, mat, M.Transform.from_matrix(m)))
+    sc.lights.append(M.ImageLight(environment_image(env[0], env[1], seed=seed + 3)))
+    return sc
+
+
 def _rot_x(deg, position, scale=1.0):
     """Object-to-world: rotate about x by `deg`, scale, then translate."""
     c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))

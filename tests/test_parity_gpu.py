@@ -42,11 +42,17 @@ def image_light():
 
 
 @pytest.fixture(scope="module")
+def instances():
+    # the large scene's construction at test size: instanced blob meshes, Disney, image light
+    return compile_scene(G.large_scene(cells=48, instances=120, resolution=(128, 72), env=(128, 64), extent=40.0), layout_version=2)
+
+
+@pytest.fixture(scope="module")
 def terrain():
     return compile_scene(G.terrain_spheres(cells=128, n_spheres=300, resolution=(160, 90), seed=11), layout_version=2)
 
 
-@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney", "materials", "image_light"])
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney", "materials", "image_light", "instances"])
 def test_ray_casting_hit_ids(scene_name, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.RAY_CASTING)
@@ -70,7 +76,7 @@ def test_depth_camera(scene_name, request):
     assert np.mean(np.all(np.abs(mg - mo) <= 1e-4 + 1e-4 * np.abs(mo), axis=-1)) >= 0.999
 
 
-@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16), ("materials", 16), ("image_light", 16)])
+@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16), ("materials", 16), ("image_light", 16), ("instances", 8)])
 def test_path_tracing_sigma(scene_name, spp, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.PATH_TRACING, spp=spp, max_bounce=8)
