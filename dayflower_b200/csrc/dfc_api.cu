@@ -57,7 +57,7 @@ struct dfc_renderer {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_marks;  // (stage, index of the start event)
   int sm_count = 148;
-  int trace_blocks = 6, ao_blocks = 5;  // resident blocks per SM of k_trace / k_trace_ao (persistent grids)
+  int trace_blocks = 6, ao_blocks = 5, rt_blocks = 4;  // resident blocks per SM of k_trace / k_trace_ao / k_ray_trace
 };
 
 namespace {
@@ -266,6 +266,11 @@ int enqueue_pass(dfc_renderer* r) {
       stage_end(r, ev);
       r->launches += 4;
     }
+  } else if (algo == DFC_RAY_TRACING) {
+    ShadeArgs a = shade_args(r, 0);
+    k_ray_trace<<<r->sm_count * r->rt_blocks, kTraceThreads, 0, r->stream>>>(a, r->d_overflow.as<unsigned>(),
+                                                                             r->d_ray_total.as<unsigned long long>());
+    r->launches += 1;
   } else {
     trace_kernel(r)<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, 0));
     ShadeArgs a = shade_args(r, 0);
@@ -288,7 +293,8 @@ int enqueue_pass(dfc_renderer* r) {
       r->launches += 2;
     }
   }
-  k_sum_counts<<<1, 1, 0, r->stream>>>(counts, algo == DFC_PATH_TRACING ? steps : 1, r->d_ray_total.as<unsigned long long>());
+  if (algo != DFC_RAY_TRACING)  // the ray tracer counts its own rays
+    k_sum_counts<<<1, 1, 0, r->stream>>>(counts, algo == DFC_PATH_TRACING ? steps : 1, r->d_ray_total.as<unsigned long long>());
   DFC_CK(cudaGetLastError(), "kernel launch");
   r->pass++;
   r->total_paths += r->paths;
@@ -319,6 +325,8 @@ int dfc_create(int device, dfc_renderer** out) {
     r->trace_blocks = std::min(r->trace_blocks, nb);
   nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_ao, kTraceThreads, 0) == cudaSuccess && nb > 0) r->ao_blocks = nb;
+  nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ray_trace, kTraceThreads, 0) == cudaSuccess && nb > 0) r->rt_blocks = nb;
   cudaGetLastError();
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
@@ -455,7 +463,6 @@ int dfc_render(dfc_renderer* r, int passes, int* completed) {
   std::lock_guard<std::mutex> lk(r->mu);
   if (passes < 1) return fail(r, DFC_E_INVALID_ARG, "renderPasses < 1");  // AbstractGPURenderer.java:323
   if (!r->set_up) return fail(r, DFC_E_STATE, "render() before setup()");
-  if (r->algorithm == DFC_RAY_TRACING) return fail(r, DFC_E_UNSUPPORTED, "RAY_TRACING is not implemented by this renderer");
   cudaSetDevice(r->device);
   if (r->algorithm == DFC_AMBIENT_OCCLUSION) {
     const size_t n = (size_t)r->paths * r->ao_samples;

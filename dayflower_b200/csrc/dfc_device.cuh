@@ -780,7 +780,9 @@ DFC_D void build_disney(const DMaterial& m, Bsdf* B) {
 // for the resolved kinds (scene/material/*Material.java).  u_material is the
 // random number ClearCoatMaterial draws per hit (ClearCoatMaterial.java:323).
 // Returns false when the material gives no BSDF (the ray passes through).
-DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_material, Bsdf* B) {
+// multi = isAllowingMultipleLobes: false (the ray tracer) builds smooth glass
+// as separate specular reflection and transmission lobes (GlassMaterial.java:520).
+DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_material, Bsdf* B, bool multi = true) {
   B->n = 0; B->eta = 1.0f;
   B->fr_i = 1.0f; B->fr_t = 1.0f; B->bt_a = 1.0f; B->bt_b = 1.0f; B->metallic = 0.0f;
   B->ca = V3{0, 0, 0}; B->cb = V3{0, 0, 0};
@@ -792,8 +794,14 @@ DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_m
       B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0));
       break;
     case kMatGlassSpec:
-      B->l[B->n++] = make_lobe(kFresnelSpec, kRefl | kTrans | kSpecular, ld3(m.c0));
-      B->ca = ld3(m.c1);
+      if (multi) {
+        B->l[B->n++] = make_lobe(kFresnelSpec, kRefl | kTrans | kSpecular, ld3(m.c0));
+        B->ca = ld3(m.c1);
+      } else {
+        if (m.has_kr) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0)); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+        if (m.has_kt) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c1), 1.0f, m.eta);
+        B->fr_i = 1.0f; B->fr_t = m.eta;
+      }
       B->bt_a = 1.0f; B->bt_b = m.eta; B->eta = m.eta;
       break;
     case kMatGlassRough: {

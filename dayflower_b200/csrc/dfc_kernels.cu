@@ -915,6 +915,109 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_ao(AoArgs a) {
   }
 }
 
+// ---- RAY_TRACING --------------------------------------------------------------
+// scene/Scene.java:786 doRadianceRayTracer: at each hit its emission, every
+// light sampled once (checkLightVisibility: closest hit on the light for area
+// lights, occlusion otherwise, t in (0.001, distance + 0.001)), then below the
+// bounce limit the BSDF's specular reflection and specular transmission
+// samples recursively; no BSDF: the ray passes through.  The recursion is a
+// depth-first walk over an explicit per-thread stack; each node's weight is the
+// product of f |cos| / pdf along its branch.  Random numbers per node n (root
+// 0; reflection, transmission, pass-through children 3n+1, 3n+2, 3n+3): key
+// rng_path_key(sample key, n, kRtSalt), dims 0-1 reflection, 2-3
+// transmission, 4 the material draw, 8+3k.. light k (as the oracle).
+constexpr uint32_t kRtSalt = 0x52545243u;
+constexpr int kRtMaxNodes = 4096;  // nodes per sample; beyond it the tree is cut and counted
+constexpr int kRtStack = 24;
+struct RtEntry { V3 o, d, w; int bounce; uint32_t nid; };
+
+__global__ void __launch_bounds__(kTraceBlock) k_ray_trace(ShadeArgs a, unsigned* overflow, unsigned long long* rays) {
+  __shared__ int stack_smem[kStack * kTraceBlock];
+  int* tstack = stack_smem + threadIdx.x;
+  const SceneView& S = a.scene;
+  const unsigned stride = gridDim.x * blockDim.x;
+  unsigned long long nrays = 0;
+  for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < a.paths; p += stride) {
+    const uint4 meta = a.meta[p];
+    if (!(meta.w & kAlive)) continue;  // no camera ray: no sample (AbstractCPURenderer.java:221)
+    const uint32_t key = meta.y;
+    const float4 ro = a.ray_o[p], rd = a.ray_d[p];
+    RtEntry st[kRtStack];
+    int sp = 0, nodes = 0;
+    st[sp++] = RtEntry{V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, V3{1, 1, 1}, 0, 0u};
+    V3 L = {0, 0, 0};
+    const bool rec = a.record_primary && p < a.pixels;
+    while (sp > 0) {
+      const RtEntry e = st[--sp];
+      if (++nodes > kRtMaxNodes) { atomicAdd(overflow, 1u); break; }
+      const uint32_t nk = rng_path_key(key, e.nid, kRtSalt);
+      Hit h = {0.0f, -1, -1, 0.0f};
+      ++nrays;
+      const bool found = trace_ray<true>(S, e.o, e.d, kFltMax, false, &h, tstack, overflow);
+      if (!found) {
+        if (rec && e.nid == 0u) { a.primary_prim[p] = -1; a.primary_t[p] = __int_as_float(0x7fc00000); }
+        V3 Le = {0, 0, 0};
+        for (int k = 0; k < S.light_count; ++k) Le = Le + light_Le_miss(S, S.lights[k], e.d);
+        L = L + mul(e.w, Le);
+        continue;
+      }
+      const DPrim& pr = S.prims[h.prim];
+      Surface sf;
+      surface_of<true>(S, pr, h.aux, e.o, e.d, h.t_obj, &sf);
+      if (rec && e.nid == 0u) { a.primary_prim[p] = h.prim; a.primary_t[p] = world_t(pr, e.o, sf); }
+      Bsdf B;
+      if (!build_bsdf(S.materials[pr.material], sf, e.d, rng_uniform(nk, 4), &B, false)) {
+        if (sp < kRtStack) st[sp++] = RtEntry{sf.p, e.d, e.w, e.bounce, e.nid * 3u + 3u};
+        else atomicAdd(overflow, 1u);
+        continue;
+      }
+      const V3 n = sf.s.w, wo = -e.d;
+      V3 Ln;
+      if (pr.light >= 0) {
+        const DLight& lt = S.lights[pr.light];
+        Ln = (lt.two_sided || dot(n, wo) > 0.0f) ? ld3(lt.radiance) : V3{0, 0, 0};
+      } else {
+        Ln = ld3(S.materials[pr.material].emission);
+      }
+      for (int k = 0; k < S.light_count; ++k) {
+        const DLight& lt = S.lights[k];
+        LightS ls;
+        if (!light_sample(S, lt, sf, rng_uniform(nk, 8 + 3 * k), rng_uniform(nk, 9 + 3 * k), rng_uniform(nk, 10 + 3 * k), &ls)) continue;
+        if (is_black(ls.L) || !(ls.pdf > 0.0f)) continue;
+        const V3 f = bsdf_f(B, kAll, ls.wi);
+        if (is_black(f)) continue;
+        const V3 toL = ls.p - sf.p;
+        const float dist = fabsf(len(toL)) + 0.001f;
+        Hit sh = {0.0f, -1, -1, 0.0f};
+        ++nrays;
+        bool vis;
+        if (lt.type == kLightDiffuseArea) {
+          vis = trace_ray<true>(S, sf.p, normalize(toL), dist, false, &sh, tstack, overflow) && S.prims[sh.prim].light == k;
+        } else {
+          vis = !trace_ray<true>(S, sf.p, normalize(toL), dist, true, &sh, tstack, overflow);
+        }
+        if (vis) Ln = Ln + mul(f, ls.L) * (fabsf(dot(ls.wi, n)) * (1.0f / ls.pdf));
+      }
+      L = L + mul(e.w, Ln);
+      if (e.bounce + 1 < a.max_bounce) {
+#pragma unroll 1
+        for (int b = 0; b < 2; ++b) {
+          BSample bs;
+          if (!bsdf_sample(B, b == 0 ? (kSpecular | kRefl) : (kSpecular | kTrans), rng_uniform(nk, 2 * b), rng_uniform(nk, 2 * b + 1), &bs)) continue;
+          const float c = fabsf(dot(bs.wi, n));
+          if (is_black(bs.f) || !(bs.pdf > 0.0f) || !(c > 0.0f)) continue;
+          if (sp < kRtStack) st[sp++] = RtEntry{sf.p, bs.wi, mul(e.w, bs.f * (c / bs.pdf)), e.bounce + 1, e.nid * 3u + 1u + (uint32_t)b};
+          else atomicAdd(overflow, 1u);
+        }
+      }
+    }
+    film_add(a, meta.x, L);
+  }
+  // rays traced by this block's threads, one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) nrays += __shfl_down_sync(0xffffffffu, nrays, off);
+  if ((threadIdx.x & 31u) == 0u && nrays) atomicAdd(rays, nrays);
+}
+
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples) {
   const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.paths) return;

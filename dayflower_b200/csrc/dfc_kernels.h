@@ -200,6 +200,9 @@ __global__ void k_shade_path_batch(ShadeArgs a);     // batch engine: scene, fil
 __global__ void k_shade_path_batch_records(ShadeArgs a);
 __global__ void k_shade_primary(ShadeArgs a, int algorithm);
 __global__ void k_trace_ao(AoArgs a);
+// RAY_TRACING (scene/Scene.java:786 doRadianceRayTracer): one thread per camera
+// sample walks the sample's specular reflection/transmission tree depth first.
+__global__ void k_ray_trace(ShadeArgs a, unsigned* overflow, unsigned long long* rays);
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);
 __global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out);
 

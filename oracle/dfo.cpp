@@ -2005,6 +2005,57 @@ struct Params {
 };
 
 // scene/Scene.java:451 radiancePathTracer
+// scene/Scene.java:786 doRadianceRayTracer (Whitted): at each hit, emission,
+// every light sampled once (Light.sampleRadianceIncoming, checkLightVisibility),
+// then, below the bounce limit, the specular reflection and the specular
+// transmission samples of the BSDF (built with isAllowingMultipleLobes = false)
+// traced recursively; a material without a BSDF passes the ray through.
+// Random numbers: node n of a sample's tree (root 0; reflection, transmission
+// and pass-through children 3n+1, 3n+2, 3n+3) has key rng_path_key(key, n, kRtSalt);
+// dims 0-1 reflection, 2-3 transmission, 4 the material draw, 8+3k.. light k.
+// A tree is cut after kRtMaxNodes nodes (counted in *overflow).
+constexpr uint32_t kRtSalt = 0x52545243u;
+constexpr int kRtMaxNodes = 4096;
+struct RtCtx { uint32_t key; int nodes; bool overflow; };
+inline V3 rt_node(const Scene& sc, Ray ray, const Params& P, RtCtx& C, uint32_t nid, int bounce, RayStats* st, bool* unsupported) {
+  if (++C.nodes > kRtMaxNodes) { C.overflow = true; return {0, 0, 0}; }
+  const uint32_t nk = rng_path_key(C.key, nid, kRtSalt);
+  Hit h;
+  if (!scene_intersect(sc, ray, kTMinimum, kTMaximum, &h, st)) {
+    V3 L = {0, 0, 0};
+    for (int k = 0; k < (int)sc.lights.size(); ++k) L = L + light_Le_ray(sc, light_ref(sc, k), ray);
+    return L;
+  }
+  const int32_t* pr = sc.prims.data() + h.prim * 8;
+  Bsdf B; bool sup;
+  if (!build_bsdf(sc, pr[4], pr[5], h, false, rng_uniform(nk, 4), &B, &sup)) {
+    if (!sup) *unsupported = true;
+    return rt_node(sc, make_ray(h.w.p, ray.d), P, C, nid * 3u + 3u, bounce, st, unsupported);
+  }
+  const V3 n = h.w.s.w, wo = -ray.d;
+  V3 L = hit_Le(sc, h, wo);
+  for (int k = 0; k < (int)sc.lights.size(); ++k) {
+    const LightRef lr = light_ref(sc, k);
+    LightSample ls;
+    if (!light_sample(sc, lr, h, rng_uniform(nk, 8 + 3 * k), rng_uniform(nk, 9 + 3 * k), rng_uniform(nk, 10 + 3 * k), &ls)) continue;
+    if (black(ls.L) || !(ls.pdf > 0.0f)) continue;
+    const V3 f = bsdf_f(B, kAll, ls.wi);
+    if (!black(f) && visible(sc, h, lr, ls, st)) L = L + mul(f, ls.L) * std::fabs(dot(ls.wi, n)) * (1.0f / ls.pdf);
+  }
+  if (bounce + 1 < P.max_bounce) {
+    const int flags[2] = {kSpecular | kRefl, kSpecular | kTrans};
+    for (int b = 0; b < 2; ++b) {  // doComputeSpecularReflection, doComputeSpecularTransmission
+      BsdfSample bs;
+      if (!bsdf_sample(B, flags[b], rng_uniform(nk, 2 * b), rng_uniform(nk, 2 * b + 1), &bs)) continue;
+      const float c = std::fabs(dot(bs.wi, n));
+      if (black(bs.f) || !(bs.pdf > 0.0f) || !(c > 0.0f)) continue;
+      const V3 Li = rt_node(sc, make_ray(h.w.p, bs.wi), P, C, nid * 3u + 1u + (uint32_t)b, bounce + 1, st, unsupported);
+      L = L + mul(bs.f, Li) * c * (1.0f / bs.pdf);
+    }
+  }
+  return L;
+}
+
 inline V3 radiance_path(const Scene& sc, Ray ray, const Params& P, uint32_t key, RayStats* st, bool* unsupported) {
   const int nl = (int)sc.lights.size();
   V3 L = {0, 0, 0}, beta = {1, 1, 1};
@@ -2212,6 +2263,7 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
   std::atomic<int> next_row(rb);
   std::atomic<long long> rays(0);
   std::atomic<int> unsupported(0);
+  std::atomic<int> rt_overflow(0);
   auto work = [&]() {
     RayStats st;
     bool unsup = false;
@@ -2236,6 +2288,13 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
             case kAlgoAO: c = radiance_ao(*sc, r, P, key, &st, &h); break;
             case kAlgoDepth: c = radiance_depth(*sc, r, P, &st, &h); break;
             case kAlgoRayCast: c = radiance_raycast(*sc, r, P, &st, &h); break;
+            case kAlgoRayTrace: {
+              RtCtx C{key, 0, false};
+              c = rt_node(*sc, r, P, C, 0u, 0, &st, &unsup);
+              if (C.overflow) rt_overflow = 1;
+              if (k == 0 && (hit_prim || hit_t)) { RayStats dummy; scene_intersect(*sc, r, kTMinimum, kTMaximum, &h, &dummy); }
+              break;
+            }
             case kAlgoPath: default: {
               c = radiance_path(*sc, r, P, key, &st, &unsup);
               if (k == 0 && (hit_prim || hit_t)) { RayStats dummy; scene_intersect(*sc, r, kTMinimum, kTMaximum, &h, &dummy); }
@@ -2262,6 +2321,7 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
   work();
   for (auto& t : pool) t.join();
   if (unsupported.load()) return -2;
+  if (rt_overflow.load()) return -5;  // a RAY_TRACING tree exceeded kRtMaxNodes
   return rays.load();
 }
 

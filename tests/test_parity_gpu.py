@@ -94,3 +94,15 @@ def test_ambient_occlusion_sigma(scene_name, request):
     o = PT.render_oracle(cs, RA.AMBIENT_OCCLUSION, spp=4, ao_samples=16, ao_distance=200.0)
     ok, _, _ = PT.sigma_test(g, o)
     assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
+
+
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "materials"])
+def test_ray_tracing_sigma(scene_name, request):
+    # Whitted ray tracer (Scene.java:786): every light per hit, specular reflection and transmission recursively
+    cs = request.getfixturevalue(scene_name)
+    g = PT.render_gpu(cs, RA.RAY_TRACING, spp=8, max_bounce=8)
+    o = PT.render_oracle(cs, RA.RAY_TRACING, spp=8, max_bounce=8)
+    PT.check_primary(g, o, PT.render_oracle_no_drift(cs, RA.RAY_TRACING))
+    ok, mg, mo = PT.sigma_test(g, o)
+    assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
+    assert abs(mg.mean() - mo.mean()) <= 0.02 * max(mo.mean(), 1e-3) + 1e-4
