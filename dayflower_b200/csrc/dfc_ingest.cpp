@@ -510,11 +510,12 @@ struct Decoder {
 
   // CompiledShape3FCache.java:90-310 record lengths
   struct RecordArray { int id; const char* name; int length; size_t base; };
-  RecordArray record_arrays[7] = {
+  // (length 0: Polygon3F, variable length 13 + 2 * point count)
+  RecordArray record_arrays[8] = {
       {kShapeDisk, "shape3FDisk3FArray", 4, 0}, {kShapeCylinder, "shape3FCylinder3FArray", 4, 0},
       {kShapeCone, "shape3FCone3FArray", 4, 0}, {kShapeParaboloid, "shape3FParaboloid3FArray", 4, 0},
       {kShapeHyperboloid, "shape3FHyperboloid3FArray", 16, 0}, {kShapeCuboid, "shape3FRectangularCuboid3FArray", 8, 0},
-      {kShapeTorus, "shape3FTorus3FArray", 2, 0}};
+      {kShapeTorus, "shape3FTorus3FArray", 2, 0}, {kShapePolygon, "shape3FPolygon3FArray", 0, 0}};
 
   void run() {
     const auto& P = I("primitiveArray");
@@ -583,12 +584,19 @@ struct Decoder {
           pr.data = 0;
           break;
         case kShapeDisk: case kShapeCylinder: case kShapeCone: case kShapeParaboloid: case kShapeHyperboloid:
-        case kShapeCuboid: case kShapeTorus: {
+        case kShapeCuboid: case kShapeTorus: case kShapePolygon: {
           const RecordArray* ra = nullptr;
           for (const RecordArray& x : record_arrays) if (x.id == pr.shape) ra = &x;
-          const size_t n = F(ra->name).size();
-          if (soff < 0 || soff % ra->length != 0 || (size_t)soff + (size_t)ra->length > n)
+          const auto& A = F(ra->name);
+          const size_t n = A.size();
+          if (ra->length == 0) {  // Polygon3F: 13 + 2 * count floats
+            if (soff < 0 || (size_t)soff + 13 > n) throw Fail{DFC_E_INVALID_ARG, "polygon offset out of range"};
+            const float cnt = A[soff + 12];
+            if (!(cnt >= 3.0f) || cnt != std::floor(cnt) || (size_t)soff + 13 + 2 * (size_t)cnt > n)
+              throw Fail{DFC_E_INVALID_ARG, "polygon point count out of range"};
+          } else if (soff < 0 || soff % ra->length != 0 || (size_t)soff + (size_t)ra->length > n) {
             throw Fail{DFC_E_INVALID_ARG, std::string(ra->name) + " offset out of range"};
+          }
           pr.data = (int)(ra->base + (size_t)soff);
           hs.record_shapes = true;
           break;

@@ -221,6 +221,41 @@ DFC_D float torus_t(const float* q, V3 o, V3 d, float tmin, float tmax) {
   return -1.0f;
 }
 
+// geometry/shape/Polygon3F.java over the compiled record: points 0, 1 and n-1
+// at +0, +3, +6, surface normal +9, point count +12, the polygon projected on
+// its plane at +13 (two floats per point).  Containment is Polygon2F.contains:
+// on an edge (LineSegment2F.contains) or inside by the crossing test.
+DFC_D bool polygon_contains(const float* q, V3 p) {
+  const V3 a = ld3(q), w = ld3(q + 9);
+  const V3 u = normalize(ld3(q + 3) - a), v = cross(w, u);
+  const V3 ap = p - a;
+  const float px = dot(ap, u), py = dot(ap, v);
+  const int n = (int)q[12];
+  const float* P = q + 13;
+  for (int i = 0, j = 1; i < n; ++i, j = (j + 1) % n) {
+    const float ax = P[2 * i], ay = P[2 * i + 1], bx = P[2 * j], by = P[2 * j + 1];
+    const float dx = px - ax, dy = py - ay, ex = bx - ax, ey = by - ay;
+    if (dx * ey - dy * ex != 0.0f) continue;
+    if (fabsf(ex) >= fabsf(ey) ? (ex > 0.0f ? ax <= px && px <= bx : bx <= px && px <= ax)
+                               : (ey > 0.0f ? ay <= py && py <= by : by <= py && py <= ay))
+      return true;
+  }
+  bool inside = false;
+  for (int i = 0, j = n - 1; i < n; j = i++) {
+    const float ix = P[2 * i], iy = P[2 * i + 1], jx = P[2 * j], jy = P[2 * j + 1];
+    if ((iy > py) != (jy > py) && px < (jx - ix) * (py - iy) / (jy - iy) + ix) inside = !inside;
+  }
+  return inside;
+}
+DFC_D float polygon_t(const float* q, V3 o, V3 d, float tmin, float tmax) {  // Polygon3F.java:321
+  const V3 n = ld3(q + 9);
+  const float dp = dot(n, d);
+  if (dp == 0.0f) return -1.0f;
+  const float t = dot(ld3(q) - o, n) / dp;
+  if (t > tmin && t < tmax && polygon_contains(q, point_at(o, d, t))) return t;
+  return -1.0f;
+}
+
 // Object-space t of one record shape; -1 on a miss.  Out of line, so that
 // its double-precision torus solve stays out of the traversal loop's frame.
 __device__ __noinline__ float record_shape_t(int shape, const float* q, V3 o, V3 d, float tmin, float tmax) {
@@ -228,6 +263,7 @@ __device__ __noinline__ float record_shape_t(int shape, const float* q, V3 o, V3
     case kShapeDisk: return disk_t(q, o, d, tmin, tmax);
     case kShapeCuboid: return cuboid_t(q, o, d, tmin, tmax);
     case kShapeTorus: return torus_t(q, o, d, tmin, tmax);
+    case kShapePolygon: return polygon_t(q, o, d, tmin, tmax);
     case kShapeCylinder: case kShapeCone: case kShapeParaboloid: case kShapeHyperboloid:
       return quadric_root_t(shape, q, o, d, tmin, tmax);
     default: return -1.0f;
@@ -304,6 +340,21 @@ __device__ __noinline__ Surface record_shape_surface(int shape, const float* q, 
       if (x0 || x1) { s.tu = nrm(p.z, q[5], q[2]); s.tv = nrm(p.y, q[4], q[1]); }
       else if (y0 || y1) { s.tu = nrm(p.x, q[3], q[0]); s.tv = nrm(p.z, q[5], q[2]); }
       else if (z0 || z1) { s.tu = nrm(p.x, q[3], q[0]); s.tv = nrm(p.y, q[4], q[1]); }
+      break;
+    }
+    case kShapePolygon: {  // Polygon3F.doCreateSurfaceIntersection / doCreateTextureCoordinates
+      const V3 n = ld3(q + 9);
+      const V3 na = {fabsf(n.x), fabsf(n.y), fabsf(n.z)};
+      const bool isx = na.x > na.y && na.x > na.z, isy = na.y > na.z;
+      auto px = [&](const float* c) { return isx ? c[1] : isy ? c[2] : c[0]; };
+      auto py = [&](const float* c) { return isx ? c[2] : isy ? c[0] : c[1]; };
+      // vB from the last point, vC from the second, as the reference pairs them
+      const float ax = px(q), ay = py(q), abx = px(q + 6) - ax, aby = py(q + 6) - ay, acx = px(q + 3) - ax, acy = py(q + 3) - ay;
+      const float dr = 1.0f / (abx * acy - aby * acx);
+      const float hu = isx ? p.y : isy ? p.z : p.x, hv = isx ? p.z : isy ? p.x : p.y;
+      s.g = onb_w(n);
+      s.tu = hu * (-aby * dr) + hv * (abx * dr) + (ax * aby - ay * abx) * dr;
+      s.tv = hu * (acy * dr) + hv * (-acx * dr) + (acx * ay - acy * ax) * dr;
       break;
     }
     default: {  // torus

@@ -114,7 +114,8 @@ def _world_aabb(points_obj: np.ndarray, o2w: np.ndarray):
 # Shapes stored as one fixed-length record each (CompiledShape3FCache.java:90-310).
 _RECORD_SHAPES = {M.Disk: "shape3FDisk3FArray", M.Cylinder: "shape3FCylinder3FArray", M.Cone: "shape3FCone3FArray",
                   M.Paraboloid: "shape3FParaboloid3FArray", M.Hyperboloid: "shape3FHyperboloid3FArray",
-                  M.RectangularCuboid: "shape3FRectangularCuboid3FArray", M.Torus: "shape3FTorus3FArray"}
+                  M.RectangularCuboid: "shape3FRectangularCuboid3FArray", M.Torus: "shape3FTorus3FArray",
+                  M.Polygon: "shape3FPolygon3FArray"}
 
 
 def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> CompiledScene:

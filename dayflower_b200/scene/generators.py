@@ -358,8 +358,8 @@ def _rot_x(deg, position, scale=1.0):
 
 
 def quadrics_scene(resolution=(128, 96), with_lights=True) -> M.Scene:
-    """Disk, cylinder, cone, paraboloid, hyperboloid, rectangular cuboid and torus
-    (full and partial sweeps) standing on a ground plane, z-up objects turned
+    """Disk, cylinder, cone, paraboloid, hyperboloid, rectangular cuboid, torus
+    (full and partial sweeps) and polygons standing on a ground plane, z-up objects turned
     upright, lit by a point light, a directional light and a spherical area light."""
     cam = M.Camera(eye=(0.0, 3.8, 9.0), look_at=(0.0, 1.0, 0.0), fov_x_deg=70.0, resolution=resolution)
     sc = M.Scene(camera=cam, name="quadrics")
@@ -375,6 +375,11 @@ def quadrics_scene(resolution=(128, 96), with_lights=True) -> M.Scene:
         (M.RectangularCuboid((-0.7, -0.7, 0.0), (0.7, 0.7, 1.4)), M.Matte(kd=(0.5, 0.5, 0.8)), _rot_x(up, (1.5, 0.0, 3.0))),
         (M.Torus(0.35, 1.0), M.Metal(roughness_u=0.15, roughness_v=0.15), _rot_x(-60.0, (-1.5, 1.4, 3.5))),
         (M.Torus(0.25, 0.8), M.Matte(kd=(0.9, 0.5, 0.1)), _rot_x(0.0, (4.5, 2.2, 3.0))),
+        # a concave pentagon and a hexagon standing upright (Polygon3F)
+        (M.Polygon([(0, 0, 0), (1.6, 0, 0), (1.6, 1.4, 0), (0.8, 0.6, 0), (0, 1.4, 0)]), M.Matte(kd=(0.3, 0.4, 0.9)),
+         M.Transform.from_matrix(np.array([[1, 0, 0, -4.6], [0, 1, 0, 0.0], [0, 0, 1, 3.0], [0, 0, 0, 1]], dtype=np.float64))),
+        (M.Polygon([(math.cos(k * math.pi / 3), math.sin(k * math.pi / 3), 0.0) for k in range(6)]), M.Plastic(kd=(0.8, 0.8, 0.3)),
+         M.Transform.from_matrix(np.array([[1, 0, 0, 0.0], [0, 1, 0, 4.4], [0, 0, 1, 0.5], [0, 0, 0, 1]], dtype=np.float64))),
     ]
     for shp, mat, tr in shapes:
         sc.add(M.Primitive(shp, mat, tr))

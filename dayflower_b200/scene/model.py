@@ -299,6 +299,36 @@ class Torus(Shape):
         return _box_corners((-r, -r, -r), (r, r, r))
 
 
+class Polygon(Shape):
+    """``geometry/shape/Polygon3F``: a planar polygon of n >= 3 coplanar points."""
+    ID = SHAPE_POLYGON
+
+    def __init__(self, points):
+        pts = np.asarray(points, dtype=np.float32).reshape(-1, 3)
+        if pts.shape[0] < 3:
+            raise ValueError("a polygon needs at least 3 points")
+        self.points = pts
+        a, b, c = (pts[0].astype(np.float32), pts[1].astype(np.float32), pts[2].astype(np.float32))
+        # Vector3F.normalNormalized(a, b, c) = normalize(cross(normalize(b - a), normalize(c - a)))
+        n = np.cross(normalize(b - a), normalize(c - a))
+        self.normal = normalize(n).astype(np.float32)
+        u = normalize(b - a)
+        v = np.cross(self.normal, u)
+        d = pts - a
+        if np.abs(d @ self.normal).max() > 1e-4 * max(1.0, float(np.abs(pts).max())):
+            raise ValueError("The provided Point3F instances are not coplanar.")
+        self.projected = np.stack([d @ u, d @ v], axis=1).astype(np.float32)  # Polygon3F.doCreateProjectedPolygon
+
+    def to_array(self):
+        """``CompiledShape3FCache.toPolygon3F``: points 0, 1, n-1, normal, count, projected points, padded to 8."""
+        rec = np.concatenate([self.points[0], self.points[1], self.points[-1], self.normal, [len(self.points)],
+                              self.projected.reshape(-1)]).astype(np.float32)
+        return np.concatenate([rec, np.zeros((-len(rec)) % 8, dtype=np.float32)])
+
+    def corners(self):
+        return self.points
+
+
 # ------------------------------------------------------------- materials ----
 @dataclass(eq=False)
 class Material:

@@ -644,6 +644,54 @@ inline float mesh_t(const Scene& sc, int mesh_off, const Ray& r, float tmin, flo
   return best;
 }
 
+// geometry/shape/Polygon3F.java over the compiled record (CompiledShape3FCache:
+// points 0, 1 and n-1 at +0, +3, +6, surface normal +9, point count +12, the
+// polygon projected on its plane at +13, two floats per point).
+inline bool polygon_contains(const float* q, V3 p) {  // Polygon3F.doContains + Polygon2F.contains
+  const V3 a = {q[0], q[1], q[2]}, b = {q[3], q[4], q[5]}, w = {q[9], q[10], q[11]};
+  const V3 u = normalize(b - a), v = cross(w, u);
+  const V3 ap = p - a;
+  const float px = dot(ap, u), py = dot(ap, v);
+  const int n = (int)q[12];
+  const float* P = q + 13;
+  for (int i = 0, j = 1; i < n; ++i, j = (j + 1) % n) {  // LineSegment2F.contains on every edge
+    const float ax = P[2 * i], ay = P[2 * i + 1], bx = P[2 * j], by = P[2 * j + 1];
+    const float dx = px - ax, dy = py - ay, ex = bx - ax, ey = by - ay;
+    if (dx * ey - dy * ex != 0.0f) continue;
+    if (std::fabs(ex) >= std::fabs(ey) ? (ex > 0.0f ? ax <= px && px <= bx : bx <= px && px <= ax)
+                                       : (ey > 0.0f ? ay <= py && py <= by : by <= py && py <= ay))
+      return true;
+  }
+  bool inside = false;  // Polygon2F.doContains (crossing test)
+  for (int i = 0, j = n - 1; i < n; j = i++) {
+    const float ix = P[2 * i], iy = P[2 * i + 1], jx = P[2 * j], jy = P[2 * j + 1];
+    if ((iy > py) != (jy > py) && px < (jx - ix) * (py - iy) / (jy - iy) + ix) inside = !inside;
+  }
+  return inside;
+}
+inline float polygon_t(const float* q, const Ray& r, float tmin, float tmax) {  // Polygon3F.java:321
+  const V3 n = {q[9], q[10], q[11]}, a = {q[0], q[1], q[2]};
+  const float dp = dot(n, r.d);
+  if (dp == 0.0f) return NAN;
+  const float t = dot(a - r.o, n) / dp;
+  if (t > tmin && t < tmax && polygon_contains(q, point_at(r, t))) return t;
+  return NAN;
+}
+inline Surface polygon_surface(const float* q, const Ray& r, float t) {  // Polygon3F.doCreateSurfaceIntersection
+  const V3 p = point_at(r, t);
+  const V3 n = {q[9], q[10], q[11]};
+  const V3 na = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
+  const bool isx = na.x > na.y && na.x > na.z, isy = na.y > na.z;
+  auto proj = [&](const float* c) { return isx ? std::make_pair(c[1], c[2]) : isy ? std::make_pair(c[2], c[0]) : std::make_pair(c[0], c[1]); };
+  const auto A = proj(q), B = proj(q + 6), C = proj(q + 3);  // vB from the last point, vC from the second (doCreateTextureCoordinates)
+  const float abx = B.first - A.first, aby = B.second - A.second, acx = C.first - A.first, acy = C.second - A.second;
+  const float dr = 1.0f / (abx * acy - aby * acx);
+  const float hu = isx ? p.y : isy ? p.z : p.x, hv = isx ? p.z : isy ? p.x : p.y;
+  const float tu = hu * (-aby * dr) + hv * (abx * dr) + (A.first * aby - A.second * abx) * dr;
+  const float tv = hu * (acy * dr) + hv * (-acx * dr) + (acx * A.second - acy * A.first) * dr;
+  return simple_surface(r, t, p, onb_from_w(n), tu, tv);
+}
+
 // Shape3F.intersectionT dispatch (object space).  aux receives the mesh's
 // winning triangle offset.
 inline float shape_t(const Scene& sc, int sid, int soff, const Ray& r, float tmin, float tmax, int* aux) {
@@ -660,6 +708,7 @@ inline float shape_t(const Scene& sc, int sid, int soff, const Ray& r, float tmi
     case kShapeHyperboloid: return hyperboloid_t(sc.F("shape3FHyperboloid3FArray").data() + soff, r, tmin, tmax);
     case kShapeCuboid: return cuboid_t(sc.F("shape3FRectangularCuboid3FArray").data() + soff, r, tmin, tmax);
     case kShapeTorus: return torus_t(sc.F("shape3FTorus3FArray").data() + soff, r, tmin, tmax);
+    case kShapePolygon: return polygon_t(sc.F("shape3FPolygon3FArray").data() + soff, r, tmin, tmax);
     default: return NAN;
   }
 }
@@ -701,6 +750,7 @@ inline bool shape_surface(const Scene& sc, int sid, int soff, const Ray& r, floa
     DFO_SIMPLE_SHAPE(kShapeHyperboloid, "shape3FHyperboloid3FArray", hyperboloid_t, hyperboloid_surface)
     DFO_SIMPLE_SHAPE(kShapeCuboid, "shape3FRectangularCuboid3FArray", cuboid_t, cuboid_surface)
     DFO_SIMPLE_SHAPE(kShapeTorus, "shape3FTorus3FArray", torus_t, torus_surface)
+    DFO_SIMPLE_SHAPE(kShapePolygon, "shape3FPolygon3FArray", polygon_t, polygon_surface)
 #undef DFO_SIMPLE_SHAPE
     default: return false;
   }
@@ -2228,6 +2278,12 @@ int dfo_scene_commit(void* s, int layout) {
     const int sid = sc->prims[p * 8 + 6], soff = sc->prims[p * 8 + 7];
     for (const auto& rc : recs)
       if (rc.id == sid && (soff < 0 || (size_t)soff + rc.len > sc->F(rc.arr).size())) return -4;
+    if (sid == kShapePolygon) {  // variable length: 13 + 2 * count floats
+      const auto& A = sc->F("shape3FPolygon3FArray");
+      if (soff < 0 || (size_t)soff + 13 > A.size()) return -4;
+      const float cnt = A[soff + 12];
+      if (!(cnt >= 3.0f) || (size_t)soff + 13 + 2 * (size_t)cnt > A.size()) return -4;
+    }
   }
   sc->lights = sc->I("lightIDAndOffsetArray");
   const auto& cam = sc->F("cameraArray");

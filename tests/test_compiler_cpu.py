@@ -117,7 +117,7 @@ def test_oracle_render_counts_and_guard(oracle):
 
 
 def test_record_shapes_layout_and_oracle():
-    """Disk ... torus compile into their reference records (CompiledShape3FCache.to*3F)
+    """Disk ... torus and polygons compile into their reference records (CompiledShape3FCache.to*3F)
     and every one of them is hit by the oracle's primary rays."""
     import numpy as np
 
@@ -140,8 +140,11 @@ def test_record_shapes_layout_and_oracle():
     res = o.render(3, spp=1, threads=4)
     hit = set(res["prim"].ravel().tolist())
     record_prims = [i for i, p in enumerate(prims) if p[6] in (M.SHAPE_DISK, M.SHAPE_CYLINDER, M.SHAPE_CONE, M.SHAPE_PARABOLOID,
-                                                             M.SHAPE_HYPERBOLOID, M.SHAPE_CUBOID, M.SHAPE_TORUS)]
-    assert len(record_prims) == 9
+                                                             M.SHAPE_HYPERBOLOID, M.SHAPE_CUBOID, M.SHAPE_TORUS, M.SHAPE_POLYGON)]
+    assert len(record_prims) == 11
+    pg = a["shape3FPolygon3FArray"]
+    assert pg[12] == 5 and pg.size % 8 == 0  # 13 + 2 * 5 floats padded to 24, then the hexagon
+    assert pg[24 + 12] == 6
     assert set(record_prims) <= hit
 
 
