@@ -106,3 +106,18 @@ def test_ray_tracing_sigma(scene_name, request):
     ok, mg, mo = PT.sigma_test(g, o)
     assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
     assert abs(mg.mean() - mo.mean()) <= 0.02 * max(mo.mean(), 1e-3) + 1e-4
+
+
+@pytest.mark.parametrize("scene_name", ["cornell", "disney"])
+def test_path_tracing_rmse_against_converged(scene_name, request):
+    # PATH_TRACING criterion: at equal spp (16), the RMSE against a converged
+    # 16,384-spp image is within 2% of the CPU oracle's RMSE.  The converged
+    # image is rendered on the device with an independent seed.
+    cs = request.getfixturevalue(scene_name)
+    conv = PT.render_gpu(cs, RA.PATH_TRACING, spp=16384, max_bounce=8, seed=0xC0FFEE)
+    ref = conv["sum"] / np.maximum(conv["count"], 1)[..., None]
+    g = PT.render_gpu(cs, RA.PATH_TRACING, spp=16, max_bounce=8)
+    o = PT.render_oracle(cs, RA.PATH_TRACING, spp=16, max_bounce=8)
+    rmse_g = float(np.sqrt(np.mean((g["sum"] / np.maximum(g["count"], 1)[..., None] - ref) ** 2)))
+    rmse_o = float(np.sqrt(np.mean((o["sum"] / np.maximum(o["count"], 1)[..., None] - ref) ** 2)))
+    assert abs(rmse_g - rmse_o) <= 0.02 * rmse_o, "RMSE device %.5f oracle %.5f" % (rmse_g, rmse_o)
