@@ -41,6 +41,8 @@ SIGNATURES = [
     ("dfc_update_matrices", _c_int, [_c_p, _c_p, _c_i64]),
     ("dfc_read_image_rgba8", _c_int, [_c_p, _c_p, _c_i64]),
     ("dfc_read_film", _c_int, [_c_p, _c_p, _c_i64]),
+    ("dfc_set_film_filter", _c_int, [_c_p, _c_int]),
+    ("dfc_read_pixel_film", _c_int, [_c_p, _c_p, _c_i64]),
     ("dfc_read_primary_hits", _c_int, [_c_p, _c_p, _c_p, _c_i64]),
     ("dfc_read_counters", _c_int, [_c_p, _c_p]),
     ("dfc_read_stage_times", _c_int, [_c_p, _c_p]),

@@ -46,6 +46,8 @@ struct dfc_renderer {
   unsigned pixels = 0, paths = 0;
   int steps = 0;
   DevBuf d_film_sum, d_film_sq, d_primary_prim, d_primary_t, d_rgba;
+  int film_filter = 0;   // 0: per-pixel box film; 1: the CPU renderer's Gaussian XYZ film (PixelImageF)
+  DevBuf d_film_consts;  // Gaussian film: filter table, sRGB -> XYZ, XYZ -> sRGB
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_overflow, d_ray_total;
   DevBuf d_sort_keys, d_sort_bins, d_sorted;
@@ -110,6 +112,38 @@ void collect_stages(dfc_renderer* r) {
   r->ev_marks.clear();
 }
 
+// The CPU renderer's film constants: the 16x16 table of GaussianFilter2F(2, 2, 2)
+// (filter/Filter2F.java:119, GaussianFilter2F.java:117) and the sRGB matrices of
+// ColorSpaceF (color/ColorSpaceF.java:85, derived from the primaries and white
+// point), laid out as k_resolve_rgba8 and film_splat read them.
+std::vector<float> pixel_film_constants() {
+  std::vector<float> c(kFilmTable * kFilmTable + 18);
+  auto gauss = [](float d) {
+    const float e = std::exp(-2.0f * 2.0f * 2.0f);
+    return std::fmax(0.0f, std::exp(-2.0f * d * d) - e);
+  };
+  for (int y = 0; y < kFilmTable; ++y)
+    for (int x = 0; x < kFilmTable; ++x)
+      c[y * kFilmTable + x] = gauss((x + 0.5f) * 2.0f * (1.0f / kFilmTable)) * gauss((y + 0.5f) * 2.0f * (1.0f / kFilmTable));
+  const float xR = 0.64f, yR = 0.33f, xG = 0.3f, yG = 0.6f, xB = 0.15f, yB = 0.06f, xW = 0.31271f, yW = 0.32902f;
+  const float zR = 1.0f - (xR + yR), zG = 1.0f - (xG + yG), zB = 1.0f - (xB + yB), zW = 1.0f - (xW + yW);
+  const float rX = (yG * zB) - (yB * zG), rY = (xB * zG) - (xG * zB), rZ = (xG * yB) - (xB * yG);
+  const float rW = ((rX * xW) + (rY * yW) + (rZ * zW)) / yW;
+  const float gX = (yB * zR) - (yR * zB), gY = (xR * zB) - (xB * zR), gZ = (xB * yR) - (xR * yB);
+  const float gW = ((gX * xW) + (gY * yW) + (gZ * zW)) / yW;
+  const float bX = (yR * zG) - (yG * zR), bY = (xG * zR) - (xR * zG), bZ = (xR * yG) - (xG * yR);
+  const float bW = ((bX * xW) + (bY * yW) + (bZ * zW)) / yW;
+  const float m[9] = {rX / rW, rY / rW, rZ / rW, gX / gW, gY / gW, gZ / gW, bX / bW, bY / bW, bZ / bW};  // XYZ -> RGB rows
+  const float a = m[0] * (m[4] * m[8] - m[7] * m[5]), b = m[1] * (m[3] * m[8] - m[6] * m[5]), cc = m[2] * (m[3] * m[7] - m[6] * m[4]);
+  const float sd = 1.0f / (a - b + cc);
+  const float inv[9] = {sd * (m[4] * m[8] - m[5] * m[7]), sd * (m[5] * m[6] - m[3] * m[8]), sd * (m[3] * m[7] - m[4] * m[6]),
+                        sd * (m[2] * m[7] - m[1] * m[8]), sd * (m[0] * m[8] - m[2] * m[6]), sd * (m[1] * m[6] - m[0] * m[7]),
+                        sd * (m[1] * m[5] - m[2] * m[4]), sd * (m[2] * m[3] - m[0] * m[5]), sd * (m[0] * m[4] - m[1] * m[3])};
+  std::memcpy(c.data() + kFilmTable * kFilmTable, inv, sizeof inv);  // RGB -> XYZ, column-major
+  std::memcpy(c.data() + kFilmTable * kFilmTable + 9, m, sizeof m);
+  return c;
+}
+
 int alloc_wavefront(dfc_renderer* r) {
   const unsigned W = (unsigned)r->width, H = (unsigned)r->height;
   r->pixels = W * H;
@@ -136,6 +170,11 @@ int alloc_wavefront(dfc_renderer* r) {
   DFC_CK(r->d_ray_total.ensure(16), "counters");
   DFC_CK(r->d_sort_keys.ensure(P), "sort");
   DFC_CK(r->d_sorted.ensure(P * 4), "sort");
+  if (r->film_filter == 1) {
+    const std::vector<float> c = pixel_film_constants();
+    DFC_CK(r->d_film_consts.ensure(c.size() * sizeof(float)), "film");
+    DFC_CK(cudaMemcpy(r->d_film_consts.p, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice), "film");
+  }
   return DFC_OK;
 }
 
@@ -156,6 +195,9 @@ int clear_film(dfc_renderer* r) {
 ShadeArgs shade_args(dfc_renderer* r, int step) {
   ShadeArgs a{};
   a.scene = r->scene.view;
+  a.pixel_film = r->film_filter == 1 ? r->d_film_consts.as<float>() : nullptr;
+  a.width = (unsigned)r->width;
+  a.height = (unsigned)r->height;
   a.paths = r->paths;
   a.pixels = r->pixels;
   a.max_bounce = r->max_bounce;
@@ -544,7 +586,11 @@ int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t cap) {
   std::lock_guard<std::mutex> lk(r->mu);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
   if (cap < (int64_t)r->pixels * 4) return fail(r, DFC_E_INVALID_ARG, "destination too small");
-  k_resolve_rgba8<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->d_film_sum.as<float4>(), (int)r->pixels, r->tone_mapper, 1.0f, r->d_rgba.as<uchar4>());
+  // the tone mapper applies to PATH_TRACING only; the other algorithms are gamma-encoded as they are
+  // (renderer/gpu/GPURenderer.java:108-110, :312-335)
+  const int tm = r->algorithm == DFC_PATH_TRACING ? r->tone_mapper : DFC_TONE_MAPPER_NONE;
+  k_resolve_rgba8<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->d_film_sum.as<float4>(), (int)r->pixels, tm, 1.0f, r->d_rgba.as<uchar4>(),
+                                                                  r->film_filter == 1 ? r->d_film_consts.as<float>() : nullptr);
   DFC_CK(cudaMemcpyAsync(dst, r->d_rgba.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
   DFC_CK(cudaStreamSynchronize(r->stream), "readback");
   return DFC_OK;
@@ -554,6 +600,7 @@ int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
   if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
   std::lock_guard<std::mutex> lk(r->mu);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
+  if (r->film_filter != 0) return fail(r, DFC_E_STATE, "the film is the Gaussian pixel film: read it with dfc_read_pixel_film");
   const size_t P = r->pixels;
   if (cap < (int64_t)P * 7) return fail(r, DFC_E_INVALID_ARG, "destination too small");
   std::vector<float> s(P * 4), q(P * 4);
@@ -565,6 +612,26 @@ int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
     dst[i * 7 + 3] = q[i * 4 + 0]; dst[i * 7 + 4] = q[i * 4 + 1]; dst[i * 7 + 5] = q[i * 4 + 2];
     dst[i * 7 + 6] = s[i * 4 + 3];
   }
+  return DFC_OK;
+}
+
+int dfc_set_film_filter(dfc_renderer* r, int filter) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (filter != 0 && filter != 1) return fail(r, DFC_E_INVALID_ARG, "film filter is 0 (box) or 1 (Gaussian pixel film)");
+  r->film_filter = filter;
+  r->set_up = false;  // a new film: call setup() again
+  return DFC_OK;
+}
+
+int dfc_read_pixel_film(dfc_renderer* r, float* dst, int64_t cap) {
+  if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
+  if (r->film_filter != 1) return fail(r, DFC_E_STATE, "the film is the box film: read it with dfc_read_film");
+  if (cap < (int64_t)r->pixels * 4) return fail(r, DFC_E_INVALID_ARG, "destination too small");
+  DFC_CK(cudaMemcpyAsync(dst, r->d_film_sum.p, (size_t)r->pixels * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+  DFC_CK(cudaStreamSynchronize(r->stream), "readback");
   return DFC_OK;
 }
 

@@ -564,7 +564,34 @@ DFC_D void film_add_to(float4* film_sum, float4* film_sq, unsigned pix, V3 L) {
   float* g = reinterpret_cast<float*>(film_sq + pix);
   atomicAdd(g + 0, L.x * L.x); atomicAdd(g + 1, L.y * L.y); atomicAdd(g + 2, L.z * L.z);
 }
-DFC_D void film_add(const ShadeArgs& a, unsigned pix, V3 L) { film_add_to(a.film_sum, a.film_sq, pix, L); }
+// image/PixelImageF.java:569 filmAddColorXYZ (GaussianFilter2F(2, 2, 2) table):
+// the sample at film position (x + jitter x, y + jitter y) adds its XYZ, weighted
+// by the filter table entry, and the weight to every pixel within radius 2.
+DFC_D void film_splat(const ShadeArgs& a, unsigned pix, uint32_t key, V3 L) {
+  if (!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z))) return;  // AbstractCPURenderer.java:231
+  if (luminance(L) < -1.0e-5f) return;
+  const float* T = a.pixel_film;
+  const float* m = T + kFilmTable * kFilmTable;  // column-major sRGB -> XYZ (ColorSpaceF)
+  const V3 X = {m[0] * L.x + m[3] * L.y + m[6] * L.z, m[1] * L.x + m[4] * L.y + m[7] * L.z, m[2] * L.x + m[5] * L.y + m[8] * L.z};
+  const unsigned W = a.width, H = a.height;
+  const float dx = (float)(pix % W) + rng_uniform(key, kDimPixelX) - 0.5f;
+  const float dy = (float)(pix / W) + rng_uniform(key, kDimPixelY) - 0.5f;
+  const int x0 = (int)fmaxf(ceilf(dx - 2.0f), 0.0f), x1 = (int)fminf(floorf(dx + 2.0f), (float)(W - 1));
+  const int y0 = (int)fmaxf(ceilf(dy - 2.0f), 0.0f), y1 = (int)fminf(floorf(dy + 2.0f), (float)(H - 1));
+  for (int fy = y0; fy <= y1; ++fy) {
+    const int oy = min((int)floorf(fabsf((fy - dy) * 0.5f * 16.0f)), kFilmTable - 1);
+    for (int fx = x0; fx <= x1; ++fx) {
+      const int ox = min((int)floorf(fabsf((fx - dx) * 0.5f * 16.0f)), kFilmTable - 1);
+      const float w = T[oy * kFilmTable + ox];
+      float* f = reinterpret_cast<float*>(a.film_sum + (size_t)fy * W + fx);
+      atomicAdd(f + 0, X.x * w); atomicAdd(f + 1, X.y * w); atomicAdd(f + 2, X.z * w); atomicAdd(f + 3, w);
+    }
+  }
+}
+DFC_D void film_add(const ShadeArgs& a, unsigned pix, uint32_t key, V3 L) {
+  if (a.pixel_film) film_splat(a, pix, key, L);
+  else film_add_to(a.film_sum, a.film_sq, pix, L);
+}
 
 // One shade step of the path tracer for every path on the work list.  In
 // the batch engine (kMulti) the scene, film and bounce limits come from the
@@ -757,7 +784,7 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
       if (last_step) { keep = false; spawn_shadow = spawn_mis = false; }
       if (!keep && !(flags & kNoSample)) {
         if constexpr (kMulti) film_add_to(J->film_sum, J->film_sq, meta.x, L);
-        else film_add(a, meta.x, L);
+        else film_add(a, meta.x, meta.y, L);
       }
       retire = kMulti && !keep;
       a.beta[p] = make_float4(beta.x, beta.y, beta.z, eta_scale);
@@ -863,7 +890,7 @@ __global__ void k_shade_primary(ShadeArgs a, int algorithm) {
       if (a.preview) L = {1, 1, 1};
       else if (algorithm == DFC_ALGO_RAY_CASTING) for (int k = 0; k < S.light_count; ++k) L = L + light_Le_miss(S, S.lights[k], ray_d);
       if (algorithm == DFC_ALGO_AO) { a.radiance[p] = make_float4(L.x, L.y, L.z, -1.0f); continue; }
-      film_add(a, meta.x, L);
+      film_add(a, meta.x, meta.y, L);
       continue;
     }
     const DPrim& pr = S.prims[hp];
@@ -872,11 +899,11 @@ __global__ void k_shade_primary(ShadeArgs a, int algorithm) {
     if (a.record_primary && p < a.pixels) { a.primary_prim[p] = hp; a.primary_t[p] = world_t(pr, ray_o, sf); }
     if (algorithm == DFC_ALGO_RAY_CASTING) {
       float c = fabsf(dot(sf.s.w, ray_d)) * 0.5f;
-      film_add(a, meta.x, V3{c, c, c});
+      film_add(a, meta.x, meta.y, V3{c, c, c});
     } else if (algorithm == DFC_ALGO_DEPTH) {
       V3 dd = sf.p - ray_o;
       float in = clampf(1.0f / (dot(dd, dd) * 0.5f), 0.0f, 1.0f);
-      film_add(a, meta.x, V3{in, in, in});
+      film_add(a, meta.x, meta.y, V3{in, in, in});
     } else {
       // AO: store the geometric basis' hit point and spawn samples into the AO ray pool
       a.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1011,7 +1038,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_ray_trace(ShadeArgs a, unsigned
         }
       }
     }
-    film_add(a, meta.x, L);
+    film_add(a, meta.x, key, L);
   }
   // rays traced by this block's threads, one atomic per warp
   for (int off = 16; off > 0; off >>= 1) nrays += __shfl_down_sync(0xffffffffu, nrays, off);
@@ -1033,25 +1060,43 @@ __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples) {
     v = v / kPi;
     L = {v, v, v};
   }
-  film_add(a, meta.x, L);
+  film_add(a, meta.x, meta.y, L);
 }
 
 // Film resolve: mean radiance -> tone mapper -> sRGB -> RGBA8
 // (renderer/gpu/AbstractImageKernel.java:1104-1160, 1189-1325).
-__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out) {
+__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out, const float* film_consts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= pixels) return;
   const float4 s = film_sum[i];
-  V3 c = s.w > 0.0f ? V3{s.x / s.w, s.y / s.w, s.z / s.w} : V3{0, 0, 0};
-  switch (tone_mapper) {
-    case 2: c = V3{c.x / (1.0f + c.x), c.y / (1.0f + c.y), c.z / (1.0f + c.z)}; break;  // Reinhard
-    case 0: {  // filmic ACES (Narkowicz fit)
-      auto f = [](float x) { return clampf((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f), 0.0f, 1.0f); };
-      c = V3{f(c.x), f(c.y), f(c.z)};
-      break;
+  V3 c;
+  if (film_consts) {  // PixelImageF.filmRender: XYZ -> RGB, multiplyAndSaturateNegative(1 / weight sum)
+    const float* m = film_consts + kFilmTable * kFilmTable + 9;
+    c = V3{m[0] * s.x + m[1] * s.y + m[2] * s.z, m[3] * s.x + m[4] * s.y + m[5] * s.z, m[6] * s.x + m[7] * s.y + m[8] * s.z};
+    if (s.w != 0.0f) {
+      const float r = 1.0f / s.w;
+      c = V3{fmaxf(c.x * r, 0.0f), fmaxf(c.y * r, 0.0f), fmaxf(c.z * r, 0.0f)};
     }
-    default: break;
+    tone_mapper = 1;  // no tone mapper on this film
+  } else {
+    c = s.w > 0.0f ? V3{s.x / s.w, s.y / s.w, s.z / s.w} : V3{0, 0, 0};
   }
+  // renderer/gpu/AbstractImageKernel.java:1189-1325 (exposure e)
+  auto tm = [&](float x) {
+    const float b = x * exposure;
+    switch (tone_mapper) {
+      case 0: {  // imageToneMapFilmicCurveACESModifiedVersion1: filmic curve (2.51, 0.03, 2.43, 0.59, 0.14)
+        const float v = fmaxf(b - 0.0f, -3.4028235e38f);
+        return clampf((v * (2.51f * v + 0.03f)) / (v * (2.43f * v + 0.59f) + 0.14f), 0.0f, 1.0f);
+      }
+      case 2: return b / (1.0f + b);                                     // imageToneMapReinhard
+      case 3: return b * (1.0f + b / (4.0f * 4.0f)) / (1.0f + b);         // ...ReinhardModifiedVersion1, L_white 4
+      case 4: return 1.0f - expf(-b * exposure);                          // ...ReinhardModifiedVersion2
+      case 5: return b / (b + 0.155f) * 1.019f;                           // imageToneMapUnreal3
+      default: return x;                                                  // NONE
+    }
+  };
+  c = V3{tm(c.x), tm(c.y), tm(c.z)};
   auto enc = [](float v) {
     v = clampf(v, 0.0f, 1.0f);
     // sRGB redo-gamma with the ColorSpaceF parameters (break point 0.00304, gamma 2.4)

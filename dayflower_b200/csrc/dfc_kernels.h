@@ -92,6 +92,10 @@ struct RaygenArgs {
 
 struct ShadeArgs {
   SceneView scene;
+  // PixelImageF film (Gaussian XYZ splat): filter table [0, 256) and sRGB -> XYZ
+  // matrix [256, 265); nullptr: the per-pixel box film (sum, sum of squares)
+  const float* pixel_film;
+  unsigned width, height;
   // batch engine only (see TraceArgs); retired slots go back on the free stack
   const SceneView* scenes;
   const DJob* jobs;
@@ -204,7 +208,12 @@ __global__ void k_trace_ao(AoArgs a);
 // sample walks the sample's specular reflection/transmission tree depth first.
 __global__ void k_ray_trace(ShadeArgs a, unsigned* overflow, unsigned long long* rays);
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);
-__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out);
+// film_consts: nullptr for the box film (mean, tone mapper, sRGB); else the
+// PixelImageF resolve (filmRender: XYZ -> RGB over the weight sum, negative
+// parts dropped, sRGB) with the XYZ -> sRGB matrix at film_consts[265, 274).
+__global__ void k_resolve_rgba8(const float4* film_sum, int pixels, int tone_mapper, float exposure, uchar4* out,
+                                const float* film_consts = nullptr);
+constexpr int kFilmTable = 16;  // Filter2F.TABLE_SIZE
 
 constexpr int kTraceThreads = 128;
 

@@ -120,6 +120,13 @@ class GPURenderer:
     def setToneMapper(self, v: int): self._check(self._lib.dfc_set_tone_mapper(self._h, int(v)))
     def setPreviewMode(self, v: bool): self._check(self._lib.dfc_set_preview_mode(self._h, 1 if v else 0))
     def setSeed(self, seed: int): self._check(self._lib.dfc_set_seed(self._h, int(seed) & 0xFFFFFFFF))
+
+    FILM_BOX, FILM_GAUSSIAN = 0, 1
+
+    def setFilmFilter(self, film: int):
+        """0: per-pixel box film (getFilm); 1: the CPU renderer's Gaussian XYZ film
+        (PixelImageF, getPixelFilm).  Takes effect at the next setup()."""
+        self._check(self._lib.dfc_set_film_filter(self._h, int(film)))
     def setStageTiming(self, on: bool): self._check(self._lib.dfc_set_stage_timing(self._h, 1 if on else 0))
 
     def setRenderingAlgorithm(self, algorithm):
@@ -199,6 +206,12 @@ class GPURenderer:
         out = np.empty((self._height, self._width, 7), dtype=np.float32)
         self._check(self._lib.dfc_read_film(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size))
         return out[..., 0:3], out[..., 3:6], out[..., 6]
+
+    def getPixelFilm(self) -> np.ndarray:
+        """The Gaussian XYZ film: per pixel X, Y, Z sums and the filter weight sum, (H, W, 4)."""
+        out = np.empty((self._height, self._width, 4), dtype=np.float32)
+        self._check(self._lib.dfc_read_pixel_film(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size))
+        return out
 
     def getRadiance(self) -> np.ndarray:
         s, _, n = self.getFilm()

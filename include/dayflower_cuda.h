@@ -143,6 +143,18 @@ int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t capacity_bytes);
  * squares (3 floats) and sample count (1 float), width*height*7 floats. */
 int dfc_read_film(dfc_renderer* r, float* dst, int64_t capacity_floats);
 
+/* Film of later setup() calls: 0 (default) the per-pixel box film read by
+ * dfc_read_film; 1 the CPU renderer's film (image/PixelImageF.java:569
+ * filmAddColorXYZ, GaussianFilter2F(2, 2, 2)): each sample is converted to XYZ
+ * and splatted, filter-weighted, to the pixels within radius 2 of its film
+ * position; dfc_read_image_rgba8 then resolves it as PixelImageF.filmRender
+ * (XYZ -> sRGB over the weight sum, sRGB gamma, no tone mapper). */
+int dfc_set_film_filter(dfc_renderer* r, int filter);
+
+/* The Gaussian pixel film: per pixel X, Y, Z sums and the filter weight sum,
+ * width*height*4 floats (film filter 1 only). */
+int dfc_read_pixel_film(dfc_renderer* r, float* dst, int64_t capacity_floats);
+
 /* Per-pixel primitive index hit by the first pass's primary ray (-1 on a miss)
  * and its world-space distance.  Either pointer may be NULL. */
 int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t capacity);

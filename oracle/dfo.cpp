@@ -2309,6 +2309,104 @@ typedef struct dfo_params {
 //   hit_prim  primitive index of the first sample's primary hit (-1 miss)
 //   hit_t     world-space t of the first sample's primary hit
 // Returns the number of rays traced, or a negative error.
+// One camera sample of pixel (x, y): AbstractCPURenderer.java:215-236 up to
+// the radiance (CPURenderer.java:20-37 dispatch).  Returns false when the
+// camera gives no ray.  *fx, *fy receive the film position x + jitter.
+static bool render_sample(const Scene& sc, const Params& P, int x, int y, int k, bool want_hit, V3* c, Hit* h, RayStats* st, bool* unsup,
+                          bool* rt_over, float* fx, float* fy) {
+  const size_t pix = (size_t)y * P.width + x;
+  uint32_t key = rng_path_key(P.seed, (uint32_t)pix, (uint32_t)(P.sample_base + k));
+  float jx = rng_uniform(key, kDimPixelX), jy = rng_uniform(key, kDimPixelY);
+  if (fx) *fx = (float)x + jx;
+  if (fy) *fy = (float)y + jy;
+  Ray r;
+  if (!primary_ray(sc.cam, (float)x, (float)y, jx, jy, rng_uniform(key, kDimLensU), rng_uniform(key, kDimLensV), &r)) return false;
+  switch (P.algo) {
+    case kAlgoAO: *c = radiance_ao(sc, r, P, key, st, h); break;
+    case kAlgoDepth: *c = radiance_depth(sc, r, P, st, h); break;
+    case kAlgoRayCast: *c = radiance_raycast(sc, r, P, st, h); break;
+    case kAlgoRayTrace: {
+      RtCtx C{key, 0, false};
+      *c = rt_node(sc, r, P, C, 0u, 0, st, unsup);
+      if (C.overflow) *rt_over = true;
+      if (want_hit) { RayStats dummy; scene_intersect(sc, r, kTMinimum, kTMaximum, h, &dummy); }
+      break;
+    }
+    case kAlgoPath: default: {
+      *c = radiance_path(sc, r, P, key, st, unsup);
+      if (want_hit) { RayStats dummy; scene_intersect(sc, r, kTMinimum, kTMaximum, h, &dummy); }
+      break;
+    }
+  }
+  return true;
+}
+
+float dfo_gaussian_filter(float x, float y, float rx, float ry, float falloff);
+
+// The CPU renderer's film (image/PixelImageF.java:569 filmAddColorXYZ with
+// GaussianFilter2F(2, 2, 2), the 16x16 table of filter/Filter2F.java:119):
+// every accepted sample converted to XYZ and added, filter-weighted, to the
+// pixels within the filter radius of its film position.  out: per pixel X, Y,
+// Z sums and the weight sum.  Samples are computed in parallel, then splatted
+// in row, column, sample order.
+long long dfo_render_pixel_film(void* s, const dfo_params* pp, float* xyzw, int threads) {
+  Scene* sc = (Scene*)s;
+  Params P;
+  std::memcpy(&P, pp, sizeof P);
+  if (P.width <= 0 || P.height <= 0 || P.spp < 0) return -1;
+  const int W = P.width, H = P.height, S = P.spp;
+  struct Smp { float fx, fy; V3 xyz; bool ok; };
+  std::vector<Smp> smp((size_t)W * H * S);
+  if (threads < 1) threads = 1;
+  std::atomic<int> next_row(0);
+  std::atomic<long long> rays(0);
+  std::atomic<int> bad(0);
+  auto work = [&]() {
+    RayStats st;
+    bool unsup = false, over = false;
+    for (;;) {
+      const int y = next_row.fetch_add(1);
+      if (y >= H) break;
+      for (int x = 0; x < W; ++x)
+        for (int k = 0; k < S; ++k) {
+          Smp& m = smp[((size_t)y * W + x) * S + k];
+          Hit h;
+          V3 c;
+          m.ok = render_sample(*sc, P, x, y, k, false, &c, &h, &st, &unsup, &over, &m.fx, &m.fy) &&
+                 std::isfinite(c.x) && std::isfinite(c.y) && std::isfinite(c.z) && luminance(c) >= -1.0e-5f;
+          if (m.ok) m.xyz = srgb().to_xyz(c);  // AbstractCPURenderer.java:231-233
+        }
+    }
+    rays += st.rays;
+    if (unsup || over) bad = 1;
+  };
+  std::vector<std::thread> pool;
+  for (int i = 0; i < threads; ++i) pool.emplace_back(work);
+  for (auto& t : pool) t.join();
+  if (bad.load()) return -2;
+  float table[16 * 16];
+  for (int ty = 0; ty < 16; ++ty)
+    for (int tx = 0; tx < 16; ++tx)
+      table[ty * 16 + tx] = dfo_gaussian_filter((tx + 0.5f) * 2.0f * (1.0f / 16.0f), (ty + 0.5f) * 2.0f * (1.0f / 16.0f), 2.0f, 2.0f, 2.0f);
+  std::memset(xyzw, 0, sizeof(float) * 4 * (size_t)W * H);
+  for (const Smp& m : smp) {
+    if (!m.ok) continue;
+    const float dx = m.fx - 0.5f, dy = m.fy - 0.5f;
+    const int x0 = (int)std::fmax(std::ceil(dx - 2.0f), 0.0f), x1 = (int)std::fmin(std::floor(dx + 2.0f), (float)(W - 1));
+    const int y0 = (int)std::fmax(std::ceil(dy - 2.0f), 0.0f), y1 = (int)std::fmin(std::floor(dy + 2.0f), (float)(H - 1));
+    for (int fy = y0; fy <= y1; ++fy) {
+      const int oy = std::min((int)std::floor(std::fabs((fy - dy) * 0.5f * 16.0f)), 15);
+      for (int fx = x0; fx <= x1; ++fx) {
+        const int ox = std::min((int)std::floor(std::fabs((fx - dx) * 0.5f * 16.0f)), 15);
+        const float w = table[oy * 16 + ox];
+        float* q = xyzw + ((size_t)fy * W + fx) * 4;
+        q[0] += m.xyz.x * w; q[1] += m.xyz.y * w; q[2] += m.xyz.z * w; q[3] += w;  // PixelF.addColorXYZ, sample weight 1
+      }
+    }
+  }
+  return rays.load();
+}
+
 long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq_rgb, int* count, int* hit_prim, float* hit_t, int threads) {
   Scene* sc = (Scene*)s;
   Params P;
@@ -2331,32 +2429,14 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
         V3 acc = {0, 0, 0}, acc2 = {0, 0, 0};
         int n = 0;
         for (int k = 0; k < P.spp; ++k) {
-          uint32_t key = rng_path_key(P.seed, (uint32_t)pix, (uint32_t)(P.sample_base + k));
-          float jx = rng_uniform(key, kDimPixelX), jy = rng_uniform(key, kDimPixelY);
-          Ray r;
-          if (!primary_ray(sc->cam, (float)x, (float)y, jx, jy, rng_uniform(key, kDimLensU), rng_uniform(key, kDimLensV), &r)) {
+          Hit h;
+          V3 c;
+          bool over = false;
+          if (!render_sample(*sc, P, x, y, k, k == 0 && (hit_prim || hit_t), &c, &h, &st, &unsup, &over, nullptr, nullptr)) {
             if (k == 0) { if (hit_prim) hit_prim[pix] = -1; if (hit_t) hit_t[pix] = NAN; }
             continue;
           }
-          Hit h;
-          V3 c;
-          switch (P.algo) {
-            case kAlgoAO: c = radiance_ao(*sc, r, P, key, &st, &h); break;
-            case kAlgoDepth: c = radiance_depth(*sc, r, P, &st, &h); break;
-            case kAlgoRayCast: c = radiance_raycast(*sc, r, P, &st, &h); break;
-            case kAlgoRayTrace: {
-              RtCtx C{key, 0, false};
-              c = rt_node(*sc, r, P, C, 0u, 0, &st, &unsup);
-              if (C.overflow) rt_overflow = 1;
-              if (k == 0 && (hit_prim || hit_t)) { RayStats dummy; scene_intersect(*sc, r, kTMinimum, kTMaximum, &h, &dummy); }
-              break;
-            }
-            case kAlgoPath: default: {
-              c = radiance_path(*sc, r, P, key, &st, &unsup);
-              if (k == 0 && (hit_prim || hit_t)) { RayStats dummy; scene_intersect(*sc, r, kTMinimum, kTMaximum, &h, &dummy); }
-              break;
-            }
-          }
+          if (over) rt_overflow = 1;
           if (k == 0) {
             if (hit_prim) hit_prim[pix] = h.prim;
             if (hit_t) hit_t[pix] = h.prim >= 0 ? h.w.t : NAN;

@@ -52,6 +52,8 @@ def lib() -> ctypes.CDLL:
         L.dfo_scene_commit.argtypes = [_c_p, _c_i]
         L.dfo_render.restype = ctypes.c_longlong
         L.dfo_render.argtypes = [_c_p, ctypes.POINTER(Params), _c_p, _c_p, _c_p, _c_p, _c_p, _c_i]
+        L.dfo_render_pixel_film.restype = ctypes.c_longlong
+        L.dfo_render_pixel_film.argtypes = [_c_p, ctypes.POINTER(Params), _c_p, _c_i]
         for n in ("dfo_plane_intersection", "dfo_sphere_intersection"):
             getattr(L, n).argtypes = [_c_p, _c_p, _c_f, _c_f, _c_p]
         L.dfo_sphere_intersection_t.restype = _c_f
@@ -129,3 +131,15 @@ class OracleScene:
         if rays < 0:
             raise RuntimeError("oracle render failed (%d): the scene uses features the oracle does not restate" % rays)
         return {"sum": s, "sumsq": q, "count": n, "prim": prim, "t": t, "rays": int(rays)}
+
+    def render_pixel_film(self, algorithm: int, spp: int = 1, sample_base: int = 0, max_bounce: int = 20, min_rr: int = 5,
+                          ao_samples: int = 10, ao_distance: float = 20.0, seed: int = 0x5EED1234, threads: int = 1):
+        """The CPU renderer's Gaussian XYZ film (PixelImageF): per pixel X, Y, Z sums and the filter weight sum, (H, W, 4)."""
+        W, H = self.width, self.height
+        p = Params(int(algorithm), W, H, int(spp), int(sample_base), int(max_bounce), int(min_rr), int(ao_samples),
+                   float(ao_distance), 0, int(seed) & 0xFFFFFFFF, 0, H)
+        out = np.zeros((H, W, 4), np.float32)
+        rays = lib().dfo_render_pixel_film(self._s, ctypes.byref(p), ptr(out), int(threads))
+        if rays < 0:
+            raise RuntimeError("oracle render failed (%d)" % rays)
+        return out
