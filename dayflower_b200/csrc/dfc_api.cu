@@ -304,7 +304,8 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
       a.work_list = so.sorted;
-      (r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)<<<shade_grid, 256, 0, r->stream>>>(a);
+      (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
+          <<<shade_grid, 256, 0, r->stream>>>(a);
       stage_end(r, ev);
       r->launches += 4;
     }

@@ -20,7 +20,8 @@ cudaError_t put(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
 size_t scene_device_bytes(const HostScene& hs) {
   return vbytes(hs.prims) + vbytes(hs.materials) + vbytes(hs.lights) + vbytes(hs.nodes) + vbytes(hs.tlas_items) +
          vbytes(hs.tlas_bound) + vbytes(hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded) + vbytes(hs.tri_pos) +
-         vbytes(hs.tri_attr) + vbytes(hs.rects) + vbytes(hs.shapes) + vbytes(hs.perez) + 19 * sizeof(float);
+         vbytes(hs.tri_attr) + vbytes(hs.rects) + vbytes(hs.shapes) + vbytes(hs.perez) + 19 * sizeof(float) +
+         vbytes(hs.textures) + vbytes(hs.texels) + vbytes(hs.modifiers) + vbytes(hs.composites) + vbytes(hs.texmats);
 }
 
 size_t DeviceScene::device_bytes() const { return scene_device_bytes(host); }
@@ -43,6 +44,11 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
   DFC_PUT(perez, hs.perez);
   const std::vector<float> cam(hs.camera, hs.camera + 19);
   DFC_PUT(camera, cam);
+  DFC_PUT(textures, hs.textures);
+  DFC_PUT(texels, hs.texels);
+  DFC_PUT(modifiers, hs.modifiers);
+  DFC_PUT(composites, hs.composites);
+  DFC_PUT(texmats, hs.texmats);
 #undef DFC_PUT
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
@@ -64,6 +70,11 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
   v.shapes = ds->shapes.as<float>();
   v.perez = ds->perez.as<float>();
   v.camera = ds->camera.as<float>();
+  v.textures = ds->textures.as<DTexture>();
+  v.texels = ds->texels.as<unsigned>();
+  v.modifiers = ds->modifiers.as<DModifier>();
+  v.composites = ds->composites.as<DComposite>();
+  v.texmats = ds->texmats.as<DTexMaterial>();
   ds->host = std::move(hs);
   return cudaSuccess;
 }

@@ -38,6 +38,7 @@ struct DevBuf {
 
 struct DeviceScene {
   DevBuf prims, mats, lights, nodes, tlas_items, tlas_bound, unbounded, tri_pos, tri_attr, rects, shapes, perez, camera;
+  DevBuf textures, texels, modifiers, composites, texmats;
   SceneView view{};
   HostScene host;  // decoded records kept for updates (camera, matrices) and sizes
   size_t device_bytes() const;

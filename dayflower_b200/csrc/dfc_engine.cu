@@ -59,7 +59,7 @@ struct SceneEntry {
   int caller_refs = 0;
   int job_refs = 0;  // queued or running jobs on this scene
   bool live = false;
-  bool records = false;
+  int variant = 0;  // kernel variant it needs: 0 plain, 1 record shapes, 2 materials evaluated per hit
   size_t bytes = 0;
 };
 
@@ -118,7 +118,7 @@ struct dfc_engine {
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_sort_keys, d_sort_bins, d_sorted, d_free_stack, d_slot_job, d_overflow;
   cudaGraphExec_t graph = nullptr;
-  bool graph_records = false;
+  int graph_variant = 0;
   // progress read-back (pinned), double-buffered
   BatchState* h_state[2] = {nullptr, nullptr};
   unsigned long long* h_done[2] = {nullptr, nullptr};
@@ -162,10 +162,12 @@ int ecuda(dfc_engine* e, cudaError_t c, const char* what) {
 
 size_t used_bytes(const dfc_engine* e) { return e->wave_bytes + e->scene_bytes + e->film_bytes; }
 
-bool any_records(const dfc_engine* e) {
+// The most general kernel variant a live scene needs (the captured graph serves every resident scene).
+int kernel_variant(const dfc_engine* e) {
+  int v = 0;
   for (const SceneEntry& s : e->scenes)
-    if (s.live && s.records) return true;
-  return false;
+    if (s.live) v = std::max(v, s.variant);
+  return v;
 }
 
 dfc_engine_config resolved(const dfc_engine* e, dfc_engine_config c) {
@@ -270,7 +272,7 @@ void iteration_args(dfc_engine* e, int b, BatchArgs* ba, TraceArgs* ta, SortArgs
 
 constexpr int kKernelsPerIteration = 6;
 
-void enqueue_iteration(dfc_engine* e, int b, bool records) {
+void enqueue_iteration(dfc_engine* e, int b, int variant) {
   BatchArgs ba;
   TraceArgs ta;
   SortArgs so;
@@ -280,20 +282,21 @@ void enqueue_iteration(dfc_engine* e, int b, bool records) {
   const int shade_grid = e->sm_count * c.shade_blocks_per_sm;
   k_batch_plan<<<1, 32, 0, e->stream>>>(ba);
   k_batch_regen<<<e->sm_count * 4, 256, 0, e->stream>>>(ba);
-  (records ? k_trace_batch_records : k_trace_batch)<<<e->sm_count * c.trace_blocks_per_sm, kTraceThreads, 0, e->stream>>>(ta);
+  (variant >= 1 ? k_trace_batch_records : k_trace_batch)<<<e->sm_count * c.trace_blocks_per_sm, kTraceThreads, 0, e->stream>>>(ta);
   k_sort_count_batch<<<shade_grid, 256, 0, e->stream>>>(so);
   k_sort_scatter<<<shade_grid, 256, 0, e->stream>>>(so);
-  (records ? k_shade_path_batch_records : k_shade_path_batch)<<<shade_grid, c.shade_threads, 0, e->stream>>>(sa);
+  (variant == 2 ? k_shade_path_batch_textured : variant == 1 ? k_shade_path_batch_records : k_shade_path_batch)
+      <<<shade_grid, c.shade_threads, 0, e->stream>>>(sa);
 }
 
 // Captures iterations_per_launch iterations (alternating parity) into the graph.
-int capture_graph(dfc_engine* e, bool records) {
+int capture_graph(dfc_engine* e, int variant) {
   if (e->graph) {
     cudaGraphExecDestroy(e->graph);
     e->graph = nullptr;
   }
   DFC_ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-  for (int it = 0; it < e->active.iterations_per_launch; ++it) enqueue_iteration(e, it & 1, records);
+  for (int it = 0; it < e->active.iterations_per_launch; ++it) enqueue_iteration(e, it & 1, variant);
   cudaGraph_t g = nullptr;
   cudaError_t c = cudaStreamEndCapture(e->stream, &g);
   if (c == cudaSuccess) c = cudaGetLastError();
@@ -304,7 +307,7 @@ int capture_graph(dfc_engine* e, bool records) {
   c = cudaGraphInstantiate(&e->graph, g, 0);
   cudaGraphDestroy(g);
   if (c != cudaSuccess) return ecuda(e, c, "graph instantiate");
-  e->graph_records = records;
+  e->graph_variant = variant;
   return DFC_OK;
 }
 
@@ -360,7 +363,7 @@ int build_wavefront(dfc_engine* e) {
   iteration_args(e, 0, &ba, &ta, &so, &sa);
   k_batch_init<<<e->sm_count * 4, 256, 0, e->stream>>>(ba);
   DFC_ECK(cudaGetLastError(), "wavefront init");
-  int rc = capture_graph(e, any_records(e));
+  int rc = capture_graph(e, kernel_variant(e));
   if (rc) return rc;
   e->built = true;
   return DFC_OK;
@@ -395,9 +398,9 @@ int service(dfc_engine* e, bool idle_device) {
     DFC_ECK(cudaMemcpyAsync(e->d_scene_table.p, table.data(), table.size() * sizeof(SceneView), cudaMemcpyHostToDevice, e->stream),
             "scene table");
     e->table_dirty = false;
-    const bool rec = any_records(e);
-    if (rec != e->graph_records) {
-      int rc = capture_graph(e, rec);
+    const int var = kernel_variant(e);
+    if (var != e->graph_variant) {
+      int rc = capture_graph(e, var);
       if (rc) return rc;
     }
   }
@@ -823,7 +826,7 @@ int dfc_engine_scene_commit(dfc_engine* e, int layout_version, int32_t* scene_id
   e->staged = Staged();
   if (rc != DFC_OK) return efail(e, rc, err);
   const size_t bytes = scene_device_bytes(hs);
-  const bool records = hs.record_shapes;
+  const int variant = hs.textured() ? 2 : hs.record_shapes ? 1 : 0;
   int slot = -1;
   {
     std::lock_guard<std::mutex> lk(e->mu);
@@ -847,7 +850,7 @@ int dfc_engine_scene_commit(dfc_engine* e, int layout_version, int32_t* scene_id
   s.caller_refs = 1;
   s.job_refs = 0;
   s.live = true;
-  s.records = records;
+  s.variant = variant;
   s.bytes = bytes;
   e->table_dirty = true;
   *scene_id = slot;

@@ -21,6 +21,7 @@
 #include <sstream>
 
 #include "dfc_bvh.h"
+#include "dfc_matderive.h"
 
 namespace dfc {
 namespace {
@@ -29,7 +30,7 @@ enum {
   kMatClearCoatId = 3, kMatDisneyId = 4, kMatGlassId = 7, kMatGlossyId = 8, kMatMatteId = 11, kMatMetalId = 12, kMatMirrorId = 13,
   kMatPlasticId = 14, kMatSubstrateId = 16, kMatTranslucentId = 18, kMatUberId = 19
 };
-enum { kTexConstantId = 4, kModNoOpId = 2 };
+enum { kTexConstantId = 4 };
 enum { kBVAabbId = 1, kBVSphereId = 2, kBVInfiniteId = 3 };
 
 // Runs f(begin, end) over [0, n) in contiguous chunks on the host's threads.
@@ -54,11 +55,6 @@ const std::vector<T>& get(const std::map<std::string, std::vector<T>>& m, const 
   static const std::vector<T> empty;
   auto it = m.find(name);
   return it == m.end() ? empty : it->second;
-}
-
-float roughness_to_alpha(float r) {  // scene/microfacet/MicrofacetDistribution.java:convertRoughnessToAlpha
-  float x = std::fmax(r, 1.0e-3f), y = std::log(x);
-  return 1.62142f + 0.819955f * y + 0.1734f * y * y + 0.0171201f * y * y * y + 0.000640711f * y * y * y * y;
 }
 
 struct Decoder {
@@ -102,213 +98,204 @@ struct Decoder {
     if (off < 0 || k + 3 > C.size()) throw Fail{DFC_E_INVALID_ARG, "constant texture offset out of range"};
     out[0] = C[k]; out[1] = C[k + 1]; out[2] = C[k + 2];
   }
-  float value(int id, int off) { float c[3]; color(id, off, c); return (c[0] + c[1] + c[2]) / 3.0f; }
-  void check_modifier(int id) {
-    if (id != kModNoOpId && id != 0) throw Fail{DFC_E_UNSUPPORTED, "modifier id " + std::to_string(id) + " is not supported"};
+
+  // ---- textures (renderer/gpu/AbstractTextureKernel.java:152-435, scene/texture/*.java getColor)
+  std::map<std::pair<int, int>, int> texture_index;
+  std::vector<int> texture_blend_depth;  // BlendTexture nesting below each node
+
+  static float jcos(float a) { return (float)std::cos((double)a); }  // utility/Floats.java cos, sin: Math in double
+  static float jsin(float a) { return (float)std::sin((double)a); }
+  static void unpack_argb(float f, float* out) {  // Color3F.unpack(ARGB) of a packed colour stored in a float
+    const int c = (int)f;
+    out[0] = (float)((c >> 16) & 0xFF) / 255.0f; out[1] = (float)((c >> 8) & 0xFF) / 255.0f; out[2] = (float)(c & 0xFF) / 255.0f;
+  }
+  const float* record(const char* name, size_t off, size_t len) {
+    const auto& A = F(name);
+    if (off + len > A.size()) throw Fail{DFC_E_INVALID_ARG, std::string(name) + ": record out of range"};
+    return A.data() + off;
+  }
+  // An LDR image record (angle, scale x, y, resolution x, y, ARGB pixels): its texels go to the pool.
+  void image(const char* name, const char* offsets, int rel, int* texel, int* rx, int* ry, float* p4) {
+    const auto& O = I(offsets);
+    if (rel < 0 || (size_t)rel >= O.size()) throw Fail{DFC_E_INVALID_ARG, std::string(offsets) + ": index out of range"};
+    const float* q = record(name, (size_t)O[rel], 5);
+    *rx = (int)q[3]; *ry = (int)q[4];
+    if (*rx <= 0 || *ry <= 0) throw Fail{DFC_E_INVALID_ARG, "image resolution must be positive"};
+    q = record(name, (size_t)O[rel], 5 + (size_t)*rx * (size_t)*ry);
+    *texel = (int)hs.texels.size();
+    for (size_t k = 0; k < (size_t)*rx * (size_t)*ry; ++k) hs.texels.push_back((unsigned)(int)q[5 + k]);
+    p4[0] = jcos(q[0]); p4[1] = jsin(q[0]); p4[2] = q[1]; p4[3] = q[2];
+  }
+  static void unpack16(float f, int* id, int* off) { const int v = (int)f; *id = (v >> 16) & 0xFFFF; *off = v & 0xFFFF; }
+
+  int texture_node(int id, int off, int depth) {
+    const auto key = std::make_pair(id, off);
+    auto it = texture_index.find(key);
+    if (it != texture_index.end()) return it->second;
+    if (depth > 64) throw Fail{DFC_E_UNSUPPORTED, "texture tree deeper than 64 (or cyclic)"};
+    DTexture t{};
+    t.kind = id; t.a = t.b = t.c = -1;
+    int blend = 0;
+    auto children = [&](float fa, float fb) {
+      int ia, oa, ib, ob;
+      unpack16(fa, &ia, &oa);
+      unpack16(fb, &ib, &ob);
+      t.a = texture_node(ia, oa, depth + 1);
+      t.b = texture_node(ib, ob, depth + 1);
+      blend = std::max(texture_blend_depth[t.a], texture_blend_depth[t.b]);
+    };
+    switch (id) {
+      case kTexConstant: color(id, off, t.p); break;
+      case kTexBlend: {
+        const float* q = record("textureBlendTextureArray", (size_t)off * 8, 8);
+        children(q[0], q[1]);
+        t.p[0] = q[2]; t.p[1] = q[3]; t.p[2] = q[4];
+        blend += 1;
+        break;
+      }
+      case kTexBullseye: {
+        const float* q = record("textureBullseyeTextureArray", (size_t)off * 8, 8);
+        children(q[3], q[4]);
+        t.p[0] = q[0]; t.p[1] = q[1]; t.p[2] = q[2]; t.p[3] = q[5];
+        break;
+      }
+      case kTexCheckerboard: case kTexPolkaDot: {
+        const float* q = record(id == kTexCheckerboard ? "textureCheckerboardTextureArray" : "texturePolkaDotTextureArray", (size_t)off * 8, 8);
+        children(q[2], q[3]);
+        t.p[0] = jcos(q[1]); t.p[1] = jsin(q[1]); t.p[2] = q[4]; t.p[3] = q[5];
+        break;
+      }
+      case kTexLDRImage:
+        image("textureLDRImageTextureArray", "textureLDRImageTextureOffsetArray", off, &t.c, &t.a, &t.b, t.p);
+        break;
+      case kTexMarble: {
+        const float* q = record("textureMarbleTextureArray", (size_t)off * 8, 8);
+        unpack_argb(q[0], t.p); unpack_argb(q[1], t.p + 3); unpack_argb(q[2], t.p + 6);
+        t.p[9] = q[3]; t.p[10] = q[4]; t.a = (int)q[6];
+        break;
+      }
+      case kTexSimplexFBM: {
+        const float* q = record("textureSimplexFractionalBrownianMotionTextureArray", (size_t)off * 4, 4);
+        unpack_argb(q[0], t.p);
+        t.p[3] = q[1]; t.p[4] = q[2]; t.a = (int)q[3];
+        break;
+      }
+      case kTexDotProduct: case kTexSurfaceNormal: case kTexUV: break;
+      default: {
+        std::ostringstream os;
+        os << "texture id " << id << " is not supported";
+        throw Fail{DFC_E_UNSUPPORTED, os.str()};
+      }
+    }
+    const int idx = (int)hs.textures.size();
+    hs.textures.push_back(t);
+    texture_blend_depth.push_back(blend);
+    texture_index[key] = idx;
+    return idx;
   }
 
-  int material(int mid, int moff) {
+  // ---- modifiers (renderer/gpu/AbstractModifierKernel.java:75, scene/modifier/*.java modify)
+  std::map<std::pair<int, int>, int> modifier_index;
+  int modifier(int id, int off) {
+    if (id == kModNoOp || id == 0) return -1;
+    const auto key = std::make_pair(id, off);
+    auto it = modifier_index.find(key);
+    if (it != modifier_index.end()) return it->second;
+    DModifier d{};
+    d.kind = id;
+    if (id == kModNormalMapLDRImage) {
+      image("modifierNormalMapLDRImageModifierArray", "modifierNormalMapLDRImageModifierOffsetArray", off, &d.texel, &d.rx, &d.ry, d.p);
+    } else if (id == kModSimplexNoiseNormalMap) {
+      const float* q = record("modifierSimplexNoiseNormalMapModifierArray", (size_t)off * 2, 2);
+      d.p[0] = q[0]; d.p[1] = q[1];
+    } else {
+      throw Fail{DFC_E_UNSUPPORTED, "modifier id " + std::to_string(id) + " is not supported"};
+    }
+    const int idx = (int)hs.modifiers.size();
+    hs.modifiers.push_back(d);
+    modifier_index[key] = idx;
+    return idx;
+  }
+
+  int material(int mid, int moff, int depth = 0) {
     auto key = std::make_pair(mid, moff);
     auto it = material_index.find(key);
     if (it != material_index.end()) return it->second;
-    DMaterial m;
-    std::memset(&m, 0, sizeof m);
-    int a, ao, b, bo;
-    const char* name = nullptr;
-    switch (mid) {
-      case kMatMatteId: name = "materialMatteMaterialArray"; break;
-      case kMatMirrorId: name = "materialMirrorMaterialArray"; break;
-      case kMatGlassId: name = "materialGlassMaterialArray"; break;
-      case kMatMetalId: name = "materialMetalMaterialArray"; break;
-      case kMatPlasticId: name = "materialPlasticMaterialArray"; break;
-      case kMatDisneyId: name = "materialDisneyMaterialArray"; break;
-      case kMatClearCoatId: name = "materialClearCoatMaterialArray"; break;
-      case kMatGlossyId: name = "materialGlossyMaterialArray"; break;
-      case kMatSubstrateId: name = "materialSubstrateMaterialArray"; break;
-      case kMatTranslucentId: name = "materialTranslucentMaterialArray"; break;
-      case kMatUberId: name = "materialUberMaterialArray"; break;
-      default: throw Fail{DFC_E_UNSUPPORTED, "material id " + std::to_string(mid) + " is not supported"};
-    }
-    const auto& A = I(name);
+    if (depth > 64) throw Fail{DFC_E_UNSUPPORTED, "composite materials nested deeper than 64 (or cyclic)"};
     if (moff < 0) throw Fail{DFC_E_INVALID_ARG, "negative material offset"};
-    texref(A, moff, 0, &a, &ao, &b, &bo);  // emission texture, modifier
-    color(a, ao, m.emission);
-    check_modifier(b);
-    auto sat0 = [](float* c) { for (int k = 0; k < 3; ++k) c[k] = std::fmax(c[k], 0.0f); };
-    auto black = [](const float* c) { return c[0] == 0.0f && c[1] == 0.0f && c[2] == 0.0f; };
-    switch (mid) {
-      case kMatMatteId: {  // scene/material/MatteMaterial.java:285
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        float ang = value(a, ao);
-        color(b, bo, m.c0); sat0(m.c0);
-        ang = std::fmin(std::fmax(ang, 0.0f), 90.0f) * (3.14159265358979323846f / 180.0f);
-        if (ang == 0.0f) m.kind = kMatLambert;
-        else { m.kind = kMatOrenNayar; float s2 = ang * ang; m.on_a = 1.0f - (s2 / (2.0f * (s2 + 0.33f))); m.on_b = 0.45f * s2 / (s2 + 0.09f); }
-        break;
+    DMaterial m{};
+    if (mid == kRefBullseye || mid == kRefCheckerboard || mid == kRefPolkaDot) {
+      // CompiledMaterialCache.java toBullseyeMaterial / toCheckerboardMaterial / toPolkaDotMaterial (absolute offsets)
+      const char* name = mid == kRefBullseye ? "materialBullseyeMaterialArray"
+                         : mid == kRefCheckerboard ? "materialCheckerboardMaterialArray" : "materialPolkaDotMaterialArray";
+      const float* q = record(name, (size_t)moff, 8);
+      DComposite c{};
+      c.kind = mid;
+      int ia, oa, ib, ob;
+      if (mid == kRefBullseye) {
+        unpack16(q[3], &ia, &oa); unpack16(q[4], &ib, &ob);
+        c.p[0] = q[0]; c.p[1] = q[1]; c.p[2] = q[2]; c.p[3] = q[5];
+      } else {
+        unpack16(q[2], &ia, &oa); unpack16(q[3], &ib, &ob);
+        c.p[0] = jcos(q[1]); c.p[1] = jsin(q[1]); c.p[2] = q[4]; c.p[3] = q[5];
       }
-      case kMatMirrorId: {  // MirrorMaterial.java:235
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c0); sat0(m.c0);
-        m.kind = black(m.c0) ? kMatNone : kMatMirror;
-        break;
+      c.a = material(ia, oa, depth + 1);
+      c.b = material(ib, ob, depth + 1);
+      m.kind = kMatComposite;
+      m.flags = (int)hs.composites.size();
+      hs.composites.push_back(c);
+    } else {
+      const char* name = nullptr;
+      switch (mid) {
+        case kMatMatteId: name = "materialMatteMaterialArray"; break;
+        case kMatMirrorId: name = "materialMirrorMaterialArray"; break;
+        case kMatGlassId: name = "materialGlassMaterialArray"; break;
+        case kMatMetalId: name = "materialMetalMaterialArray"; break;
+        case kMatPlasticId: name = "materialPlasticMaterialArray"; break;
+        case kMatDisneyId: name = "materialDisneyMaterialArray"; break;
+        case kMatClearCoatId: name = "materialClearCoatMaterialArray"; break;
+        case kMatGlossyId: name = "materialGlossyMaterialArray"; break;
+        case kMatSubstrateId: name = "materialSubstrateMaterialArray"; break;
+        case kMatTranslucentId: name = "materialTranslucentMaterialArray"; break;
+        case kMatUberId: name = "materialUberMaterialArray"; break;
+        default: throw Fail{DFC_E_UNSUPPORTED, "material id " + std::to_string(mid) + " is not supported"};
       }
-      case kMatGlassId: {  // GlassMaterial.java:501
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        m.eta = value(a, ao);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        color(a, ao, m.c0); sat0(m.c0); color(b, bo, m.c1); sat0(m.c1);
-        texref(A, moff, 3, &a, &ao, &b, &bo);
-        float ru = value(a, ao), rv = value(b, bo);
-        bool remap = plain(A, moff, 4) != 0;
-        m.has_kr = !black(m.c0); m.has_kt = !black(m.c1);
-        if (!m.has_kr && !m.has_kt) m.kind = kMatNone;
-        else if (ru == 0.0f && rv == 0.0f) m.kind = kMatGlassSpec;
-        else {
-          m.kind = kMatGlassRough;
-          m.ax = remap ? roughness_to_alpha(ru) : ru;
-          m.ay = remap ? roughness_to_alpha(rv) : rv;
+      const auto& A = I(name);
+      const MatShape sh = mat_shape(mid);
+      int ids[kTexPositions], offs[kTexPositions];
+      for (int slot = 0; slot < kTexPositions / 2; ++slot) {
+        const bool needed = ((sh.tex_mask >> (2 * slot)) & 3u) != 0 || slot == 0 || 2 * slot + 1 == sh.plain_pos;
+        if (needed) texref(A, moff, slot, &ids[2 * slot], &offs[2 * slot], &ids[2 * slot + 1], &offs[2 * slot + 1]);
+        else ids[2 * slot] = ids[2 * slot + 1] = offs[2 * slot] = offs[2 * slot + 1] = 0;
+      }
+      int plain_v = 0;
+      if (sh.plain_slot >= 0) plain_v = plain(A, moff, sh.plain_slot);
+      if (sh.plain_pos >= 0) plain_v = ids[sh.plain_pos];
+      const int mod = modifier(ids[1], offs[1]);
+      bool all_constant = mod < 0;
+      for (int p = 0; p < kTexPositions; ++p)
+        if (((sh.tex_mask >> p) & 1u) && ids[p] != kTexConstantId) all_constant = false;
+      if (all_constant) {
+        MatInputs in{};
+        for (int p = 0; p < kTexPositions; ++p)
+          if ((sh.tex_mask >> p) & 1u) color(ids[p], offs[p], in.c[p]);
+        in.plain = plain_v;
+        derive_material(mid, in, &m);
+      } else {
+        DTexMaterial tm{};
+        tm.ref_id = mid;
+        tm.modifier = mod;
+        tm.plain = plain_v;
+        for (int p = 0; p < kTexPositions; ++p) {
+          tm.tex[p] = -1;
+          if (!((sh.tex_mask >> p) & 1u)) continue;
+          tm.tex[p] = texture_node(ids[p], offs[p], 0);
+          if (texture_blend_depth[tm.tex[p]] > kMaxBlendDepth)
+            throw Fail{DFC_E_UNSUPPORTED, "BlendTexture nested deeper than " + std::to_string(kMaxBlendDepth)};
         }
-        break;
-      }
-      case kMatMetalId: {  // MetalMaterial.java:436
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c1); color(b, bo, m.c2);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        float ru = value(a, ao), rv = value(b, bo);
-        bool remap = plain(A, moff, 3) != 0;
-        m.ax = remap ? roughness_to_alpha(ru) : ru;
-        m.ay = remap ? roughness_to_alpha(rv) : rv;
-        m.kind = kMatMetal;
-        break;
-      }
-      case kMatPlasticId: {  // PlasticMaterial.java:389
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c0); sat0(m.c0); color(b, bo, m.c1); sat0(m.c1);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        float r = value(a, ao);
-        bool remap = plain(A, moff, 3) != 0;
-        m.ax = m.ay = remap ? roughness_to_alpha(r) : r;
-        m.has_kr = !black(m.c0); m.has_kt = !black(m.c1);
-        m.kind = (m.has_kr || m.has_kt) ? kMatPlastic : kMatNone;
-        break;
-      }
-      case kMatClearCoatId: {  // ClearCoatMaterial.java: kd, ks (the lobe is chosen per hit)
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c0); color(b, bo, m.c1);
-        m.kind = kMatClearCoat;
-        break;
-      }
-      case kMatGlossyId: {  // GlossyMaterial.java: TorranceSparrowBRDF(kr, ConductorFresnel(kr, 1, 1), TR(r, r))
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c0);
-        const float r = value(b, bo);
-        m.ax = m.ay = std::fmax(r, 0.001f);
-        // ConductorFresnel with etaI = kr, etaT = k = 1: relative eta and k are 1 / kr
-        for (int k = 0; k < 3; ++k) { m.c1[k] = 1.0f / m.c0[k]; m.c2[k] = 1.0f / m.c0[k]; }
-        m.kind = kMatGlossy;
-        break;
-      }
-      case kMatSubstrateId: {  // SubstrateMaterial.java: FresnelBlendBRDF(kd, ks, TR(ru, rv))
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, m.c0); sat0(m.c0); color(b, bo, m.c1); sat0(m.c1);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        const float ru = value(a, ao), rv = value(b, bo);
-        const bool remap = plain(A, moff, 3) != 0;
-        m.ax = std::fmax(remap ? roughness_to_alpha(ru) : ru, 0.001f);
-        m.ay = std::fmax(remap ? roughness_to_alpha(rv) : rv, 0.001f);
-        m.kind = (black(m.c0) && black(m.c1)) ? kMatNone : kMatSubstrate;
-        break;
-      }
-      case kMatTranslucentId: {  // TranslucentMaterial.java; flags: 1 Lambert BRDF, 2 Lambert BTDF, 4 TS BRDF, 8 TS BTDF
-        float kd[3], ks[3], rf[3], tr[3];
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, kd); sat0(kd); color(b, bo, ks); sat0(ks);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        color(a, ao, rf); sat0(rf); color(b, bo, tr); sat0(tr);
-        texref(A, moff, 3, &a, &ao, &b, &bo);  // roughness, (isRemappingRoughness, 0)
-        const float r = value(a, ao);
-        const float al = std::fmax(b != 0 ? roughness_to_alpha(r) : r, 0.001f);
-        m.flags = 0;
-        if (!black(rf) || !black(tr)) {
-          if (!black(kd)) m.flags |= (black(rf) ? 0 : 1) | (black(tr) ? 0 : 2);
-          if (!black(ks)) m.flags |= (black(rf) ? 0 : 4) | (black(tr) ? 0 : 8);
-        }
-        for (int k = 0; k < 3; ++k) { m.c0[k] = kd[k] * rf[k]; m.c1[k] = kd[k] * tr[k]; m.c2[k] = ks[k] * rf[k]; m.c3[k] = ks[k] * tr[k]; }
-        m.ax = m.ay = al;
-        m.kind = m.flags ? kMatTranslucent : kMatNone;  // no lobe: no BSDF, the ray passes through
-        break;
-      }
-      case kMatUberId: {  // UberMaterial.java; flags: 1 transparency BTDF, 2 Lambert, 4 TS BRDF, 8 specular BRDF, 16 specular BTDF
-        float kd[3], kr[3], ks[3], kt[3], op[3];
-        texref(A, moff, 1, &a, &ao, &b, &bo);
-        color(a, ao, kd); sat0(kd); color(b, bo, kr); sat0(kr);
-        texref(A, moff, 2, &a, &ao, &b, &bo);
-        color(a, ao, ks); sat0(ks); color(b, bo, kt); sat0(kt);
-        texref(A, moff, 3, &a, &ao, &b, &bo);
-        m.eta = value(a, ao);
-        color(b, bo, op); sat0(op);
-        texref(A, moff, 4, &a, &ao, &b, &bo);
-        const float ru = value(a, ao), rv = value(b, bo);
-        const bool remap = plain(A, moff, 5) != 0;
-        m.ax = std::fmax(remap ? roughness_to_alpha(ru) : ru, 0.001f);
-        m.ay = std::fmax(remap ? roughness_to_alpha(rv) : rv, 0.001f);
-        for (int k = 0; k < 3; ++k) {
-          m.c0[k] = op[k] * kd[k]; m.c1[k] = op[k] * ks[k]; m.c2[k] = op[k] * kr[k]; m.c3[k] = op[k] * kt[k];
-          m.c4[k] = std::fmax(1.0f - op[k], 0.0f);
-        }
-        m.flags = (black(m.c4) ? 0 : 1) | (black(m.c0) ? 0 : 2) | (black(m.c1) ? 0 : 4) | (black(m.c2) ? 0 : 8) | (black(m.c3) ? 0 : 16);
-        m.kind = kMatUber;
-        break;
-      }
-      case kMatDisneyId: {  // DisneyMaterial.java:1121-1210; record slots CompiledMaterialCache.java:2751-2759
-        int ida, offa, idb, offb;
-        auto f1 = [&](int slot, bool second) {
-          texref(A, moff, slot, &ida, &offa, &idb, &offb);
-          return second ? value(idb, offb) : value(ida, offa);
-        };
-        const float aniso = f1(1, false), cc = f1(2, false), ccg = f1(2, true);
-        texref(A, moff, 3, &ida, &offa, &idb, &offb);
-        float color[3];
-        this->color(ida, offa, color);
-        sat0(color);
-        const float dt = value(idb, offb) / 2.0f;
-        const float eta = f1(4, false), flat = f1(4, true), met = f1(5, false), rough = f1(5, true);
-        texref(A, moff, 6, &ida, &offa, &idb, &offb);
-        float sd[3];
-        this->color(ida, offa, sd);
-        const float sheen = value(idb, offb);
-        const float sheen_tint = f1(7, false), spec_tint = f1(7, true);
-        texref(A, moff, 8, &ida, &offa, &idb, &offb);
-        const float st = value(ida, offa);
-        const bool thin = idb != 0;  // second pair of slot 8: (isThin, 0)
-        auto lerp = [](float a, float b, float t) { return (1.0f - t) * a + t * b; };  // utility/Floats.java:591
-        const float lum = color[0] * 0.212671f + color[1] * 0.715160f + color[2] * 0.072169f;
-        float tint[3];
-        for (int k = 0; k < 3; ++k) tint[k] = lum > 0.0f ? color[k] / lum : 1.0f;
-        m.kind = kMatDisney;
-        m.flags = (thin ? kDisneyThin : 0) | (black(sd) ? 0 : kDisneyScatter) | (sheen > 0.0f ? kDisneyHasSheen : 0) |
-                  (cc > 0.0f ? kDisneyHasClearCoat : 0) | (st > 0.0f ? kDisneyHasTransmission : 0);
-        m.eta = eta;
-        m.d_rough = rough;
-        m.d_met = met;
-        m.d_dw = (1.0f - met) * (1.0f - st);
-        m.c2[0] = flat; m.c2[1] = dt; m.c2[2] = st;
-        const float r0 = ((eta - 1.0f) * (eta - 1.0f)) / ((eta + 1.0f) * (eta + 1.0f));
-        for (int k = 0; k < 3; ++k) {
-          m.c0[k] = color[k];
-          m.c1[k] = lerp(lerp(1.0f, tint[k], spec_tint) * r0, color[k], met);
-          m.c3[k] = sheen > 0.0f ? lerp(1.0f, tint[k], sheen_tint) * (m.d_dw * sheen) : 0.0f;
-          m.c4[k] = std::sqrt(color[k]) * st;
-        }
-        const float aspect = std::sqrt(1.0f - aniso * 0.9f);
-        m.ax = std::fmax(0.001f, rough * rough / aspect);
-        m.ay = std::fmax(0.001f, rough * rough * aspect);
-        const float rs = (0.65f * eta - 0.35f) * rough;
-        m.on_a = std::fmax(0.001f, rs * rs / aspect);
-        m.on_b = std::fmax(0.001f, rs * rs * aspect);
-        m.d_cc = cc;
-        m.d_gloss = lerp(0.1f, 0.001f, ccg);
-        break;
+        m.kind = kMatTextured;
+        m.flags = (int)hs.texmats.size();
+        hs.texmats.push_back(tm);
       }
     }
     int idx = (int)hs.materials.size();

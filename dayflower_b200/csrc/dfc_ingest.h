@@ -29,11 +29,18 @@ struct HostScene {
   std::vector<F4> tri_pos;
   std::vector<float> tri_attr, rects, perez;
   std::vector<float> shapes;  // pool of the record-sized shapes (disk ... torus), DPrim.data = float offset
+  std::vector<DTexture> textures;      // texture nodes of the kMatTextured materials
+  std::vector<unsigned> texels;        // their images (and normal-map modifier images), packed ARGB
+  std::vector<DModifier> modifiers;
+  std::vector<DComposite> composites;
+  std::vector<DTexMaterial> texmats;
   float camera[19] = {0};
   int tlas_root = -1;
   int lights_storage_pad = 0;  // 1 when `lights` holds only a placeholder
   int64_t triangles = 0;
   bool record_shapes = false;  // any disk, cylinder, cone, paraboloid, hyperboloid, cuboid or torus primitive
+  // Materials evaluated per hit (textures, modifiers, composite materials): the textured shading variants.
+  bool textured() const { return !texmats.empty() || !composites.empty(); }
 };
 
 // Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.  On

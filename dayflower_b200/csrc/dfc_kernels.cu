@@ -17,6 +17,7 @@
 #include "dfc_device.cuh"
 #include "dfc_kernels.h"
 #include "dfc_shapes.cuh"
+#include "dfc_texture.cuh"
 
 namespace dfc {
 
@@ -598,7 +599,7 @@ DFC_D void film_add(const ShadeArgs& a, unsigned pix, uint32_t key, V3 L) {
 // path's job, a path ends at its own step max_bounce + 3 (the step count of
 // a render pass of the per-job renderer), and a retired path's slot goes back
 // on the free stack.
-template <bool kRecords, bool kMulti>
+template <bool kRecords, bool kMulti, bool kTextured = false>
 __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
   const unsigned n = *a.work_count;
   const unsigned stride = gridDim.x * blockDim.x;
@@ -683,6 +684,8 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
             if (pr.light >= 0) {
               const DLight& lt = S.lights[pr.light];
               Le = (lt.two_sided || dot(sf.s.w, wo) > 0.0f) ? ld3(lt.radiance) : V3{0, 0, 0};
+            } else if constexpr (kTextured) {
+              Le = material_Le(S, pr, ray_d, sf);
             } else {
               Le = ld3(S.materials[pr.material].emission);
             }
@@ -692,8 +695,13 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
             alive = false;
           } else {
             const DMaterial& m = S.materials[pr.material];
+            const float u_mat = rng_uniform(key, bounce_dim(dimb, kDimMaterial));
             Bsdf B;
-            if (!build_bsdf(m, sf, ray_d, rng_uniform(key, bounce_dim(dimb, kDimMaterial)), &B)) {
+            bool built;
+            // textured and composite materials only occur in scenes shaded by the kTextured variants
+            if constexpr (kTextured) built = m.kind < kMatTextured ? build_bsdf(m, sf, ray_d, u_mat, &B) : textured_bsdf(S, pr, ray_d, u_mat, true, &sf, &B);
+            else built = build_bsdf(m, sf, ray_d, u_mat, &B);
+            if (!built) {
               // Scene.java:494: no BSDF, continue straight through without counting a bounce
               a.ray_o[p] = make_float4(sf.p.x, sf.p.y, sf.p.z, kTMin);
               a.ray_d[p] = make_float4(ray_d.x, ray_d.y, ray_d.z, kFltMax);
@@ -817,6 +825,8 @@ __global__ void k_shade_path(ShadeArgs a) { shade_path<false, false>(a); }
 __global__ void k_shade_path_records(ShadeArgs a) { shade_path<true, false>(a); }
 __global__ void k_shade_path_batch(ShadeArgs a) { shade_path<false, true>(a); }
 __global__ void k_shade_path_batch_records(ShadeArgs a) { shade_path<true, true>(a); }
+__global__ void k_shade_path_textured(ShadeArgs a) { shade_path<true, false, true>(a); }
+__global__ void k_shade_path_batch_textured(ShadeArgs a) { shade_path<true, true, true>(a); }
 
 // ---- material sort of the shade work list -----------------------------------
 // Shading diverges badly when one warp holds paths on different materials (each
@@ -993,7 +1003,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_ray_trace(ShadeArgs a, unsigned
       surface_of<true>(S, pr, h.aux, e.o, e.d, h.t_obj, &sf);
       if (rec && e.nid == 0u) { a.primary_prim[p] = h.prim; a.primary_t[p] = world_t(pr, e.o, sf); }
       Bsdf B;
-      if (!build_bsdf(S.materials[pr.material], sf, e.d, rng_uniform(nk, 4), &B, false)) {
+      const DMaterial& m = S.materials[pr.material];
+      if (m.kind < kMatTextured ? !build_bsdf(m, sf, e.d, rng_uniform(nk, 4), &B, false)
+                                : !textured_bsdf(S, pr, e.d, rng_uniform(nk, 4), false, &sf, &B)) {
         if (sp < kRtStack) st[sp++] = RtEntry{sf.p, e.d, e.w, e.bounce, e.nid * 3u + 3u};
         else atomicAdd(overflow, 1u);
         continue;
@@ -1004,7 +1016,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_ray_trace(ShadeArgs a, unsigned
         const DLight& lt = S.lights[pr.light];
         Ln = (lt.two_sided || dot(n, wo) > 0.0f) ? ld3(lt.radiance) : V3{0, 0, 0};
       } else {
-        Ln = ld3(S.materials[pr.material].emission);
+        Ln = material_Le(S, pr, e.d, sf);  // after the BSDF, as Scene.doRadianceRayTracer: on the modified hit
       }
       for (int k = 0; k < S.light_count; ++k) {
         const DLight& lt = S.lights[k];

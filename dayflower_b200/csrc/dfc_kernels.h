@@ -202,6 +202,9 @@ __global__ void k_shade_path(ShadeArgs a);
 __global__ void k_shade_path_records(ShadeArgs a);  // with the disk ... torus surfaces
 __global__ void k_shade_path_batch(ShadeArgs a);     // batch engine: scene, film and limits per path from the job table
 __global__ void k_shade_path_batch_records(ShadeArgs a);
+// with record shapes and materials evaluated per hit (textures, modifiers, composite materials)
+__global__ void k_shade_path_textured(ShadeArgs a);
+__global__ void k_shade_path_batch_textured(ShadeArgs a);
 __global__ void k_shade_primary(ShadeArgs a, int algorithm);
 __global__ void k_trace_ao(AoArgs a);
 // RAY_TRACING (scene/Scene.java:786 doRadianceRayTracer): one thread per camera

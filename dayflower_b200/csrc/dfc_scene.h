@@ -49,8 +49,63 @@ enum : int {
   kMatSubstrate = 11,  // SubstrateMaterial (FresnelBlendBRDF)
   kMatTranslucent = 12,  // TranslucentMaterial
   kMatUber = 13,       // UberMaterial
-  kMatKinds = 14
+  kMatTextured = 14,   // a material with a non-constant texture or a modifier: DMaterial.flags indexes DTexMaterial
+  kMatComposite = 15,  // Bullseye/Checkerboard/PolkaDotMaterial: DMaterial.flags indexes DComposite
+  kMatKinds = 16
 };
+
+// Reference texture ids (scene/texture/*Texture.java ID); DTexture.kind.
+enum : int {
+  kTexBlend = 1, kTexBullseye = 2, kTexCheckerboard = 3, kTexConstant = 4, kTexDotProduct = 5, kTexLDRImage = 7,
+  kTexMarble = 8, kTexPolkaDot = 9, kTexSimplexFBM = 10, kTexSurfaceNormal = 11, kTexUV = 12
+};
+enum : int { kModNoOp = 2, kModNormalMapLDRImage = 3, kModSimplexNoiseNormalMap = 4 };  // DModifier.kind
+enum : int { kCompBullseye = 1, kCompCheckerboard = 2, kCompPolkaDot = 15 };           // DComposite.kind
+constexpr int kTexPositions = 18;  // texture positions of a material record: slot s texture A at 2s, B at 2s + 1
+constexpr int kMaxBlendDepth = 3;  // BlendTexture nesting the device evaluates (checked at ingest)
+
+// One node of a texture tree (CompiledTextureCache.java records, resolved):
+//   Constant      p[0..2] colour
+//   Blend         a, b children; p[0..2] per-channel t
+//   Bullseye      a, b; p[0..2] origin (object space), p[3] scale
+//   Checkerboard  a, b; p[0] cos, p[1] sin of the angle, p[2..3] scale
+//   PolkaDot      a, b; p[0] cos, p[1] sin, p[2] cell resolution, p[3] dot radius
+//   LDRImage      a, b resolution x, y; c first texel (SceneView.texels); p[0] cos, p[1] sin, p[2..3] scale
+//   Marble        a octaves; p[0..8] colours A, B, C; p[9] frequency, p[10] scale
+//   SimplexFBM    a octaves; p[0..2] colour; p[3] frequency, p[4] gain
+//   DotProduct, SurfaceNormal, UV: no parameters
+struct alignas(16) DTexture {
+  int kind, a, b, c;
+  float p[12];
+};
+static_assert(sizeof(DTexture) == 64, "DTexture layout");
+
+// A material modifier (scene/modifier): NormalMapLDRImage (texel, rx, ry; p cos, sin, scale x, y) or
+// SimplexNoiseNormalMap (p[0] frequency, p[1] scale).
+struct alignas(16) DModifier {
+  int kind, texel, rx, ry;
+  float p[4];
+};
+static_assert(sizeof(DModifier) == 32, "DModifier layout");
+
+// A composite material: a, b are DMaterial indices; Bullseye p[0..2] origin (object space), p[3] scale;
+// Checkerboard p[0] cos, p[1] sin, p[2..3] scale; PolkaDot p[0] cos, p[1] sin, p[2] cell resolution, p[3] radius.
+struct alignas(16) DComposite {
+  int kind, a, b, pad;
+  float p[4];
+};
+static_assert(sizeof(DComposite) == 32, "DComposite layout");
+
+// A material evaluated per hit: the reference material id, its modifier
+// (DModifier index, -1 for none), the plain int of its record (roughness
+// remapping, DisneyMaterial isThin) and one DTexture per texture position
+// (-1 where the record has none).
+struct alignas(16) DTexMaterial {
+  int ref_id, modifier, plain, pad;
+  int tex[kTexPositions];
+  int pad2[2];
+};
+static_assert(sizeof(DTexMaterial) == 96, "DTexMaterial layout");
 
 // DisneyMaterial flags (DMaterial.flags); TranslucentMaterial and UberMaterial
 // use DMaterial.flags as a bit set of the lobes they build (dfc_ingest.cpp).
@@ -139,6 +194,11 @@ struct SceneView {
   const float* shapes;          // disk, cylinder, cone, paraboloid, hyperboloid, cuboid and torus records
   const float* perez;           // sky pool: lightPerezLightArray, then lightImageLightArray
   const float* camera;          // 19 floats
+  const DTexture* textures;     // texture nodes of the per-hit materials
+  const unsigned* texels;       // packed ARGB pixels of LDRImageTexture and NormalMapLDRImageModifier images
+  const DModifier* modifiers;
+  const DComposite* composites;
+  const DTexMaterial* texmats;
 };
 
 }  // namespace dfc

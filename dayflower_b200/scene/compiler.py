@@ -22,6 +22,7 @@ indices (the device multiplies them by the structure length).
 from __future__ import annotations
 
 import ctypes
+import math
 from typing import Dict, List
 
 import numpy as np
@@ -38,15 +39,16 @@ ARRAY_NAMES_F32 = [
     "textureConstantTextureArray", "textureLDRImageTextureArray", "textureMarbleTextureArray",
     "texturePolkaDotTextureArray", "textureSimplexFractionalBrownianMotionTextureArray",
     "modifierNormalMapLDRImageModifierArray", "modifierSimplexNoiseNormalMapModifierArray",
+    "materialBullseyeMaterialArray", "materialCheckerboardMaterialArray", "materialPolkaDotMaterialArray",
     "lightDiffuseAreaLightArray", "lightDirectionalLightArray", "lightImageLightArray", "lightPerezLightArray",
     "lightPointLightArray", "lightSpotLightArray", "cameraArray", "primitiveMatrix44FArray",
 ]
 ARRAY_NAMES_I32 = [
     "shape3FTriangleMesh3FArray", "textureLDRImageTextureOffsetArray",
-    "materialBullseyeMaterialArray", "materialCheckerboardMaterialArray", "materialClearCoatMaterialArray",
+    "materialClearCoatMaterialArray",
     "materialDisneyMaterialArray", "materialGlassMaterialArray", "materialGlossyMaterialArray",
     "materialMatteMaterialArray", "materialMetalMaterialArray", "materialMirrorMaterialArray",
-    "materialPlasticMaterialArray", "materialPolkaDotMaterialArray", "materialSubstrateMaterialArray",
+    "materialPlasticMaterialArray", "materialSubstrateMaterialArray",
     "materialTranslucentMaterialArray", "materialUberMaterialArray",
     "modifierNormalMapLDRImageModifierOffsetArray", "lightIDAndOffsetArray", "lightImageLightOffsetArray",
     "lightPerezLightOffsetArray", "primitiveArray",
@@ -111,6 +113,36 @@ def _world_aabb(points_obj: np.ndarray, o2w: np.ndarray):
     return w.min(axis=0), w.max(axis=0)
 
 
+def _packf(a, b) -> float:
+    """A 16/16 packed reference stored in a float array (exact below 2^24)."""
+    return float(_pack16(a, b))
+
+
+def _argb(color) -> float:
+    """``Color3F.pack()`` (ARGB, alpha 255) stored in a float array.  The 8-bit
+    rounding (saturate, * 255, + 0.5, truncate) stands in for
+    ``org.macroing.java.lang.Ints.saturateAndScaleToInt``, whose source is not
+    part of the reference; every reader unpacks the stored value."""
+    c = [int(min(max(float(x), 0.0), 1.0) * 255.0 + 0.5) for x in np.broadcast_to(np.asarray(color, dtype=np.float64), (3,))]
+    return float(np.int32(np.uint32((255 << 24) | (c[0] << 16) | (c[1] << 8) | c[2])))
+
+
+def _rad(degrees) -> float:
+    return float(np.float32(float(np.float32(degrees)) * (math.pi / 180.0)))
+
+
+def _image_record(t) -> list:
+    """``CompiledTextureCache.toLDRImageTexture`` / ``CompiledModifierCache.toNormalMapLDRImageModifier``:
+    angle (radians), scale (2), resolution x, y, the packed ARGB pixels, zero padding to 8."""
+    img = np.asarray(t.image, dtype=np.uint32).reshape(-1)
+    if img.size != t.resolution_x * t.resolution_y:
+        raise ValueError("image size does not match its resolution")
+    px = img.view(np.int32).astype(np.float64)
+    head = [_rad(t.angle_deg), t.scale[0], t.scale[1], t.resolution_x, t.resolution_y]
+    n = 5 + img.size
+    return head + px.tolist() + [0.0] * ((8 - n % 8) % 8)
+
+
 # Shapes stored as one fixed-length record each (CompiledShape3FCache.java:90-310).
 _RECORD_SHAPES = {M.Disk: "shape3FDisk3FArray", M.Cylinder: "shape3FCylinder3FArray", M.Cone: "shape3FCone3FArray",
                   M.Paraboloid: "shape3FParaboloid3FArray", M.Hyperboloid: "shape3FHyperboloid3FArray",
@@ -134,8 +166,10 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
         sizes[name] += a.size
         return off
 
-    # ---- textures (ConstantTexture only), deduplicated by value
+    # ---- textures (CompiledTextureCache.java:1530-2144): records of the pattern
+    # textures hold their children as Ints.pack(id, relative offset) in a float
     tex_index: Dict[tuple, int] = {}
+    tex_objects: Dict[int, tuple] = {}
 
     def tex(color) -> int:
         c = tuple(float(np.float32(x)) for x in (np.broadcast_to(np.asarray(color, dtype=np.float32), (3,))))
@@ -143,6 +177,66 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
             tex_index[c] = sizes["textureConstantTextureArray"] // 4
             push("textureConstantTextureArray", [c[0], c[1], c[2], 0.0])
         return tex_index[c]
+
+    def texture(t) -> tuple:
+        """(texture id, relative offset) of a texture, a colour or a number."""
+        if not isinstance(t, M.Texture):
+            return (M.TEX_CONSTANT, tex(t))
+        key = id(t)
+        if key in tex_objects:
+            return tex_objects[key]
+        if isinstance(t, M.ConstantTexture):
+            ref = (M.TEX_CONSTANT, tex(t.color))
+        elif isinstance(t, (M.DotProductTexture, M.SurfaceNormalTexture, M.UVTexture)):
+            ref = (t.ID, 0)
+        elif isinstance(t, M.BlendTexture):
+            a, b = _packf(*texture(t.a)), _packf(*texture(t.b))
+            tt = np.broadcast_to(np.asarray(t.t, dtype=np.float32), (3,))
+            ref = (t.ID, push("textureBlendTextureArray", [a, b, tt[0], tt[1], tt[2], 0, 0, 0]) // 8)
+        elif isinstance(t, M.BullseyeTexture):
+            a, b = _packf(*texture(t.a)), _packf(*texture(t.b))
+            o = t.origin
+            ref = (t.ID, push("textureBullseyeTextureArray", [o[0], o[1], o[2], a, b, t.scale, 0, 0]) // 8)
+        elif isinstance(t, M.CheckerboardTexture):
+            a, b = _packf(*texture(t.a)), _packf(*texture(t.b))
+            rec = [t.angle_deg, _rad(t.angle_deg), a, b, t.scale[0], t.scale[1], 0, 0]
+            ref = (t.ID, push("textureCheckerboardTextureArray", rec) // 8)
+        elif isinstance(t, M.PolkaDotTexture):
+            a, b = _packf(*texture(t.a)), _packf(*texture(t.b))
+            rec = [t.angle_deg, _rad(t.angle_deg), a, b, t.cell_resolution, t.radius, 0, 0]
+            ref = (t.ID, push("texturePolkaDotTextureArray", rec) // 8)
+        elif isinstance(t, M.MarbleTexture):
+            rec = [_argb(t.color_a), _argb(t.color_b), _argb(t.color_c), t.frequency, t.scale, t.stripes, t.octaves, 0]
+            ref = (t.ID, push("textureMarbleTextureArray", rec) // 8)
+        elif isinstance(t, M.SimplexFBMTexture):
+            rec = [_argb(t.color), t.frequency, t.gain, t.octaves]
+            ref = (t.ID, push("textureSimplexFractionalBrownianMotionTextureArray", rec) // 4)
+        elif isinstance(t, M.LDRImageTexture):
+            off = push("textureLDRImageTextureArray", _image_record(t))
+            ref = (t.ID, sizes["textureLDRImageTextureOffsetArray"])
+            push("textureLDRImageTextureOffsetArray", [off])
+        else:
+            raise ValueError("unsupported texture %r" % type(t).__name__)
+        tex_objects[key] = ref
+        return ref
+
+    mod_objects: Dict[int, tuple] = {}
+
+    def modifier(m) -> tuple:
+        """(modifier id, relative offset) (CompiledModifierCache.java:445-530)."""
+        if m is None or isinstance(m, M.NoOpModifier):
+            return (M.MOD_NOOP, 0)
+        key = id(m)
+        if key not in mod_objects:
+            if isinstance(m, M.NormalMapLDRImageModifier):
+                off = push("modifierNormalMapLDRImageModifierArray", _image_record(m))
+                mod_objects[key] = (m.ID, sizes["modifierNormalMapLDRImageModifierOffsetArray"])
+                push("modifierNormalMapLDRImageModifierOffsetArray", [off])
+            elif isinstance(m, M.SimplexNoiseNormalMapModifier):
+                mod_objects[key] = (m.ID, push("modifierSimplexNoiseNormalMapModifierArray", [m.frequency, m.scale]) // 2)
+            else:
+                raise ValueError("unsupported modifier %r" % type(m).__name__)
+        return mod_objects[key]
 
     def slot(a=(0, 0), b=(0, 0)):
         if layout_version == 2:
@@ -155,55 +249,68 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
     def pad_to(rec, length):
         return rec + [0] * (length * lanes - len(rec))
 
-    T = M.TEX_CONSTANT
-    noop = (M.MOD_NOOP, 0)
+    def ft(v):
+        """A float parameter: a texture, or a number as a grey constant texture."""
+        return texture(v if isinstance(v, M.Texture) else [v] * 3)
+
+    T = texture
     mat_offsets: Dict[int, tuple] = {}
+    composite_arrays = {M.BullseyeMaterial: "materialBullseyeMaterialArray",
+                        M.CheckerboardMaterial: "materialCheckerboardMaterialArray",
+                        M.PolkaDotMaterial: "materialPolkaDotMaterialArray"}
 
     def material(m: M.Material):
         key = id(m)
         if key in mat_offsets:
             return mat_offsets[key]
-        em = (T, tex(m.emission))
-        head = slot(em, noop)
+        if type(m) in composite_arrays:  # CompiledMaterialCache.java toBullseyeMaterial etc.: absolute offsets
+            if m.a is None or m.b is None:
+                raise ValueError("%s needs two materials" % type(m).__name__)
+            a, b = _packf(*material(m.a)), _packf(*material(m.b))
+            if isinstance(m, M.BullseyeMaterial):
+                o = m.origin
+                rec = [o[0], o[1], o[2], a, b, m.scale, 0, 0]
+            elif isinstance(m, M.CheckerboardMaterial):
+                rec = [m.angle_deg, _rad(m.angle_deg), a, b, m.scale[0], m.scale[1], 0, 0]
+            else:
+                rec = [m.angle_deg, _rad(m.angle_deg), a, b, m.cell_resolution, m.radius, 0, 0]
+            mat_offsets[key] = (m.ID, push(composite_arrays[type(m)], rec))
+            return mat_offsets[key]
+        head = slot(T(m.emission), modifier(m.modifier))
         if isinstance(m, M.Matte):
-            rec, name, length = head + slot((T, tex([m.angle] * 3)), (T, tex(m.kd))), "materialMatteMaterialArray", 2
+            rec, name, length = head + slot(ft(m.angle), T(m.kd)), "materialMatteMaterialArray", 2
         elif isinstance(m, M.Mirror):
-            rec, name, length = head + slot((T, tex(m.kr))), "materialMirrorMaterialArray", 2
+            rec, name, length = head + slot(T(m.kr)), "materialMirrorMaterialArray", 2
         elif isinstance(m, M.Glass):
-            rec = head + slot((T, tex([m.eta] * 3))) + slot((T, tex(m.kr)), (T, tex(m.kt))) + \
-                slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + plain(m.remap_roughness)
+            rec = head + slot(ft(m.eta)) + slot(T(m.kr), T(m.kt)) + \
+                slot(ft(m.roughness_u), ft(m.roughness_v)) + plain(m.remap_roughness)
             name, length = "materialGlassMaterialArray", 8
         elif isinstance(m, M.Metal):
-            rec = head + slot((T, tex(m.eta)), (T, tex(m.k))) + slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + \
-                plain(m.remap_roughness)
+            rec = head + slot(T(m.eta), T(m.k)) + slot(ft(m.roughness_u), ft(m.roughness_v)) + plain(m.remap_roughness)
             name, length = "materialMetalMaterialArray", 4
         elif isinstance(m, M.Plastic):
-            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness] * 3))) + plain(m.remap_roughness)
+            rec = head + slot(T(m.kd), T(m.ks)) + slot(ft(m.roughness)) + plain(m.remap_roughness)
             name, length = "materialPlasticMaterialArray", 4
         elif isinstance(m, M.ClearCoat):  # CompiledMaterialCache.java:2639-2646
-            rec, name, length = head + slot((T, tex(m.kd)), (T, tex(m.ks))), "materialClearCoatMaterialArray", 2
+            rec, name, length = head + slot(T(m.kd), T(m.ks)), "materialClearCoatMaterialArray", 2
         elif isinstance(m, M.Glossy):  # :2932-2939
-            rec, name, length = head + slot((T, tex(m.kr)), (T, tex([m.roughness] * 3))), "materialGlossyMaterialArray", 2
+            rec, name, length = head + slot(T(m.kr), ft(m.roughness)), "materialGlossyMaterialArray", 2
         elif isinstance(m, M.Substrate):  # :3373-3383
-            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + \
-                plain(m.remap_roughness)
+            rec = head + slot(T(m.kd), T(m.ks)) + slot(ft(m.roughness_u), ft(m.roughness_v)) + plain(m.remap_roughness)
             name, length = "materialSubstrateMaterialArray", 4
         elif isinstance(m, M.Translucent):  # :3466-3477
-            rec = head + slot((T, tex(m.kd)), (T, tex(m.ks))) + slot((T, tex(m.reflectance)), (T, tex(m.transmittance))) + \
-                slot((T, tex([m.roughness] * 3)), (1 if m.remap_roughness else 0, 0))
+            rec = head + slot(T(m.kd), T(m.ks)) + slot(T(m.reflectance), T(m.transmittance)) + \
+                slot(ft(m.roughness), (1 if m.remap_roughness else 0, 0))
             name, length = "materialTranslucentMaterialArray", 4
         elif isinstance(m, M.Uber):  # :3563-3577
-            rec = head + slot((T, tex(m.kd)), (T, tex(m.kr))) + slot((T, tex(m.ks)), (T, tex(m.kt))) + \
-                slot((T, tex([m.eta] * 3)), (T, tex(m.opacity))) + \
-                slot((T, tex([m.roughness_u] * 3)), (T, tex([m.roughness_v] * 3))) + plain(m.remap_roughness)
+            rec = head + slot(T(m.kd), T(m.kr)) + slot(T(m.ks), T(m.kt)) + slot(ft(m.eta), T(m.opacity)) + \
+                slot(ft(m.roughness_u), ft(m.roughness_v)) + plain(m.remap_roughness)
             name, length = "materialUberMaterialArray", 8
         elif isinstance(m, M.Disney):
             # CompiledMaterialCache.toDisneyMaterial (:2717-2760): nine packed slots of a 16-slot record
-            def ft(v):
-                return (T, tex([v] * 3))
             rec = head + slot(ft(m.anisotropic)) + slot(ft(m.clear_coat), ft(m.clear_coat_gloss)) + \
-                slot((T, tex(m.color)), ft(m.diffuse_transmission)) + slot(ft(m.eta), ft(m.flatness)) + \
-                slot(ft(m.metallic), ft(m.roughness)) + slot((T, tex(m.scatter_distance)), ft(m.sheen)) + \
+                slot(T(m.color), ft(m.diffuse_transmission)) + slot(ft(m.eta), ft(m.flatness)) + \
+                slot(ft(m.metallic), ft(m.roughness)) + slot(T(m.scatter_distance), ft(m.sheen)) + \
                 slot(ft(m.sheen_tint), ft(m.specular_tint)) + slot(ft(m.specular_transmission), (1 if m.thin else 0, 0))
             name, length = "materialDisneyMaterialArray", 16
         else:
@@ -324,5 +431,5 @@ def compile_scene(scene: M.Scene, layout_version: int = 1, resolution=None) -> C
     for k, parts in i32.items():
         arrays[k] = np.concatenate(parts).astype(np.int32) if parts else np.zeros(0, dtype=np.int32)
     stats = {"primitives": len(scene.primitives), "lights": len(scene.lights),
-             "triangles": sizes["shape3FTriangle3FArray"] // 24, "textures": len(tex_index), "meshes": len(mesh_jobs)}
+             "triangles": sizes["shape3FTriangle3FArray"] // 24, "textures": len(tex_index) + len(tex_objects), "meshes": len(mesh_jobs)}
     return CompiledScene(arrays, layout_version, stats)

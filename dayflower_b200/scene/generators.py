@@ -393,6 +393,78 @@ def quadrics_scene(resolution=(128, 96), with_lights=True) -> M.Scene:
     return sc
 
 
+def ldr_image(width: int, height: int, seed: int) -> np.ndarray:
+    """A seeded packed-ARGB image (alpha 255): smooth colour gradients plus blocks of noise."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:height, 0:width]
+    r = (x * 255 // max(width - 1, 1)).astype(np.uint32)
+    g = (y * 255 // max(height - 1, 1)).astype(np.uint32)
+    b = rng.integers(0, 256, size=(height, width), dtype=np.uint32)
+    return ((np.uint32(255) << 24) | (r << 16) | (g << 8) | b).reshape(-1).astype(np.uint32)
+
+
+def normal_map_image(width: int, height: int, seed: int) -> np.ndarray:
+    """A seeded tangent-space normal map: unit normals tilted up to ~35 degrees, packed ARGB."""
+    rng = np.random.default_rng(seed)
+    t = rng.normal(0.0, 0.35, size=(height * width, 2))
+    n = np.concatenate([t, np.ones((height * width, 1))], axis=1)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    c = np.clip(np.round((n + 1.0) * 0.5 * 255.0), 0, 255).astype(np.uint32)
+    return ((np.uint32(255) << 24) | (c[:, 0] << 16) | (c[:, 1] << 8) | c[:, 2]).astype(np.uint32)
+
+
+def textures_scene(resolution=(128, 72), with_lights=True, point_light_only=False) -> M.Scene:
+    """Every texture the compiled scene format carries (checkerboard, polka dot,
+    bullseye, marble, simplex fBm, LDR image, blend, surface normal, dot product,
+    UV, constant), both shading-normal modifiers, the three composite materials,
+    textured float parameters (Disney roughness and metallic, Matte angle) and a
+    textured emission, on spheres over a ground plane with a composite material.
+    With ``point_light_only`` the first-bounce radiance is the same per sample
+    on every renderer that shares the random numbers (no light is sampled)."""
+    cam = M.Camera(eye=(0.0, 4.2, 6.8), look_at=(0.0, 0.4, -0.6), fov_x_deg=62.0, resolution=resolution)
+    sc = M.Scene(camera=cam, name="textures")
+    checker = M.CheckerboardTexture(a=(0.85, 0.2, 0.15), b=(0.15, 0.25, 0.85), angle_deg=30.0, scale=(8.0, 4.0))
+    polka = M.PolkaDotTexture(a=(0.9, 0.9, 0.2), b=(0.2, 0.5, 0.3), angle_deg=15.0, cell_resolution=6.0, radius=0.3)
+    bull = M.BullseyeTexture(a=(0.8, 0.4, 0.1), b=M.UVTexture(), origin=(0.3, 0.5, 0.2), scale=3.0)  # object space: off-centre rings
+    marble = M.MarbleTexture(color_a=(0.8, 0.8, 0.8), color_b=(0.4, 0.2, 0.1), color_c=(0.06, 0.04, 0.02), frequency=2.0, scale=5.0, octaves=4)
+    fbm = M.SimplexFBMTexture(color=(0.75, 0.5, 0.75), frequency=1.5, gain=0.5, octaves=4)
+    image = M.LDRImageTexture(resolution_x=16, resolution_y=8, image=ldr_image(16, 8, seed=3), angle_deg=10.0, scale=(2.0, 1.0))
+    blend = M.BlendTexture(a=checker, b=M.BlendTexture(a=M.UVTexture(), b=marble, t=(0.5, 0.5, 0.5)), t=(0.3, 0.5, 0.7))
+    nmap = M.NormalMapLDRImageModifier(resolution_x=8, resolution_y=8, image=normal_map_image(8, 8, seed=4), scale=(4.0, 2.0))
+    mats = [
+        M.Matte(kd=checker),
+        M.Matte(kd=polka, angle=M.CheckerboardTexture(a=(0.0, 0.0, 0.0), b=(30.0, 30.0, 30.0), scale=(4.0, 4.0))),
+        M.Matte(kd=bull),
+        M.Matte(kd=marble),
+        M.Plastic(kd=fbm, ks=(0.3, 0.3, 0.3), roughness=0.2),
+        M.Matte(kd=image),
+        M.Matte(kd=blend),
+        M.Matte(kd=M.SurfaceNormalTexture()),
+        M.Matte(kd=M.DotProductTexture()),
+        M.Disney(color=marble, roughness=M.CheckerboardTexture(a=(0.2, 0.2, 0.2), b=(0.7, 0.7, 0.7), scale=(6.0, 3.0)),
+                 metallic=M.PolkaDotTexture(a=(1.0, 1.0, 1.0), b=(0.0, 0.0, 0.0), cell_resolution=5.0, radius=0.35)),
+        M.Matte(kd=(0.7, 0.7, 0.7), modifier=nmap),
+        M.Plastic(kd=(0.3, 0.5, 0.8), ks=(0.4, 0.4, 0.4), roughness=0.1, modifier=M.SimplexNoiseNormalMapModifier(frequency=4.0, scale=1.0)),
+        M.CheckerboardMaterial(a=M.Matte(kd=(0.9, 0.2, 0.2)), b=M.Glass(), scale=(6.0, 3.0)),
+        M.PolkaDotMaterial(a=M.Matte(kd=(0.95, 0.95, 0.95)), b=M.Metal(roughness_u=0.2, roughness_v=0.2), cell_resolution=5.0, radius=0.3),
+        M.Matte(kd=(0.2, 0.2, 0.2), emission=M.CheckerboardTexture(a=(2.0, 1.5, 0.5), b=(0.0, 0.0, 0.0), scale=(10.0, 5.0))),
+    ]
+    for k, m in enumerate(mats):  # three rows of five
+        x = -3.4 + 1.7 * (k % 5)
+        z = 1.4 - 1.9 * (k // 5)
+        sc.add(M.Primitive(M.Sphere(), m, M.Transform.translate_scale((x, 0.7, z), 0.7)))
+    ground = M.BullseyeMaterial(a=M.Matte(kd=(0.55, 0.55, 0.55)), b=M.Plastic(kd=(0.3, 0.3, 0.35), ks=(0.3, 0.3, 0.3), roughness=0.3),
+                                origin=(0.0, 0.0, 0.0), scale=0.5)
+    sc.add(M.Primitive(M.Plane(), ground, _rot_x(-90.0, (0.0, 0.0, 0.0))))
+    if with_lights:
+        sc.lights.append(M.PointLight((2.0, 8.0, 6.0), (60.0, 60.0, 60.0)))
+        if not point_light_only:
+            sl = M.DiffuseAreaLight(M.Sphere(), (6.0, 5.0, 4.0), transform=M.Transform.translate_scale((-4.0, 6.0, 4.0), 0.6))
+            sc.lights.append(sl)
+            sc.add(M.Primitive(sl.shape, M.Matte(kd=(0.0, 0.0, 0.0)), M.Transform.translate_scale((-4.0, 6.0, 4.0), 0.6), area_light=sl))
+    return sc
+
+
 # ---- batched-job mix: eight seeded scenes and a job list over them --------------
 # Sphere counts 10 .. 10k and heightfield sizes 10k .. 2M triangles, each spaced
 # evenly in log scale over the eight scenes and paired in a shuffled order.

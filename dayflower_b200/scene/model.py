@@ -21,8 +21,10 @@ SHAPE_PARABOLOID, SHAPE_PLANE, SHAPE_POLYGON, SHAPE_RECTANGLE = 9, 10, 11, 13
 SHAPE_CUBOID, SHAPE_SPHERE, SHAPE_TORUS, SHAPE_TRIANGLE, SHAPE_MESH = 14, 15, 16, 17, 18
 MAT_DISNEY, MAT_GLASS, MAT_MATTE, MAT_METAL, MAT_MIRROR, MAT_PLASTIC = 4, 7, 11, 12, 13, 14
 MAT_CLEAR_COAT, MAT_GLOSSY, MAT_SUBSTRATE, MAT_TRANSLUCENT, MAT_UBER = 3, 8, 16, 18, 19
-TEX_CONSTANT = 4
-MOD_NOOP = 2
+MAT_BULLSEYE, MAT_CHECKERBOARD, MAT_POLKA_DOT = 1, 2, 15
+TEX_BLEND, TEX_BULLSEYE, TEX_CHECKERBOARD, TEX_CONSTANT, TEX_DOT_PRODUCT = 1, 2, 3, 4, 5
+TEX_LDR_IMAGE, TEX_MARBLE, TEX_POLKA_DOT, TEX_SIMPLEX_FBM, TEX_SURFACE_NORMAL, TEX_UV = 7, 8, 9, 10, 11, 12
+MOD_NOOP, MOD_NORMAL_MAP_LDR_IMAGE, MOD_SIMPLEX_NOISE_NORMAL_MAP = 2, 3, 4
 LIGHT_DIFFUSE_AREA, LIGHT_DIRECTIONAL, LIGHT_IMAGE, LIGHT_PEREZ = 1, 2, 3, 4
 LIGHT_POINT, LIGHT_SPOT = 5, 7
 BV_AABB, BV_SPHERE, BV_INFINITE = 1, 2, 3
@@ -329,10 +331,146 @@ class Polygon(Shape):
         return self.points
 
 
+# -------------------------------------------------------------- textures ----
+# A material parameter is a number, a colour or one of these (``scene/texture/``).
+# Children of the pattern textures are textures or plain colours.
+class Texture:
+    ID = 0
+
+
+@dataclass(eq=False)
+class ConstantTexture(Texture):
+    """``scene/texture/ConstantTexture``."""
+    color: Sequence[float] = (0.5, 0.5, 0.5)
+    ID = TEX_CONSTANT
+
+
+@dataclass(eq=False)
+class BlendTexture(Texture):
+    """``scene/texture/BlendTexture``: per-channel lerp(a, b, t)."""
+    a: object = (0.5, 0.5, 0.5)
+    b: object = (1.0, 1.0, 1.0)
+    t: Sequence[float] = (0.5, 0.5, 0.5)
+    ID = TEX_BLEND
+
+
+@dataclass(eq=False)
+class BullseyeTexture(Texture):
+    """``scene/texture/BullseyeTexture``: rings around ``origin`` (object space)."""
+    a: object = (0.5, 0.5, 0.5)
+    b: object = (1.0, 1.0, 1.0)
+    origin: Sequence[float] = (0.0, 10.0, 0.0)
+    scale: float = 1.0
+    ID = TEX_BULLSEYE
+
+
+@dataclass(eq=False)
+class CheckerboardTexture(Texture):
+    """``scene/texture/CheckerboardTexture`` over the texture coordinates."""
+    a: object = (0.5, 0.5, 0.5)
+    b: object = (1.0, 1.0, 1.0)
+    angle_deg: float = 0.0
+    scale: Sequence[float] = (1.0, 1.0)
+    ID = TEX_CHECKERBOARD
+
+
+@dataclass(eq=False)
+class DotProductTexture(Texture):
+    """``scene/texture/DotProductTexture``: |n_s . d|."""
+    ID = TEX_DOT_PRODUCT
+
+
+@dataclass(eq=False)
+class LDRImageTexture(Texture):
+    """``scene/texture/LDRImageTexture``: a packed-ARGB image, bilinear, wrapping."""
+    resolution_x: int = 1
+    resolution_y: int = 1
+    image: object = None  # uint32 ARGB, row-major, resolution_x * resolution_y
+    angle_deg: float = 0.0
+    scale: Sequence[float] = (1.0, 1.0)
+    ID = TEX_LDR_IMAGE
+
+
+@dataclass(eq=False)
+class MarbleTexture(Texture):
+    """``scene/texture/MarbleTexture`` (Perlin turbulence); colours are packed to 8 bits."""
+    color_a: Sequence[float] = (0.8, 0.8, 0.8)
+    color_b: Sequence[float] = (0.4, 0.2, 0.1)
+    color_c: Sequence[float] = (0.06, 0.04, 0.02)
+    frequency: float = 1.0
+    scale: float = 5.0
+    stripes: float = 0.15
+    octaves: int = 8
+    ID = TEX_MARBLE
+
+
+@dataclass(eq=False)
+class PolkaDotTexture(Texture):
+    """``scene/texture/PolkaDotTexture`` over the texture coordinates."""
+    a: object = (0.5, 0.5, 0.5)
+    b: object = (1.0, 1.0, 1.0)
+    angle_deg: float = 0.0
+    cell_resolution: float = 10.0
+    radius: float = 0.25
+    ID = TEX_POLKA_DOT
+
+
+@dataclass(eq=False)
+class SimplexFBMTexture(Texture):
+    """``scene/texture/SimplexFractionalBrownianMotionTexture``; the colour is packed to 8 bits."""
+    color: Sequence[float] = (0.75, 0.5, 0.75)
+    frequency: float = 5.0
+    gain: float = 0.5
+    octaves: int = 16
+    ID = TEX_SIMPLEX_FBM
+
+
+@dataclass(eq=False)
+class SurfaceNormalTexture(Texture):
+    """``scene/texture/SurfaceNormalTexture``: (n_s + 1) / 2, n_s facing the ray."""
+    ID = TEX_SURFACE_NORMAL
+
+
+@dataclass(eq=False)
+class UVTexture(Texture):
+    """``scene/texture/UVTexture``: (u, v, 0)."""
+    ID = TEX_UV
+
+
+# ------------------------------------------------------------- modifiers ----
+class Modifier:
+    ID = 0
+
+
+@dataclass(eq=False)
+class NoOpModifier(Modifier):
+    ID = MOD_NOOP
+
+
+@dataclass(eq=False)
+class NormalMapLDRImageModifier(Modifier):
+    """``scene/modifier/NormalMapLDRImageModifier``: shading normal from an image, in the geometric frame."""
+    resolution_x: int = 1
+    resolution_y: int = 1
+    image: object = None
+    angle_deg: float = 0.0
+    scale: Sequence[float] = (1.0, 1.0)
+    ID = MOD_NORMAL_MAP_LDR_IMAGE
+
+
+@dataclass(eq=False)
+class SimplexNoiseNormalMapModifier(Modifier):
+    """``scene/modifier/SimplexNoiseNormalMapModifier``: shading normal perturbed by simplex fBm."""
+    frequency: float = 16.0
+    scale: float = 1.0
+    ID = MOD_SIMPLEX_NOISE_NORMAL_MAP
+
+
 # ------------------------------------------------------------- materials ----
 @dataclass(eq=False)
 class Material:
     emission: Sequence[float] = (0.0, 0.0, 0.0)
+    modifier: Optional[Modifier] = None
     ID = 0
 
 
@@ -458,6 +596,38 @@ class Uber(Material):
     roughness_v: float = 0.1
     remap_roughness: bool = True
     ID = MAT_UBER
+
+
+@dataclass(eq=False)
+class BullseyeMaterial(Material):
+    """``scene/material/BullseyeMaterial``: material ``a`` where the object-space
+    distance to ``origin`` times ``scale`` has a fractional part above 0.5."""
+    a: Optional[Material] = None
+    b: Optional[Material] = None
+    origin: Sequence[float] = (0.0, 10.0, 0.0)
+    scale: float = 1.0
+    ID = MAT_BULLSEYE
+
+
+@dataclass(eq=False)
+class CheckerboardMaterial(Material):
+    """``scene/material/CheckerboardMaterial`` over the texture coordinates."""
+    a: Optional[Material] = None
+    b: Optional[Material] = None
+    angle_deg: float = 0.0
+    scale: Sequence[float] = (1.0, 1.0)
+    ID = MAT_CHECKERBOARD
+
+
+@dataclass(eq=False)
+class PolkaDotMaterial(Material):
+    """``scene/material/PolkaDotMaterial`` over the texture coordinates."""
+    a: Optional[Material] = None
+    b: Optional[Material] = None
+    angle_deg: float = 0.0
+    cell_resolution: float = 10.0
+    radius: float = 0.25
+    ID = MAT_POLKA_DOT
 
 
 # ---------------------------------------------------------------- lights ----

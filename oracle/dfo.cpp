@@ -19,6 +19,7 @@
 // uploads (CompiledScene arrays, same names), decoded here independently of
 // the device renderer's ingest.
 #include "dfo_math.h"
+#include "dfo_noise.h"
 
 #include <algorithm>
 #include <atomic>
@@ -38,9 +39,14 @@ enum { kShapeCone = 2, kShapeCylinder = 5, kShapeDisk = 6, kShapeHyperboloid = 7
        kShapeMesh = 18 };
 enum {
   kMatClearCoat = 3, kMatDisney = 4, kMatGlass = 7, kMatGlossy = 8, kMatMatte = 11, kMatMetal = 12, kMatMirror = 13, kMatPlastic = 14,
-  kMatSubstrate = 16, kMatTranslucent = 18, kMatUber = 19
+  kMatSubstrate = 16, kMatTranslucent = 18, kMatUber = 19,
+  kMatBullseye = 1, kMatCheckerboard = 2, kMatPolkaDot = 15  // composite: pick material A or B per hit
 };
-enum { kTexConstant = 4 };
+enum {  // scene/texture/*Texture.java ID
+  kTexBlend = 1, kTexBullseye = 2, kTexCheckerboard = 3, kTexConstant = 4, kTexDotProduct = 5, kTexLDRImage = 7, kTexMarble = 8,
+  kTexPolkaDot = 9, kTexSimplexFBM = 10, kTexSurfaceNormal = 11, kTexUV = 12
+};
+enum { kModNoOp = 2, kModNormalMapLDRImage = 3, kModSimplexNoiseNormalMap = 4 };  // scene/modifier/*Modifier.java ID
 enum { kLightDiffuseArea = 1, kLightDirectional = 2, kLightImage = 3, kLightPerez = 4, kLightPoint = 5, kLightSpot = 7 };
 enum { kAlgoAO = 0, kAlgoDepth = 1, kAlgoPath = 2, kAlgoRayCast = 3, kAlgoRayTrace = 4 };
 
@@ -773,6 +779,7 @@ struct Hit {  // scene/Intersection.java
   int prim = -1;
   int tri = -1;
   Surface w;  // world space
+  V3 p_obj;   // object-space surface intersection point (BullseyeTexture, BullseyeMaterial)
 };
 
 // geometry/SurfaceIntersector3F.java:188 doTransformT
@@ -827,6 +834,7 @@ inline bool scene_intersect(const Scene& sc, const Ray& ray_in, float tmin, floa
   if (!shape_surface(sc, P[6], P[7], ro, kTMinimum, kTMaximum, &so, &tri)) return false;
   hit->prim = prim; hit->tri = tri;
   hit->w = surface_transform(so, sc.o2w[prim], sc.w2o[prim]);
+  hit->p_obj = so.p;
   return true;
 }
 
@@ -844,14 +852,119 @@ inline void material_slot(const Scene& sc, const std::vector<int32_t>& arr, int 
 inline int material_int(const Scene& sc, const std::vector<int32_t>& arr, int base, int slot) {
   return sc.layout == 2 ? arr[base + slot * 4] : arr[base + slot];
 }
-// renderer/gpu/AbstractTextureKernel.java:152 (ConstantTexture only)
+// What a texture sees of the intersection (scene/Intersection.java): world
+// point, object-space point, shading normal (after the material's modifier),
+// ray direction and texture coordinates.
+struct TexCtx { V3 p, p_obj, ns, d; float u, v; };
+thread_local const TexCtx* g_tex = nullptr;  // set while a material is evaluated at a hit
+
+inline TexCtx tex_ctx(const Hit& h) { return TexCtx{h.w.p, h.p_obj, h.w.s.w, h.w.ray.d, h.w.tu, h.w.tv}; }
+
+inline float jsin(float a) { return (float)std::sin((double)a); }  // utility/Floats.java sin, cos: Math in double
+inline float jcos(float a) { return (float)std::cos((double)a); }
+inline float frac(float x) { return x - std::floor(x); }            // Floats.fractionalPart(x, false)
+inline float jmod(float x, float y) { return std::fmod(x, y); }     // Java float %
+inline float pos_mod(float x, float y) { return x < 0.0f ? jmod(jmod(x, y) + y, y) : jmod(x, y); }  // Floats.positiveModulo
+inline int pos_mod_i(int x, int y) { return x < 0 ? (x % y + y) % y : x % y; }                         // Ints.positiveModulo
+inline V3 unpack_argb(int c) {  // Color3F.unpack(ARGB): 8-bit channels / 255
+  return {(float)((c >> 16) & 0xFF) / 255.0f, (float)((c >> 8) & 0xFF) / 255.0f, (float)(c & 0xFF) / 255.0f};
+}
+inline V3 lerp3(V3 a, V3 b, V3 t) { return {(1.0f - t.x) * a.x + t.x * b.x, (1.0f - t.y) * a.y + t.y * b.y, (1.0f - t.z) * a.z + t.z * b.z}; }
+inline TexRef unpack16(float f) { const int v = (int)f; return TexRef{(v >> 16) & 0xFFFF, v & 0xFFFF}; }
+
+// LDRImageTexture.doGetColorRGB / AbstractLDRImageModifier.getColorRGB over a
+// compiled image record (angle radians, scale x, y, resolution x, y, ARGB pixels).
+inline V3 image_texel(const float* rec, int x, int y) {
+  const int rx = (int)rec[3], ry = (int)rec[4];
+  return unpack_argb((int)rec[5 + pos_mod_i(y, ry) * rx + pos_mod_i(x, rx)]);
+}
+inline void image_point(const float* rec, float u, float v, float* x, float* y) {
+  const float c = jcos(rec[0]), s = jsin(rec[0]);  // Point2F.rotateCounterclockwise
+  const float ru = u * c - v * s, rv = v * c + u * s;
+  const float rx = (float)(int)rec[3], ry = (float)(int)rec[4];
+  *x = pos_mod(ru * rec[1] * rx - 0.5f, rx);  // Point2F.scale, Point2F.toImage
+  *y = pos_mod(rv * rec[2] * ry - 0.5f, ry);
+}
+inline V3 image_bilinear(const float* rec, float x, float y) {
+  const int x0 = (int)std::floor(x), x1 = (int)std::ceil(x), y0 = (int)std::floor(y), y1 = (int)std::ceil(y);
+  if (x0 == x1 && y0 == y1) return image_texel(rec, x0, y0);
+  const float tx = x - (float)x0, ty = y - (float)y0;
+  const V3 t3{tx, tx, tx}, s3{ty, ty, ty};
+  return lerp3(lerp3(image_texel(rec, x0, y0), image_texel(rec, x1, y0), t3), lerp3(image_texel(rec, x0, y1), image_texel(rec, x1, y1), t3), s3);
+}
+
+// Texture.getColor(intersection) of every compiled texture (scene/texture/*.java getColor).
+inline V3 tex_eval(const Scene& sc, TexRef t, const TexCtx& c, int depth) {
+  if (depth > 32) return {0.5f, 0.5f, 0.5f};
+  switch (t.id) {
+    case kTexConstant: {
+      const float* q = sc.F("textureConstantTextureArray").data() + (size_t)t.off * 4;
+      return {q[0], q[1], q[2]};
+    }
+    case kTexBlend: {  // BlendTexture: Color3F.blend(A, B, t1, t2, t3)
+      const float* q = sc.F("textureBlendTextureArray").data() + (size_t)t.off * 8;
+      return lerp3(tex_eval(sc, unpack16(q[0]), c, depth + 1), tex_eval(sc, unpack16(q[1]), c, depth + 1), V3{q[2], q[3], q[4]});
+    }
+    case kTexBullseye: {  // BullseyeTexture: object-space distance to the origin
+      const float* q = sc.F("textureBullseyeTextureArray").data() + (size_t)t.off * 8;
+      const V3 dir = c.p_obj - V3{q[0], q[1], q[2]};
+      const float r = jmod(length(dir) * q[5], 1.0f);
+      return tex_eval(sc, unpack16(r > 0.5f ? q[3] : q[4]), c, depth + 1);
+    }
+    case kTexCheckerboard: {
+      const float* q = sc.F("textureCheckerboardTextureArray").data() + (size_t)t.off * 8;
+      const float cs = jcos(q[1]), sn = jsin(q[1]);
+      const bool iu = frac((c.u * cs - c.v * sn) * q[4]) > 0.5f;
+      const bool iv = frac((c.v * cs + c.u * sn) * q[5]) > 0.5f;
+      return tex_eval(sc, unpack16((iu ^ iv) ? q[2] : q[3]), c, depth + 1);
+    }
+    case kTexPolkaDot: {
+      const float* q = sc.F("texturePolkaDotTextureArray").data() + (size_t)t.off * 8;
+      const float cs = jcos(q[1]), sn = jsin(q[1]);
+      const float x = frac((c.u * cs - c.v * sn) * q[4]) - 0.5f;
+      const float y = frac((c.v * cs + c.u * sn) * q[4]) - 0.5f;
+      return tex_eval(sc, unpack16(x * x + y * y < q[5] * q[5] ? q[2] : q[3]), c, depth + 1);
+    }
+    case kTexDotProduct: {  // |n_s . d|
+      const float d = std::fabs(dot(c.ns, c.d));
+      return {d, d, d};
+    }
+    case kTexLDRImage: {
+      const int abs_off = sc.I("textureLDRImageTextureOffsetArray")[t.off];
+      const float* q = sc.F("textureLDRImageTextureArray").data() + abs_off;
+      float x, y;
+      image_point(q, c.u, c.v, &x, &y);
+      return image_bilinear(q, x, y);
+    }
+    case kTexMarble: {  // MarbleTexture (colours as compiled: packed ARGB)
+      const float* q = sc.F("textureMarbleTextureArray").data() + (size_t)t.off * 8;
+      const float x = c.p.x * q[3], y = c.p.y * q[3], z = c.p.z * q[3];
+      const float r = q[4] * dfo_noise::perlin_turbulence(x, y, z, (int)q[6]);
+      const float s = 2.0f * std::fabs(jsin(x + r));
+      const float tt = s < 1.0f ? s : s - 1.0f;
+      const V3 ca = unpack_argb((int)q[0]), cb = unpack_argb((int)q[1]), cc = unpack_argb((int)q[2]);
+      return lerp3(s < 1.0f ? cc : cb, s < 1.0f ? cb : ca, V3{tt, tt, tt});
+    }
+    case kTexSimplexFBM: {
+      const float* q = sc.F("textureSimplexFractionalBrownianMotionTextureArray").data() + (size_t)t.off * 4;
+      const float n = dfo_noise::simplex_fbm(c.p.x, c.p.y, c.p.z, q[1], q[2], 0.0f, 1.0f, (int)q[3]);
+      return unpack_argb((int)q[0]) * n;
+    }
+    case kTexSurfaceNormal: {  // (n_s facing the ray + 1) / 2
+      const V3 n = dot(c.ns, c.d) > 0.0f ? -c.ns : c.ns;
+      return {(n.x + 1.0f) / 2.0f, (n.y + 1.0f) / 2.0f, (n.z + 1.0f) / 2.0f};
+    }
+    case kTexUV: return {c.u, c.v, 0.0f};
+    default: return {0.5f, 0.5f, 0.5f};
+  }
+}
 inline V3 tex_color(const Scene& sc, TexRef t) {
   if (t.id == kTexConstant) {
-    const auto& C = sc.F("textureConstantTextureArray");
-    const float* q = C.data() + (size_t)t.off * 4;
+    const float* q = sc.F("textureConstantTextureArray").data() + (size_t)t.off * 4;
     return {q[0], q[1], q[2]};
   }
-  return {0, 0, 0};
+  if (!g_tex) return {0.5f, 0.5f, 0.5f};
+  return tex_eval(sc, t, *g_tex, 0);
 }
 inline float tex_float(const Scene& sc, TexRef t) { V3 c = tex_color(sc, t); return (c.x + c.y + c.z) / 3.0f; }  // ConstantTexture.getFloat = average
 inline V3 sat0(V3 c) { return {std::fmax(c.x, 0.0f), std::fmax(c.y, 0.0f), std::fmax(c.z, 0.0f)}; }  // Color3F.saturate(c, 0, MAX)
@@ -1270,7 +1383,7 @@ inline Lobe make_tr_lobe(LobeKind k, int type, V3 scale, float ax, float ay) {
 // (scene/compiler/CompiledMaterialCache.java:2830-3294).
 // u_material: the random number a material draws when it builds its BSDF
 // (ClearCoatMaterial.java:323, Floats.random()).
-inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool multi, float u_material, Bsdf* B, bool* supported) {
+inline bool build_bsdf_material(const Scene& sc, int mid, int moff, const Hit& h, bool multi, float u_material, Bsdf* B, bool* supported) {
   *supported = true;
   B->n = 0; B->eta = 1.0f; B->present = false;
   TexRef a, b;
@@ -1524,26 +1637,117 @@ inline bool build_bsdf(const Scene& sc, int mid, int moff, const Hit& h, bool mu
   return true;
 }
 
-// Material.emittance (the emission texture of every supported material is slot 0, texture A)
-inline V3 material_emission(const Scene& sc, int mid, int moff) {
-  const char* name = nullptr;
+inline const char* material_array(int mid) {
   switch (mid) {
-    case kMatMatte: name = "materialMatteMaterialArray"; break;
-    case kMatMirror: name = "materialMirrorMaterialArray"; break;
-    case kMatGlass: name = "materialGlassMaterialArray"; break;
-    case kMatMetal: name = "materialMetalMaterialArray"; break;
-    case kMatPlastic: name = "materialPlasticMaterialArray"; break;
-    case kMatDisney: name = "materialDisneyMaterialArray"; break;
-    case kMatClearCoat: name = "materialClearCoatMaterialArray"; break;
-    case kMatGlossy: name = "materialGlossyMaterialArray"; break;
-    case kMatSubstrate: name = "materialSubstrateMaterialArray"; break;
-    case kMatTranslucent: name = "materialTranslucentMaterialArray"; break;
-    case kMatUber: name = "materialUberMaterialArray"; break;
-    default: return {0, 0, 0};
+    case kMatMatte: return "materialMatteMaterialArray";
+    case kMatMirror: return "materialMirrorMaterialArray";
+    case kMatGlass: return "materialGlassMaterialArray";
+    case kMatMetal: return "materialMetalMaterialArray";
+    case kMatPlastic: return "materialPlasticMaterialArray";
+    case kMatDisney: return "materialDisneyMaterialArray";
+    case kMatClearCoat: return "materialClearCoatMaterialArray";
+    case kMatGlossy: return "materialGlossyMaterialArray";
+    case kMatSubstrate: return "materialSubstrateMaterialArray";
+    case kMatTranslucent: return "materialTranslucentMaterialArray";
+    case kMatUber: return "materialUberMaterialArray";
+    default: return nullptr;
   }
+}
+
+// BullseyeMaterial / CheckerboardMaterial / PolkaDotMaterial.doGetMaterial
+// (scene/material/*Material.java), repeated while the pick is itself composite.
+// Records are float arrays at absolute offsets; A and B are Ints.pack(id, offset).
+inline void resolve_material(const Scene& sc, const Hit& h, int* mid, int* moff) {
+  for (int guard = 0; guard < 64; ++guard) {
+    const float* q;
+    bool a;
+    if (*mid == kMatBullseye) {
+      q = sc.F("materialBullseyeMaterialArray").data() + *moff;
+      a = jmod(length(h.p_obj - V3{q[0], q[1], q[2]}) * q[5], 1.0f) > 0.5f;
+      q += 3;
+    } else if (*mid == kMatCheckerboard) {
+      q = sc.F("materialCheckerboardMaterialArray").data() + *moff;
+      const float cs = jcos(q[1]), sn = jsin(q[1]), u = h.w.tu, v = h.w.tv;
+      a = (frac((u * cs - v * sn) * q[4]) > 0.5f) ^ (frac((v * cs + u * sn) * q[5]) > 0.5f);
+      q += 2;
+    } else if (*mid == kMatPolkaDot) {
+      q = sc.F("materialPolkaDotMaterialArray").data() + *moff;
+      const float cs = jcos(q[1]), sn = jsin(q[1]), u = h.w.tu, v = h.w.tv;
+      const float x = frac((u * cs - v * sn) * q[4]) - 0.5f, y = frac((v * cs + u * sn) * q[4]) - 0.5f;
+      a = x * x + y * y < q[5] * q[5];
+      q += 2;
+    } else {
+      return;
+    }
+    const TexRef r = unpack16(a ? q[0] : q[1]);
+    *mid = r.id; *moff = r.off;
+  }
+  *mid = -1;  // a cycle: no material
+}
+
+// Intersection.setSurfaceNormalS: the shading frame rebuilt around n with the old v (OrthonormalBasis33F(w, v)).
+inline void set_normal_s(Hit* h, V3 n) {
+  const V3 w = normalize(n);
+  const V3 u = normalize(cross(normalize(h->w.s.v), w));
+  ONB o;
+  o.w = w; o.u = u; o.v = cross(w, u);
+  h->w.s = o;
+}
+
+// Modifier.modify (scene/modifier/*.java): the material's modifier, slot 0 texture B.
+inline void apply_modifier(const Scene& sc, int mid, int moff, Hit* h) {
+  const char* name = material_array(mid);
+  if (!name) return;
+  TexRef e, m;
+  material_slot(sc, sc.I(name), moff, 0, &e, &m);
+  if (m.id == kModNormalMapLDRImage) {  // NormalMapLDRImageModifier.modify: nearest texel, in the geometric frame
+    const int abs_off = sc.I("modifierNormalMapLDRImageModifierOffsetArray")[m.off];
+    const float* q = sc.F("modifierNormalMapLDRImageModifierArray").data() + abs_off;
+    float x, y;
+    image_point(q, h->w.tu, h->w.tv, &x, &y);
+    const V3 c = image_texel(q, (int)x, (int)y);
+    const V3 l{c.x * 2.0f - 1.0f, c.y * 2.0f - 1.0f, c.z * 2.0f - 1.0f};
+    const ONB& g = h->w.g;  // Vector3F.transform(v, ONB): u * v.x + v * v.y + w * v.z
+    const V3 n{l.x * g.u.x + l.y * g.v.x + l.z * g.w.x, l.x * g.u.y + l.y * g.v.y + l.z * g.w.y, l.x * g.u.z + l.y * g.v.z + l.z * g.w.z};
+    set_normal_s(h, normalize(n));
+  } else if (m.id == kModSimplexNoiseNormalMap) {  // SimplexNoiseNormalMapModifier.modify
+    const float* q = sc.F("modifierSimplexNoiseNormalMapModifierArray").data() + (size_t)m.off * 2;
+    const float freq = q[0], scale = q[1], rf = 1.0f / freq;
+    const V3 p = h->w.p, n = h->w.s.w;
+    const float x0 = p.x * rf, y0 = p.y * rf, z0 = p.z * rf;
+    const float x1 = n.x + dfo_noise::simplex_fbm(x0, y0, z0, freq, 0.5f, -0.25f, 0.25f, 16) * scale;
+    const float y1 = n.y + dfo_noise::simplex_fbm(y0, z0, x0, freq, 0.5f, -0.25f, 0.25f, 16) * scale;
+    const float z1 = n.z + dfo_noise::simplex_fbm(z0, x0, y0, freq, 0.5f, -0.25f, 0.25f, 16) * scale;
+    set_normal_s(h, normalize(V3{x1, y1, z1}));
+  }
+}
+
+// Material.computeScatteringFunctions: composite materials pick their material,
+// the material's modifier changes the shading frame of the hit (kept for the
+// rest of the bounce, as the reference's Intersection is), then the textures
+// are evaluated at the modified hit.
+inline bool build_bsdf(const Scene& sc, int mid, int moff, Hit& h, bool multi, float u_material, Bsdf* B, bool* supported) {
+  resolve_material(sc, h, &mid, &moff);
+  apply_modifier(sc, mid, moff, &h);
+  const TexCtx c = tex_ctx(h);
+  g_tex = &c;
+  const bool r = build_bsdf_material(sc, mid, moff, h, multi, u_material, B, supported);
+  g_tex = nullptr;
+  return r;
+}
+
+// Material.emittance (the emission texture of every supported material is slot 0, texture A)
+inline V3 material_emission(const Scene& sc, const Hit& h, int mid, int moff) {
+  resolve_material(sc, h, &mid, &moff);
+  const char* name = material_array(mid);
+  if (!name) return {0, 0, 0};
   TexRef a, b;
   material_slot(sc, sc.I(name), moff, 0, &a, &b);
-  return tex_color(sc, a);
+  const TexCtx c = tex_ctx(h);
+  g_tex = &c;
+  const V3 e = tex_color(sc, a);
+  g_tex = nullptr;
+  return e;
 }
 
 // scene/BSDF.java:evaluateDistributionFunction / evaluateProbabilityDensityFunction / sampleDistributionFunction
@@ -1976,7 +2180,7 @@ inline V3 hit_Le(const Scene& sc, const Hit& h, V3 dir) {
       return (two || dot(h.w.s.w, dir) > 0.0f) ? V3{q[32], q[33], q[34]} : V3{0, 0, 0};
     }
   }
-  return material_emission(sc, P[4], P[5]);
+  return material_emission(sc, h, P[4], P[5]);
 }
 inline bool hit_is_light(const Scene& sc, const Hit& h, const LightRef& lr) {
   uint32_t al = (uint32_t)sc.prims[h.prim * 8 + 1];
@@ -2548,6 +2752,13 @@ int dfo_primary_ray(void* s, float ix, float iy, float px, float py, float* out6
   if (!primary_ray(sc->cam, ix, iy, px, py, 0.5f, 0.5f, &r)) return 0;
   out6[0] = r.o.x; out6[1] = r.o.y; out6[2] = r.o.z; out6[3] = r.d.x; out6[4] = r.d.y; out6[5] = r.d.z;
   return 1;
+}
+// noise/PerlinNoiseF.java, noise/SimplexNoiseF.java
+float dfo_perlin(float x, float y, float z) { return dfo_noise::perlin(x, y, z); }
+float dfo_perlin_turbulence(float x, float y, float z, int octaves) { return dfo_noise::perlin_turbulence(x, y, z, octaves); }
+float dfo_simplex(float x, float y, float z) { return dfo_noise::simplex(x, y, z); }
+float dfo_simplex_fbm(float x, float y, float z, float frequency, float gain, float minimum, float maximum, int octaves) {
+  return dfo_noise::simplex_fbm(x, y, z, frequency, gain, minimum, maximum, octaves);
 }
 
 }  // extern "C"

@@ -78,6 +78,10 @@ def lib() -> ctypes.CDLL:
         L.dfo_rng_uniform.restype = _c_f
         L.dfo_rng_uniform.argtypes = [_c_u, _c_u]
         L.dfo_primary_ray.argtypes = [_c_p, _c_f, _c_f, _c_f, _c_f, _c_p]
+        for n, args in (("dfo_perlin", [_c_f] * 3), ("dfo_simplex", [_c_f] * 3), ("dfo_perlin_turbulence", [_c_f] * 3 + [_c_i]),
+                        ("dfo_simplex_fbm", [_c_f] * 7 + [_c_i])):
+            getattr(L, n).restype = _c_f
+            getattr(L, n).argtypes = args
         L.dfo_colorspace.argtypes = [_c_p, _c_i, _c_p, _c_p]
         L.dfo_onb_transform.argtypes = [_c_p, _c_p, _c_p]
         L.dfo_set_no_drift.argtypes = [_c_i]

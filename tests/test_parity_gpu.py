@@ -48,11 +48,17 @@ def instances():
 
 
 @pytest.fixture(scope="module")
+def textures():
+    return compile_scene(G.textures_scene(resolution=(128, 72)))
+
+
+@pytest.fixture(scope="module")
 def terrain():
     return compile_scene(G.terrain_spheres(cells=128, n_spheres=300, resolution=(160, 90), seed=11), layout_version=2)
 
 
-@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney", "materials", "image_light", "instances"])
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "terrain", "quadrics", "disney", "materials", "image_light", "instances",
+                                        "textures"])
 def test_ray_casting_hit_ids(scene_name, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.RAY_CASTING)
@@ -76,7 +82,8 @@ def test_depth_camera(scene_name, request):
     assert np.mean(np.all(np.abs(mg - mo) <= 1e-4 + 1e-4 * np.abs(mo), axis=-1)) >= 0.999
 
 
-@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16), ("materials", 16), ("image_light", 16), ("instances", 8)])
+@pytest.mark.parametrize("scene_name,spp", [("cornell", 16), ("mixed", 16), ("terrain", 8), ("quadrics", 16), ("disney", 16), ("materials", 16), ("image_light", 16), ("instances", 8),
+                                                 ("textures", 16)])
 def test_path_tracing_sigma(scene_name, spp, request):
     cs = request.getfixturevalue(scene_name)
     g = PT.render_gpu(cs, RA.PATH_TRACING, spp=spp, max_bounce=8)
@@ -96,7 +103,7 @@ def test_ambient_occlusion_sigma(scene_name, request):
     assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
 
 
-@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "materials"])
+@pytest.mark.parametrize("scene_name", ["cornell", "mixed", "materials", "textures"])
 def test_ray_tracing_sigma(scene_name, request):
     # Whitted ray tracer (Scene.java:786): every light per hit, specular reflection and transmission recursively
     cs = request.getfixturevalue(scene_name)
@@ -142,6 +149,20 @@ def test_path_tracing_rmse_against_converged(scene_name, request):
         mse_o.append(np.mean((o["sum"] / np.maximum(o["count"], 1)[..., None] - ref) ** 2))
     rmse_g, rmse_o = float(np.sqrt(np.mean(mse_g))), float(np.sqrt(np.mean(mse_o)))
     assert abs(rmse_g - rmse_o) <= 0.02 * rmse_o, "RMSE device %.5f oracle %.5f" % (rmse_g, rmse_o)
+
+
+def test_textures_direct_lighting_per_pixel():
+    # Point light only, first bounce: each sample's radiance is kd(texture) f cos / d^2 at the
+    # (possibly modified) hit, with no light sampling, so device and oracle agree per pixel.
+    # Covers every texture, both modifiers, the composite materials and the textured emission.
+    cs = compile_scene(G.textures_scene(resolution=(128, 72), point_light_only=True))
+    g = PT.render_gpu(cs, RA.PATH_TRACING, spp=2, max_bounce=1)
+    o = PT.render_oracle_no_drift(cs, RA.PATH_TRACING, spp=2, max_bounce=1)
+    mg = g["sum"] / np.maximum(g["count"], 1)[..., None]
+    mo = o["sum"] / np.maximum(o["count"], 1)[..., None]
+    close = np.all(np.abs(mg - mo) <= 1e-3 * np.abs(mo) + 1e-4, axis=-1)
+    assert close.mean() >= 0.999, "per-pixel agreement %.4f" % close.mean()
+    assert mo.mean() > 0.05
 
 
 def _reference_rgba8(mean, tone_mapper):
