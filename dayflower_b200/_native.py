@@ -46,6 +46,9 @@ SIGNATURES = [
     ("dfc_read_primary_hits", _c_int, [_c_p, _c_p, _c_p, _c_i64]),
     ("dfc_read_counters", _c_int, [_c_p, _c_p]),
     ("dfc_read_stage_times", _c_int, [_c_p, _c_p]),
+    ("dfc_read_commit_times", _c_int, [_c_p, _c_p]),
+    ("dfc_set_bvh_builder", _c_int, [_c_p, _c_int]),
+    ("dfc_engine_set_bvh_builder", _c_int, [_c_p, _c_int]),
     ("dfc_trace_rays_noalloc", _c_int, [_c_p, _c_p, _c_p, _c_p, _c_i64]),
     # batch and serving engine
     ("dfc_engine_create", _c_int, [_c_int, _c_i64, ctypes.POINTER(_c_p)]),

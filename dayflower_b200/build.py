@@ -18,8 +18,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 ROOT = os.path.dirname(HERE)
 
-CUDA_SOURCES = ["dfc_api.cu", "dfc_engine.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp", "dfc_devscene.cpp"]
-CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h", "dfc_devscene.h"]
+CUDA_SOURCES = ["dfc_api.cu", "dfc_engine.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp", "dfc_devscene.cpp", "dfc_blas.cu"]
+CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h", "dfc_devscene.h",
+                "dfc_blas.h", "dfc_texture.cuh", "dfc_matderive.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -8,6 +8,8 @@
 // between the bounce steps.
 #include <cuda_runtime.h>
 
+#include <chrono>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -47,6 +49,7 @@ struct dfc_renderer {
   int steps = 0;
   DevBuf d_film_sum, d_film_sq, d_primary_prim, d_primary_t, d_rgba;
   int film_filter = 0;   // 0: per-pixel box film; 1: the CPU renderer's Gaussian XYZ film (PixelImageF)
+  int bvh_builder = DFC_BVH_DEVICE;  // mesh hierarchies of later commits: device builder (default) or host SAH
   DevBuf d_film_consts;  // Gaussian film: filter table, sRGB -> XYZ, XYZ -> sRGB
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_overflow, d_ray_total;
@@ -54,6 +57,7 @@ struct dfc_renderer {
   DevBuf d_ao_o, d_ao_d, d_ao_v;
   int64_t pass = 0, total_paths = 0, launches = 0;
   float last_ms[5] = {0, 0, 0, 0, 0};
+  float commit_ms[4] = {0, 0, 0, 0};  // last dfc_scene_commit: ingest, of which BLAS, TLAS builds; upload
   // optional per-stage timing: event pairs around every launch of a render call
   int stage_timing = 0;
   std::vector<cudaEvent_t> ev_pool;
@@ -421,9 +425,15 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   cudaSetDevice(r->device);
   HostScene hs;
   std::string err;
-  int rc = ingest_scene(r->staged, layout_version, &hs, &err);
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = ingest_scene(r->staged, layout_version, &hs, &err, r->bvh_builder == DFC_BVH_DEVICE);
   if (rc != DFC_OK) return fail(r, rc, err);
+  const auto t1 = std::chrono::steady_clock::now();
+  r->commit_ms[0] = std::chrono::duration<float, std::milli>(t1 - t0).count();
+  r->commit_ms[1] = hs.blas_ms;
+  r->commit_ms[2] = hs.tlas_ms;
   DFC_CK(upload_scene(std::move(hs), r->stream, &r->scene), "scene upload");
+  r->commit_ms[3] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
   r->have_scene = true;
   r->staged = Staged();
   if (r->image_from_camera) {
@@ -616,6 +626,14 @@ int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
   return DFC_OK;
 }
 
+int dfc_set_bvh_builder(dfc_renderer* r, int builder) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(r->mu);
+  if (builder != DFC_BVH_HOST && builder != DFC_BVH_DEVICE) return fail(r, DFC_E_INVALID_ARG, "builder is DFC_BVH_HOST or DFC_BVH_DEVICE");
+  r->bvh_builder = builder;
+  return DFC_OK;
+}
+
 int dfc_set_film_filter(dfc_renderer* r, int filter) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
   std::lock_guard<std::mutex> lk(r->mu);
@@ -659,6 +677,13 @@ int dfc_read_counters(dfc_renderer* r, int64_t* out4) {
   out4[1] = r->total_paths;
   out4[2] = (int64_t)rays;
   out4[3] = r->launches;
+  return DFC_OK;
+}
+
+int dfc_read_commit_times(dfc_renderer* r, float* out4) {
+  if (!valid(r) || !out4) return fail(r, DFC_E_INVALID_ARG, "out == null");
+  std::lock_guard<std::mutex> lk(r->mu);
+  std::memcpy(out4, r->commit_ms, sizeof r->commit_ms);
   return DFC_OK;
 }
 

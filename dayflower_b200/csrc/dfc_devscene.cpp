@@ -1,6 +1,8 @@
 // Upload of a decoded scene (HostScene) into device buffers.
 #include "dfc_devscene.h"
 
+#include "dfc_blas.h"
+
 namespace dfc {
 
 namespace {
@@ -17,9 +19,12 @@ cudaError_t put(DevBuf& b, const std::vector<T>& v, cudaStream_t s) {
 
 }  // namespace
 
+size_t node_count(const HostScene& hs) { return (size_t)hs.blas_nodes + hs.nodes.size(); }
+size_t tri_pos_count(const HostScene& hs) { return hs.blas_tris > 0 ? 3 * (size_t)hs.blas_tris : hs.tri_pos.size(); }
+
 size_t scene_device_bytes(const HostScene& hs) {
-  return vbytes(hs.prims) + vbytes(hs.materials) + vbytes(hs.lights) + vbytes(hs.nodes) + vbytes(hs.tlas_items) +
-         vbytes(hs.tlas_bound) + vbytes(hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded) + vbytes(hs.tri_pos) +
+  return vbytes(hs.prims) + vbytes(hs.materials) + vbytes(hs.lights) + node_count(hs) * sizeof(BVH4Node) + vbytes(hs.tlas_items) +
+         vbytes(hs.tlas_bound) + vbytes(hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded) + tri_pos_count(hs) * sizeof(F4) +
          vbytes(hs.tri_attr) + vbytes(hs.rects) + vbytes(hs.shapes) + vbytes(hs.perez) + 19 * sizeof(float) +
          vbytes(hs.textures) + vbytes(hs.texels) + vbytes(hs.modifiers) + vbytes(hs.composites) + vbytes(hs.texmats);
 }
@@ -33,11 +38,18 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
   DFC_PUT(prims, hs.prims);
   DFC_PUT(mats, hs.materials);
   DFC_PUT(lights, hs.lights);
-  DFC_PUT(nodes, hs.nodes);
+  // nodes: the device-built bottom levels first (if any), then the host-built nodes
+  if (e == cudaSuccess) e = ds->nodes.ensure(node_count(hs) * sizeof(BVH4Node));
+  if (e == cudaSuccess && !hs.nodes.empty())
+    e = cudaMemcpyAsync(ds->nodes.as<BVH4Node>() + hs.blas_nodes, hs.nodes.data(), vbytes(hs.nodes), cudaMemcpyHostToDevice, s);
   DFC_PUT(tlas_items, hs.tlas_items);
   DFC_PUT(tlas_bound, hs.tlas_bound);
   DFC_PUT(unbounded, hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded);
-  DFC_PUT(tri_pos, hs.tri_pos);
+  if (hs.blas_tris > 0) {
+    if (e == cudaSuccess) e = ds->tri_pos.ensure(tri_pos_count(hs) * sizeof(F4));
+  } else {
+    DFC_PUT(tri_pos, hs.tri_pos);
+  }
   DFC_PUT(tri_attr, hs.tri_attr);
   DFC_PUT(rects, hs.rects);
   DFC_PUT(shapes, hs.shapes);
@@ -52,6 +64,22 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
 #undef DFC_PUT
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
+  if (!hs.blas_jobs.empty()) {  // bottom levels on the device, from the uploaded triangle records
+    int* idx = nullptr;
+    e = cudaMallocAsync(reinterpret_cast<void**>(&idx), vbytes(hs.blas_tri_index), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(idx, hs.blas_tri_index.data(), vbytes(hs.blas_tri_index), cudaMemcpyHostToDevice, s);
+    for (const HostScene::BlasJob& j : hs.blas_jobs) {
+      if (e != cudaSuccess) break;
+      cudaError_t be = cudaSuccess;
+      const int w = build_blas_device(ds->tri_attr.as<float>(), idx + j.index_off, j.count, ds->nodes.as<BVH4Node>() + j.node_base,
+                                      j.node_base, j.node_cap, ds->tri_pos.as<F4>() + 3 * (size_t)j.tri_first, j.tri_first, s, &be);
+      if (w < 0) e = be != cudaSuccess ? be : cudaErrorUnknown;
+    }
+    if (idx) cudaFreeAsync(idx, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    std::vector<int>().swap(hs.blas_tri_index);
+  }
   SceneView& v = ds->view;
   v.prims = ds->prims.as<DPrim>();
   v.prim_count = (int)hs.prims.size();

@@ -78,6 +78,7 @@ struct JobRec {
 
 struct dfc_engine {
   int device = 0;
+  int bvh_builder = DFC_BVH_DEVICE;  // mesh hierarchies of later scene commits
   int sm_count = 148;
   int max_trace_blocks = 6;
   cudaStream_t stream = nullptr, upload_stream = nullptr, read_stream = nullptr;
@@ -816,13 +817,20 @@ int dfc_engine_scene_put(dfc_engine* e, const char* name, const void* data, int6
   return DFC_OK;
 }
 
+int dfc_engine_set_bvh_builder(dfc_engine* e, int builder) {
+  if (!e || (builder != DFC_BVH_HOST && builder != DFC_BVH_DEVICE)) return DFC_E_INVALID_ARG;
+  std::lock_guard<std::mutex> c(e->commit_mu);
+  e->bvh_builder = builder;
+  return DFC_OK;
+}
+
 int dfc_engine_scene_commit(dfc_engine* e, int layout_version, int32_t* scene_id) {
   if (!e || !scene_id) return DFC_E_INVALID_ARG;
   std::lock_guard<std::mutex> c(e->commit_mu);
   cudaSetDevice(e->device);
   HostScene hs;
   std::string err;
-  int rc = ingest_scene(e->staged, layout_version, &hs, &err);
+  int rc = ingest_scene(e->staged, layout_version, &hs, &err, e->bvh_builder == DFC_BVH_DEVICE);
   e->staged = Staged();
   if (rc != DFC_OK) return efail(e, rc, err);
   const size_t bytes = scene_device_bytes(hs);

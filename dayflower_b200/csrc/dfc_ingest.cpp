@@ -12,6 +12,7 @@
 #include "dfc_ingest.h"
 
 #include <algorithm>
+#include <chrono>
 #include <thread>
 
 #include <cmath>
@@ -20,6 +21,7 @@
 #include <set>
 #include <sstream>
 
+#include "dfc_blas.h"
 #include "dfc_bvh.h"
 #include "dfc_matderive.h"
 
@@ -64,7 +66,9 @@ struct Decoder {
   std::map<std::pair<int, int>, int> material_index;
   std::map<int, int> light_by_key;  // (id << 16 | rel) -> index
 
-  Decoder(const Staged& s, int l, HostScene& h) : st(s), layout(l), hs(h) {}
+  bool device_blas = false;
+
+  Decoder(const Staged& s, int l, HostScene& h, bool dev) : st(s), layout(l), hs(h), device_blas(dev) {}
 
   const std::vector<float>& F(const char* n) { return get(st.f32, n); }
   const std::vector<int32_t>& I(const char* n) { return get(st.i32, n); }
@@ -591,11 +595,32 @@ struct Decoder {
         case kShapeMesh: {
           auto it = blas_by_offset.find(soff);
           if (it == blas_by_offset.end()) {
+            const auto t_blas = std::chrono::steady_clock::now();
             std::vector<int> offs;
             mesh_triangles(soff, offs);
             for (int to : offs)
               if (to < 0 || to % 24 != 0 || (size_t)to + 24 > T.size()) throw Fail{DFC_E_INVALID_ARG, "mesh triangle offset out of range"};
             if (offs.empty()) throw Fail{DFC_E_INVALID_ARG, "empty triangle mesh"};
+            if (device_blas) {  // the device builds this hierarchy into its own node range (dfc_blas.cu)
+              HostScene::BlasJob job;
+              job.index_off = hs.blas_tri_index.size();
+              job.count = (int)offs.size();
+              job.node_base = hs.blas_nodes;
+              job.node_cap = blas_node_capacity(job.count);
+              job.tri_first = (int)hs.blas_tris;
+              for (int to : offs) hs.blas_tri_index.push_back(to / 24);
+              hs.blas_jobs.push_back(job);
+              hs.blas_nodes += job.node_cap;
+              hs.blas_tris += job.count;
+              blas_info.push_back(BlasInfo{job.node_base, job.tri_first, job.count});
+              it = blas_by_offset.emplace(soff, (int)blas_info.size() - 1).first;
+              hs.triangles += (int64_t)offs.size();
+              hs.blas_ms += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
+              pr.data = job.node_base;
+              pr.tri_first = job.tri_first;
+              pr.tri_count = job.count;
+              break;
+            }
             std::vector<Box> boxes(offs.size());
             parallel_for(offs.size(), [&](size_t a, size_t b) {
               for (size_t k = a; k < b; ++k) {
@@ -629,6 +654,7 @@ struct Decoder {
             blas_info.push_back(BlasInfo{root, first, (int)offs.size()});
             it = blas_by_offset.emplace(soff, (int)blas_info.size() - 1).first;
             hs.triangles += (int64_t)offs.size();
+            hs.blas_ms += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_blas).count();
           }
           pr.data = blas_info[it->second].root;
           pr.tri_first = blas_info[it->second].first;
@@ -669,8 +695,16 @@ struct Decoder {
       hs.prims.push_back(pr);
     }
     if (!tlas_boxes.empty()) {
+      const auto t_tlas = std::chrono::steady_clock::now();
       std::vector<int> order;
       hs.tlas_root = build_bvh4(tlas_boxes, 4, hs.nodes, order);
+      hs.tlas_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_tlas).count();
+      if (hs.blas_nodes > 0) {  // host nodes follow the device-built region
+        for (BVH4Node& nd : hs.nodes)
+          for (int c = 0; c < 4; ++c)
+            if (nd.child[c] >= 0) nd.child[c] += hs.blas_nodes;
+        hs.tlas_root += hs.blas_nodes;
+      }
       hs.tlas_items.resize(order.size());
       hs.tlas_bound.resize(order.size());
       for (size_t k = 0; k < order.size(); ++k) {
@@ -682,7 +716,7 @@ struct Decoder {
     }
     if (hs.tlas_items.empty()) { hs.tlas_items.push_back(0); hs.tlas_bound.push_back(F4{0, 0, 0, -1}); }
     if (hs.unbounded.empty()) hs.unbounded_storage.push_back(0);
-    if (hs.tri_pos.empty()) hs.tri_pos.assign(3, F4{0, 0, 0, 0});
+    if (hs.tri_pos.empty() && hs.blas_tris == 0) hs.tri_pos.assign(3, F4{0, 0, 0, 0});
     if (hs.nodes.empty()) hs.nodes.push_back(BVH4Node{});
     if (hs.lights.empty()) { DLight z; std::memset(&z, 0, sizeof z); hs.lights_storage_pad = 1; hs.lights.push_back(z); }
     if (hs.materials.empty()) { DMaterial z; std::memset(&z, 0, sizeof z); hs.materials.push_back(z); }
@@ -691,11 +725,11 @@ struct Decoder {
 
 }  // namespace
 
-int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err) {
+int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err, bool device_blas) {
   try {
     if (layout != 1 && layout != 2) throw Fail{DFC_E_INVALID_ARG, "layout_version must be 1 or 2"};
     HostScene hs;
-    Decoder d(st, layout, hs);
+    Decoder d(st, layout, hs, device_blas);
     d.run();
     // the triangle records go to the device as they are: take them over
     auto tri = st.f32.find("shape3FTriangle3FArray");

@@ -39,12 +39,23 @@ struct HostScene {
   int lights_storage_pad = 0;  // 1 when `lights` holds only a placeholder
   int64_t triangles = 0;
   bool record_shapes = false;  // any disk, cylinder, cone, paraboloid, hyperboloid, cuboid or torus primitive
+  float blas_ms = 0.0f, tlas_ms = 0.0f;  // host time of the bottom- and top-level builds
+  // Bottom levels built on the device (dfc_blas.cu) instead of here: the node
+  // array then starts with a region of `blas_nodes` nodes the device builds
+  // fill (the host nodes follow it), and the triangle array of `blas_tris`
+  // triangles is written on the device as well.
+  struct BlasJob { size_t index_off; int count, node_base, node_cap, tri_first; };
+  std::vector<BlasJob> blas_jobs;
+  std::vector<int> blas_tri_index;  // per job: its triangles' indices in shape3FTriangle3FArray
+  int blas_nodes = 0;
+  int64_t blas_tris = 0;
   // Materials evaluated per hit (textures, modifiers, composite materials): the textured shading variants.
   bool textured() const { return !texmats.empty() || !composites.empty(); }
 };
 
 // Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.  On
 // success the triangle array is moved out of `st` into out->tri_attr.
-int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err);
+// With `device_blas`, mesh hierarchies are left to build_blas_device (upload_scene runs it).
+int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err, bool device_blas = false);
 
 }  // namespace dfc

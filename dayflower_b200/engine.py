@@ -131,6 +131,10 @@ class RenderEngine:
     def release_scene(self, scene_id: int):
         self._check(self._lib.dfc_engine_scene_release(self._h, int(scene_id)))
 
+    def set_bvh_builder(self, builder: int):
+        """Builder of the mesh hierarchies of later ``add_scene`` calls (0 host SAH, 1 device)."""
+        self._check(self._lib.dfc_engine_set_bvh_builder(self._h, int(builder)))
+
     # -- configuration -------------------------------------------------------------
     def configure(self, capacity=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, shade_threads=0, iterations_per_launch=0,
                   policy=SCHEDULE_ROUND_ROBIN, segment_paths=0, lookahead_paths=0, reserved=0):

@@ -244,3 +244,18 @@ class GPURenderer:
         out = np.zeros(5, dtype=np.float32)
         self._check(self._lib.dfc_read_stage_times(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return {"total": float(out[0]), "raygen": float(out[1]), "trace": float(out[2]), "shade": float(out[3]), "film": float(out[4])}
+
+    BVH_HOST, BVH_DEVICE = 0, 1
+
+    def setBVHBuilder(self, builder: int):
+        """Builder of the mesh hierarchies of later ``setScene`` calls: ``BVH_HOST`` (binned SAH on
+        the host) or ``BVH_DEVICE`` (built on the GPU from the uploaded triangles)."""
+        self._alive()
+        self._check(self._lib.dfc_set_bvh_builder(self._h, int(builder)))
+
+    def commitMillis(self):
+        """Host milliseconds of the last setScene commit: ingest (decode and builds), its bottom- and
+        top-level builds, and the upload."""
+        out = np.zeros(4, dtype=np.float32)
+        self._check(self._lib.dfc_read_commit_times(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        return {"ingest": float(out[0]), "blas": float(out[1]), "tlas": float(out[2]), "upload": float(out[3])}
