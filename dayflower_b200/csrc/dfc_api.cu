@@ -422,6 +422,7 @@ int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t c
 int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
   std::lock_guard<std::mutex> lk(r->mu);
+  RecycleOnExit recycle{r->staged};
   cudaSetDevice(r->device);
   HostScene hs;
   std::string err;
@@ -435,7 +436,6 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   DFC_CK(upload_scene(std::move(hs), r->stream, &r->scene), "scene upload");
   r->commit_ms[3] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
   r->have_scene = true;
-  r->staged = Staged();
   if (r->image_from_camera) {
     r->width = (int)r->scene.host.camera[17];
     r->height = (int)r->scene.host.camera[18];

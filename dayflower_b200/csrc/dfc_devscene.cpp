@@ -25,7 +25,7 @@ size_t tri_pos_count(const HostScene& hs) { return hs.blas_tris > 0 ? 3 * (size_
 size_t scene_device_bytes(const HostScene& hs) {
   return vbytes(hs.prims) + vbytes(hs.materials) + vbytes(hs.lights) + node_count(hs) * sizeof(BVH4Node) + vbytes(hs.tlas_items) +
          vbytes(hs.tlas_bound) + vbytes(hs.unbounded.empty() ? hs.unbounded_storage : hs.unbounded) + tri_pos_count(hs) * sizeof(F4) +
-         vbytes(hs.tri_attr) + vbytes(hs.rects) + vbytes(hs.shapes) + vbytes(hs.perez) + 19 * sizeof(float) +
+         hs.tri_attr_count * sizeof(float) + vbytes(hs.rects) + vbytes(hs.shapes) + vbytes(hs.perez) + 19 * sizeof(float) +
          vbytes(hs.textures) + vbytes(hs.texels) + vbytes(hs.modifiers) + vbytes(hs.composites) + vbytes(hs.texmats);
 }
 
@@ -50,7 +50,8 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
   } else {
     DFC_PUT(tri_pos, hs.tri_pos);
   }
-  DFC_PUT(tri_attr, hs.tri_attr);
+  if (e == cudaSuccess) e = ds->tri_attr.ensure(hs.tri_attr_count * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ds->tri_attr.p, hs.tri_attr, hs.tri_attr_count * sizeof(float), cudaMemcpyHostToDevice, s);
   DFC_PUT(rects, hs.rects);
   DFC_PUT(shapes, hs.shapes);
   DFC_PUT(perez, hs.perez);
@@ -103,6 +104,7 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
   v.modifiers = ds->modifiers.as<DModifier>();
   v.composites = ds->composites.as<DComposite>();
   v.texmats = ds->texmats.as<DTexMaterial>();
+  hs.tri_attr = nullptr;  // points into the staging arrays, which the caller recycles next
   ds->host = std::move(hs);
   return cudaSuccess;
 }

@@ -827,11 +827,11 @@ int dfc_engine_set_bvh_builder(dfc_engine* e, int builder) {
 int dfc_engine_scene_commit(dfc_engine* e, int layout_version, int32_t* scene_id) {
   if (!e || !scene_id) return DFC_E_INVALID_ARG;
   std::lock_guard<std::mutex> c(e->commit_mu);
+  RecycleOnExit recycle{e->staged};
   cudaSetDevice(e->device);
   HostScene hs;
   std::string err;
   int rc = ingest_scene(e->staged, layout_version, &hs, &err, e->bvh_builder == DFC_BVH_DEVICE);
-  e->staged = Staged();
   if (rc != DFC_OK) return efail(e, rc, err);
   const size_t bytes = scene_device_bytes(hs);
   const int variant = hs.textured() ? 2 : hs.record_shapes ? 1 : 0;

@@ -731,10 +731,16 @@ int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err, bool 
     HostScene hs;
     Decoder d(st, layout, hs, device_blas);
     d.run();
-    // the triangle records go to the device as they are: take them over
+    // the triangle records go to the device as they are, from the staging array
+    static const float kNoTriangle[24] = {0};
     auto tri = st.f32.find("shape3FTriangle3FArray");
-    if (tri != st.f32.end()) hs.tri_attr = std::move(tri->second);
-    if (hs.tri_attr.empty()) hs.tri_attr.assign(24, 0.0f);
+    if (tri != st.f32.end() && !tri->second.empty()) {
+      hs.tri_attr = tri->second.data();
+      hs.tri_attr_count = tri->second.size();
+    } else {
+      hs.tri_attr = kNoTriangle;
+      hs.tri_attr_count = 24;
+    }
     *out = std::move(hs);
     return DFC_OK;
   } catch (const Fail& f) {

@@ -15,6 +15,18 @@ namespace dfc {
 struct Staged {
   std::map<std::string, std::vector<float>> f32;
   std::map<std::string, std::vector<int32_t>> i32;
+  // Empties every array but keeps its allocation, so that staging the next
+  // scene of a similar size copies into memory that is already mapped.
+  void recycle() {
+    for (auto& kv : f32) kv.second.clear();
+    for (auto& kv : i32) kv.second.clear();
+  }
+};
+
+// Recycles the staging arrays when a commit ends, on every path (they are read until the upload is done).
+struct RecycleOnExit {
+  Staged& st;
+  ~RecycleOnExit() { st.recycle(); }
 };
 
 struct HostScene {
@@ -27,7 +39,11 @@ struct HostScene {
   std::vector<int> unbounded;
   std::vector<int> unbounded_storage;  // non-empty stand-in when there are no unbounded primitives
   std::vector<F4> tri_pos;
-  std::vector<float> tri_attr, rects, perez;
+  std::vector<float> rects, perez;
+  // shape3FTriangle3FArray as staged (not copied): valid until the staging arrays are recycled,
+  // which happens after the upload
+  const float* tri_attr = nullptr;
+  size_t tri_attr_count = 0;
   std::vector<float> shapes;  // pool of the record-sized shapes (disk ... torus), DPrim.data = float offset
   std::vector<DTexture> textures;      // texture nodes of the kMatTextured materials
   std::vector<unsigned> texels;        // their images (and normal-map modifier images), packed ARGB
@@ -54,7 +70,7 @@ struct HostScene {
 };
 
 // Decodes the staged arrays (layout 1 or 2).  Returns a dfc_status.  On
-// success the triangle array is moved out of `st` into out->tri_attr.
+// success out->tri_attr points into `st`, which must outlive the upload.
 // With `device_blas`, mesh hierarchies are left to build_blas_device (upload_scene runs it).
 int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err, bool device_blas = false);
 
