@@ -96,6 +96,7 @@ class GPURenderer:
             self._check(self._lib.dfc_scene_put(self._h, name.encode(), a.ctypes.data_as(ctypes.c_void_p), a.size, typ))
         self._check(self._lib.dfc_scene_commit(self._h, int(layout_version or cs.layout_version)))
         self._scene = cs
+        self._scene_version = getattr(cs, "version", 0)
         cam = cs.arrays["cameraArray"]
         self._width, self._height = int(cam[17]), int(cam[18])
         self._check(self._lib.dfc_set_image(self._h, self._width, self._height))
@@ -145,6 +146,11 @@ class GPURenderer:
         """``render()`` / ``render(int)``: True if every pass completed."""
         self._alive()
         n = 1 if render_passes is None else int(render_passes)
+        cs = self._scene
+        if cs is not None and getattr(cs, "version", 0) != getattr(self, "_scene_version", 0):
+            # AbstractGPURenderer.render: a compiled scene changed by a CompiledSceneModifier is uploaded again and the film cleared
+            self.setScene(cs)
+            self.setup()
         done = ctypes.c_int(0)
         rc = self._lib.dfc_render(self._h, n, ctypes.byref(done))
         self._render_pass += done.value
