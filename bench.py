@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=1024)
     ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--bvh-builder", default="device", choices=["device", "host"],
+                    help="mesh hierarchy builder of the scene commits (device: built on the GPU; host: binned SAH)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and served job-mix measurements")
@@ -367,6 +369,8 @@ def main():
     compiled = build_scene(args.cells)
     W, H = CONFIG["resolution"]
     r = GPURenderer(device=local)
+    builder = GPURenderer.BVH_DEVICE if args.bvh_builder == "device" else GPURenderer.BVH_HOST
+    r.setBVHBuilder(builder)
     r.setScene(compiled)
     r.setRenderingAlgorithm(RenderingAlgorithm.PATH_TRACING)
     r.setMaximumBounce(CONFIG["max_bounce"])
@@ -417,6 +421,7 @@ def main():
     if not args.no_e2e:
         h2d = compiled.nbytes()
         q = GPURenderer(device=local)
+        q.setBVHBuilder(builder)
         q.setRenderingAlgorithm(RenderingAlgorithm.PATH_TRACING)
         q.setMaximumBounce(CONFIG["max_bounce"])
         q.setMinimumBounceRussianRoulette(CONFIG["min_rr"])
@@ -450,7 +455,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp),
+            "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp, bvh_builder=args.bvh_builder),
             "rays_per_s": rays_all / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
