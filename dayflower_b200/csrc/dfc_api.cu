@@ -53,6 +53,7 @@ struct dfc_renderer {
   DevBuf d_film_consts;  // Gaussian film: filter table, sRGB -> XYZ, XYZ -> sRGB
   DevBuf d_beta, d_rad, d_meta, d_ray_o, d_ray_d, d_hits, d_pend_s, d_pend_m;
   DevBuf d_ray_list[2], d_work_list[2], d_counts, d_overflow, d_ray_total;
+  DevBuf d_ray_mask;  // path tracing: each path's new rays of the last shading step (k_ray_list_ordered)
   DevBuf d_sort_keys, d_sort_bins, d_sorted;
   DevBuf d_ao_o, d_ao_d, d_ao_v;
   int64_t pass = 0, total_paths = 0, launches = 0;
@@ -174,6 +175,8 @@ int alloc_wavefront(dfc_renderer* r) {
   DFC_CK(r->d_ray_total.ensure(16), "counters");
   DFC_CK(r->d_sort_keys.ensure(P), "sort");
   DFC_CK(r->d_sorted.ensure(P * 4), "sort");
+  DFC_CK(r->d_ray_mask.ensure(P), "ray mask");
+  DFC_CK(cudaMemset(r->d_ray_mask.p, 0, P), "ray mask");
   if (r->film_filter == 1) {
     const std::vector<float> c = pixel_film_constants();
     DFC_CK(r->d_film_consts.ensure(c.size() * sizeof(float)), "film");
@@ -308,10 +311,16 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
       a.work_list = so.sorted;
+      a.ray_mask = r->d_ray_mask.as<unsigned char>();
       (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
           <<<shade_grid, 256, 0, r->stream>>>(a);
-      stage_end(r, ev);
       r->launches += 4;
+      if (s < steps - 1) {  // the next step's ray list, in path order
+        k_ray_list_ordered<<<(r->paths + kRayListBlock - 1) / kRayListBlock, kRayListBlock, 0, r->stream>>>(
+            a.ray_mask, r->paths, a.next_ray_list, a.next_ray_count);
+        r->launches += 1;
+      }
+      stage_end(r, ev);
     }
   } else if (algo == DFC_RAY_TRACING) {
     ShadeArgs a = shade_args(r, 0);

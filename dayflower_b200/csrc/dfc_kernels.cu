@@ -800,12 +800,17 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
       a.meta[p] = make_uint4(meta.x, meta.y, ((unsigned)bounce & 0xffffu) | ((unsigned)dimb << 16), flags);
     }
     // appends (all lanes of the warp take part)
-    const unsigned r0 = warp_append(a.next_ray_count, spawn_ext);
-    if (spawn_ext) a.next_ray_list[r0] = p << 3;
-    const unsigned r1 = warp_append(a.next_ray_count, spawn_shadow);
-    if (spawn_shadow) a.next_ray_list[r1] = (p << 3) | (shadow_any ? 4u : 0u) | 1u;
-    const unsigned r2 = warp_append(a.next_ray_count, spawn_mis);
-    if (spawn_mis) a.next_ray_list[r2] = (p << 3) | 2u;
+    if (!kMulti && a.ray_mask) {
+      // rays listed later in path order (k_ray_list_ordered): pixel-coherent traversal batches
+      if (i < n) a.ray_mask[p] = (unsigned char)((spawn_ext ? 1u : 0u) | (spawn_shadow ? 2u : 0u) | (spawn_mis ? 4u : 0u) | (shadow_any ? 8u : 0u));
+    } else {
+      const unsigned r0 = warp_append(a.next_ray_count, spawn_ext);
+      if (spawn_ext) a.next_ray_list[r0] = p << 3;
+      const unsigned r1 = warp_append(a.next_ray_count, spawn_shadow);
+      if (spawn_shadow) a.next_ray_list[r1] = (p << 3) | (shadow_any ? 4u : 0u) | 1u;
+      const unsigned r2 = warp_append(a.next_ray_count, spawn_mis);
+      if (spawn_mis) a.next_ray_list[r2] = (p << 3) | 2u;
+    }
     const unsigned w = warp_append(a.next_work_count, keep);
     if (keep) a.next_work_list[w] = p;
     if constexpr (kMulti) {
@@ -819,6 +824,37 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
       if (lane == 0 && rmask) atomicAdd(&a.state->retired, (unsigned long long)__popc(rmask));
     }
   }
+}
+
+// One block per kRayListBlock consecutive paths: each thread counts its
+// path's rays, a block scan places them, one atomic reserves the block's run.
+// Within a run the rays are in path (pixel) order, so the traversal's warps
+// fetch neighbouring pixels' rays together.
+__global__ void __launch_bounds__(kRayListBlock) k_ray_list_ordered(const unsigned char* ray_mask, unsigned paths, unsigned* ray_list,
+                                                                     unsigned* ray_count) {
+  __shared__ unsigned warp_sum[kRayListBlock / 32];
+  __shared__ unsigned block_base;
+  const unsigned p = blockIdx.x * kRayListBlock + threadIdx.x;
+  const unsigned m = p < paths ? (unsigned)ray_mask[p] : 0u;
+  const unsigned c = __popc(m & 7u);
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned incl = c;  // inclusive warp scan
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+    if ((int)lane >= o) incl += v;
+  }
+  if (lane == 31u) warp_sum[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int w = 0; w < kRayListBlock / 32; ++w) { const unsigned t = warp_sum[w]; warp_sum[w] = acc; acc += t; }
+    block_base = acc ? atomicAdd(ray_count, acc) : 0u;
+  }
+  __syncthreads();
+  unsigned at = block_base + warp_sum[warp] + incl - c;
+  if (m & 1u) ray_list[at++] = p << 3;
+  if (m & 2u) ray_list[at++] = (p << 3) | ((m & 8u) ? 4u : 0u) | 1u;
+  if (m & 4u) ray_list[at] = (p << 3) | 2u;
 }
 
 // At most 256 threads a block, two blocks per SM: the shading kernels fit in

@@ -112,6 +112,10 @@ struct ShadeArgs {
   unsigned* next_work_count;
   unsigned* next_ray_list;
   unsigned* next_ray_count;
+  // When set (per-job renderer), shading records each path's new rays here
+  // (bit 0 extension, 1 shadow, 2 MIS, 3 shadow is any-hit) instead of
+  // appending them, and k_ray_list_ordered builds the next ray list in path order.
+  unsigned char* ray_mask;
   float4* beta;
   float4* radiance;
   uint4* meta;
@@ -206,6 +210,10 @@ __global__ void k_shade_path_batch_records(ShadeArgs a);
 __global__ void k_shade_path_textured(ShadeArgs a);
 __global__ void k_shade_path_batch_textured(ShadeArgs a);
 __global__ void k_shade_primary(ShadeArgs a, int algorithm);
+// The next step's ray list from ShadeArgs::ray_mask, paths in index order
+// within each block of kRayListBlock paths.
+constexpr int kRayListBlock = 256;
+__global__ void k_ray_list_ordered(const unsigned char* ray_mask, unsigned paths, unsigned* ray_list, unsigned* ray_count);
 __global__ void k_trace_ao(AoArgs a);
 // RAY_TRACING (scene/Scene.java:786 doRadianceRayTracer): one thread per camera
 // sample walks the sample's specular reflection/transmission tree depth first.
