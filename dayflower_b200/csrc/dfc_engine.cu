@@ -44,6 +44,8 @@ using namespace dfc;
 namespace {
 
 constexpr int kMaxScenes = 64;
+static_assert(kJobPathTracing == DFC_JOB_PATH_TRACING && kJobRayCasting == DFC_JOB_RAY_CASTING && kJobDepthCamera == DFC_JOB_DEPTH_CAMERA,
+              "job kinds of the kernels and of the C ABI");
 constexpr unsigned kJobRing = 4096;    // job records on the device (power of two)
 constexpr unsigned kSegRing = 65536;   // segment records on the device (power of two)
 constexpr int64_t kDefaultCapacity = int64_t(1) << 20;
@@ -457,6 +459,7 @@ int service(dfc_engine* e, bool idle_device) {
     dj.max_bounce = J.d.maximum_bounce;
     dj.min_rr = J.d.minimum_bounce_russian_roulette;
     dj.seed = J.d.seed;
+    dj.kind = J.d.kind;
     dj.cancelled = 0;
     dj.film_sum = static_cast<float4*>(film);
     dj.film_sq = static_cast<float4*>(film) + pixels;
@@ -906,6 +909,8 @@ int dfc_job_submit(dfc_engine* e, const dfc_job_desc* d, int64_t* job_id) {
   if (d->samples < 1) return efail(e, DFC_E_INVALID_ARG, "renderPasses < 1");  // AbstractGPURenderer.java:323
   if (d->maximum_bounce < 0 || d->maximum_bounce > 4096) return efail(e, DFC_E_INVALID_ARG, "maximumBounce out of range");
   if (d->minimum_bounce_russian_roulette < 0) return efail(e, DFC_E_INVALID_ARG, "minimumBounceRussianRoulette out of range");
+  if (d->kind != DFC_JOB_PATH_TRACING && d->kind != DFC_JOB_RAY_CASTING && d->kind != DFC_JOB_DEPTH_CAMERA)
+    return efail(e, DFC_E_UNSUPPORTED, "engine jobs are PATH_TRACING, RAY_CASTING or DEPTH_CAMERA");
   const int64_t id = e->next_id++;
   JobRec J;
   J.d = *d;

@@ -666,7 +666,25 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
         const bool spec = (flags & kFlagSpecular) != 0u;
         const bool rec = !kMulti && a.record_primary && bounce == 0 && dimb == 0 && p < a.pixels;
         if (rec && hp < 0) { a.primary_prim[p] = -1; a.primary_t[p] = __int_as_float(0x7fc00000); }
-        if (hp < 0) {
+        if (kMulti && J->kind != kJobPathTracing) {
+          // ray-casting and depth-camera jobs of the engine end at their camera ray, shaded as k_shade_primary does
+          if (hp < 0) {
+            if (J->kind == kJobRayCasting)
+              for (int k = 0; k < S.light_count; ++k) L = L + light_Le_miss(S, S.lights[k], ray_d);  // Scene.java:675
+          } else {
+            Surface sf;
+            surface_of<kRecords>(S, S.prims[hp], __float_as_int(h.z), ray_o, ray_d, h.w, &sf);
+            if (J->kind == kJobRayCasting) {
+              const float c = fabsf(dot(sf.s.w, ray_d)) * 0.5f;
+              L = V3{c, c, c};
+            } else {  // Scene.java:327 radianceDepthCamera
+              const V3 dd = sf.p - ray_o;
+              const float in = clampf(1.0f / (dot(dd, dd) * 0.5f), 0.0f, 1.0f);
+              L = V3{in, in, in};
+            }
+          }
+          alive = false;
+        } else if (hp < 0) {
           if (bounce == 0 && !kMulti && a.preview) L = {1, 1, 1};
           else if (bounce == 0 || spec) {
             for (int k = 0; k < S.light_count; ++k) L = L + mul(beta, light_Le_miss(S, S.lights[k], ray_d));

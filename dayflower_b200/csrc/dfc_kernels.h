@@ -8,6 +8,8 @@
 namespace dfc {
 
 enum { DFC_ALGO_AO = 0, DFC_ALGO_DEPTH = 1, DFC_ALGO_PATH = 2, DFC_ALGO_RAY_CASTING = 3, DFC_ALGO_RAY_TRACING = 4 };
+// DJob::kind (the C ABI's DFC_JOB_* values)
+enum : int { kJobPathTracing = 0, kJobRayCasting = 1, kJobDepthCamera = 2 };
 
 // Path flags (PathMeta.w)
 enum : unsigned { kFlagAlive = 1u, kFlagSpecular = 2u, kFlagPendShadow = 4u, kFlagPendMis = 8u, kFlagShadowAny = 16u, kFlagNoSample = 32u };
@@ -22,6 +24,7 @@ struct DJob {
   unsigned width, pixels;
   int max_bounce, min_rr;
   uint32_t seed;
+  int kind;                  // kJobPathTracing, kJobRayCasting or kJobDepthCamera
   unsigned cancelled;        // 1: start no more paths of this job (the plan skips them)
   float4* film_sum;          // per pixel: sum of accepted samples (xyz), count (w)
   float4* film_sq;           // per pixel: sum of squares (xyz)

@@ -36,7 +36,10 @@ JOB_STATE_NAMES = {JOB_QUEUED: "queued", JOB_RUNNING: "running", JOB_DONE: "done
 class JobDesc(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_int32), ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("samples", ctypes.c_int32),
                 ("maximum_bounce", ctypes.c_int32), ("minimum_bounce_russian_roulette", ctypes.c_int32),
-                ("seed", ctypes.c_uint32), ("reserved", ctypes.c_int32)]
+                ("seed", ctypes.c_uint32), ("kind", ctypes.c_int32)]
+
+
+JOB_PATH_TRACING, JOB_RAY_CASTING, JOB_DEPTH_CAMERA = 0, 1, 2
 
 
 class JobInfo(ctypes.Structure):
@@ -159,14 +162,15 @@ class RenderEngine:
 
     # -- jobs ----------------------------------------------------------------------
     @staticmethod
-    def _desc(scene, width, height, samples, maximum_bounce=20, minimum_bounce_russian_roulette=5, seed=0x5EED1234):
+    def _desc(scene, width, height, samples, maximum_bounce=20, minimum_bounce_russian_roulette=5, seed=0x5EED1234,
+              kind=JOB_PATH_TRACING):
         return JobDesc(int(scene), int(width), int(height), int(samples), int(maximum_bounce), int(minimum_bounce_russian_roulette),
-                       int(seed) & 0xFFFFFFFF, 0)
+                       int(seed) & 0xFFFFFFFF, int(kind))
 
     def submit(self, scene: int, width: int, height: int, samples: int, maximum_bounce: int = 20,
-               minimum_bounce_russian_roulette: int = 5, seed: int = 0x5EED1234) -> int:
-        """Queues a PATH_TRACING job; returns its id."""
-        d = self._desc(scene, width, height, samples, maximum_bounce, minimum_bounce_russian_roulette, seed)
+               minimum_bounce_russian_roulette: int = 5, seed: int = 0x5EED1234, kind: int = JOB_PATH_TRACING) -> int:
+        """Queues a job (PATH_TRACING, or RAY_CASTING / DEPTH_CAMERA with ``kind``); returns its id."""
+        d = self._desc(scene, width, height, samples, maximum_bounce, minimum_bounce_russian_roulette, seed, kind)
         jid = ctypes.c_int64(0)
         self._check(self._lib.dfc_job_submit(self._h, ctypes.byref(d), ctypes.byref(jid)))
         self._jobs[int(jid.value)] = (int(width), int(height))

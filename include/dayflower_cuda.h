@@ -253,8 +253,17 @@ typedef struct dfc_job_desc {
   int32_t maximum_bounce;                   /* setMaximumBounce */
   int32_t minimum_bounce_russian_roulette;  /* setMinimumBounceRussianRoulette */
   uint32_t seed;                            /* seed of the counter-based random numbers (dfc_set_seed) */
-  int32_t reserved;                         /* 0 */
+  int32_t kind;                             /* DFC_JOB_PATH_TRACING (0), DFC_JOB_RAY_CASTING or DFC_JOB_DEPTH_CAMERA */
 } dfc_job_desc;
+
+/* Rendering algorithm of an engine job (dfc_job_desc.kind): PATH_TRACING, or
+ * the one-step RAY_CASTING and DEPTH_CAMERA of setRenderingAlgorithm
+ * (renderer/gpu/AbstractGPURenderer.java:504), shaded as the per-job renderer
+ * shades them.  AMBIENT_OCCLUSION and RAY_TRACING jobs run on a per-job
+ * renderer (DFC_E_UNSUPPORTED here). */
+#define DFC_JOB_PATH_TRACING 0
+#define DFC_JOB_RAY_CASTING 1
+#define DFC_JOB_DEPTH_CAMERA 2
 
 typedef struct dfc_job_info {
   int32_t state;                 /* DFC_JOB_* */

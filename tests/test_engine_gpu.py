@@ -75,6 +75,27 @@ def test_engine_job_matches_per_job_renderer(engine, scenes, name):
     films_close(f, (g["sum"], g["sumsq"], g["count"]))
 
 
+@pytest.mark.parametrize("name", ["cornell", "mixed", "quadrics"])
+@pytest.mark.parametrize("kind,algorithm", [(1, RA.RAY_CASTING), (2, RA.DEPTH_CAMERA)])
+def test_engine_one_step_jobs_match_per_job_renderer(engine, scenes, name, kind, algorithm):
+    # RAY_CASTING and DEPTH_CAMERA jobs end at their camera ray; each sample is the per-job renderer's
+    from dayflower_b200.engine import JOB_DEPTH_CAMERA, JOB_RAY_CASTING
+    assert (JOB_RAY_CASTING, JOB_DEPTH_CAMERA) == (1, 2)
+    e, ids = engine
+    cs = scenes[name]
+    w, h = res_of(cs)
+    g = PT.render_gpu(cs, algorithm, spp=3, seed=91)
+    others = [e.submit(ids["terrain"], 32, 24, 2, maximum_bounce=4, seed=5)]  # shares the wavefront with a path-traced job
+    j = e.submit(ids[name], w, h, 3, seed=91, kind=kind)
+    e.run(timeout_s=120)
+    assert e.info(j)["state"] == "done"
+    f = e.film(j)
+    e.release(j)
+    for o in others:
+        e.release(o)
+    films_close(f, (g["sum"], g["sumsq"], g["count"]))
+
+
 def test_engine_job_same_alone_and_in_mix(engine, scenes):
     e, ids = engine
     w, h = res_of(scenes["cornell"])
@@ -198,3 +219,6 @@ def test_engine_rejects_bad_jobs(engine):
         e.submit(ids["cornell"], 0, 8, 1)
     with pytest.raises(ValueError):
         e.submit(ids["cornell"], 8, 8, 0)
+    from dayflower_b200.renderer import UnsupportedSceneError
+    with pytest.raises(UnsupportedSceneError):
+        e.submit(ids["cornell"], 8, 8, 1, kind=3)  # AMBIENT_OCCLUSION / RAY_TRACING run on a per-job renderer
