@@ -176,7 +176,7 @@ int alloc_wavefront(dfc_renderer* r) {
   DFC_CK(r->d_sort_keys.ensure(P), "sort");
   DFC_CK(r->d_sorted.ensure(P * 4), "sort");
   DFC_CK(r->d_ray_mask.ensure(P), "ray mask");
-  DFC_CK(cudaMemset(r->d_ray_mask.p, 0, P), "ray mask");
+  DFC_CK(cudaMemsetAsync(r->d_ray_mask.p, 0, P, r->stream), "ray mask");
   if (r->film_filter == 1) {
     const std::vector<float> c = pixel_film_constants();
     DFC_CK(r->d_film_consts.ensure(c.size() * sizeof(float)), "film");
@@ -239,6 +239,9 @@ ShadeArgs shade_args(dfc_renderer* r, int step) {
 
 // The traversal kernel for the committed scene: the one with the disk ... torus
 // tests only when the scene has such primitives.
+// Passes with at least this many paths list each step's rays in path order (k_ray_list_ordered).
+constexpr unsigned kOrderedRayListMinPaths = 1u << 18;
+
 using TraceKernel = void (*)(TraceArgs);
 TraceKernel trace_kernel(const dfc_renderer* r) { return r->scene.host.record_shapes ? k_trace_records : k_trace; }
 
@@ -311,11 +314,12 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
       a.work_list = so.sorted;
-      a.ray_mask = r->d_ray_mask.as<unsigned char>();
+      // path-ordered ray lists pay for their extra launch only on large passes; small ones stay launch-bound
+      a.ray_mask = r->paths >= kOrderedRayListMinPaths ? r->d_ray_mask.as<unsigned char>() : nullptr;
       (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
           <<<shade_grid, 256, 0, r->stream>>>(a);
       r->launches += 4;
-      if (s < steps - 1) {  // the next step's ray list, in path order
+      if (a.ray_mask && s < steps - 1) {  // the next step's ray list, in path order
         k_ray_list_ordered<<<(r->paths + kRayListBlock - 1) / kRayListBlock, kRayListBlock, 0, r->stream>>>(
             a.ray_mask, r->paths, a.next_ray_list, a.next_ray_count);
         r->launches += 1;
