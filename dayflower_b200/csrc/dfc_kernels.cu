@@ -400,7 +400,7 @@ constexpr int kRefill = 8;        // refill a warp's idle lanes once this many a
 #define DFC_NODE_STEPS 8
 #endif
 #ifndef DFC_SPECULATE
-#define DFC_SPECULATE 1
+#define DFC_SPECULATE 0  // speculative node steps measured 1.1% slower on the benchmark scene
 #endif
 constexpr int kNodeSteps = DFC_NODE_STEPS;  // bound of one node phase (the warp then tests its leaves and refills)
 constexpr bool kSpeculate = DFC_SPECULATE != 0;  // lanes holding a leaf keep walking interior nodes
