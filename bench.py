@@ -50,7 +50,7 @@ TRACE_RECORD_BYTES = 52
 # DRAM bytes (read + write) per traced ray of k_trace from an ncu capture of
 # one whole path-tracing pass of this workload at 1 spp; scaled to a launch by
 # its rays.
-TRACE_DRAM_BYTES_PER_RAY = 198.0
+TRACE_DRAM_BYTES_PER_RAY = 163.0
 TRACE_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum over one whole 1-spp pass, profiles/k_trace_terrain_spheres_1080p_1spp.md"
 
 
