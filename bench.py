@@ -455,7 +455,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp, bvh_builder=args.bvh_builder),
+            "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp), "bvh_builder": args.bvh_builder,
             "rays_per_s": rays_all / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
