@@ -47,11 +47,22 @@ CONFIG = {"workload": "terrain_2.1M_tris+2000_spheres_perez_1920x1080_pt64spp_bo
 # and direction records (2 x 16 B), hit record (16 B).  BVH node and triangle
 # fetches are data-dependent and not counted.
 TRACE_RECORD_BYTES = 52
-# DRAM bytes (read + write) per traced ray of k_trace from an ncu capture of
-# one whole path-tracing pass of this workload at 1 spp; scaled to a launch by
-# its rays.
+# Traversal is bound by instruction issue, not by HBM: its roofline is the
+# fraction of the SMs' issue slots (4 warp instructions per SM per cycle) it
+# uses.  Warp instructions per traced ray and DRAM bytes per traced ray come
+# from an ncu capture of one whole 1-spp pass of this workload (the small case
+# of the same scene, camera and rays); the bench scales them by the rays each
+# launch traced and divides by the launch times it measures with CUDA events.
+TRACE_WARP_INST_PER_RAY = 502.0
 TRACE_DRAM_BYTES_PER_RAY = 163.0
-TRACE_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum over one whole 1-spp pass, profiles/k_trace_terrain_spheres_1080p_1spp.md"
+TRACE_PROFILE = "profiles/k_trace_terrain_spheres_1080p_1spp.md"
+ISSUE_SLOTS_PER_SM_CYCLE = 4
+# Algorithmic bytes per item of the queue stages (fixed record sizes):
+#   k_raygen            per path: state 48 (beta, radiance, meta) + ray 32 + list entries 8
+#   k_sort_count        per work item: list entry 4 + meta 16 + hit 16 + key 1
+#   k_sort_scatter      per work item: key 1 + list entry 4 + sorted entry 4
+#   k_ray_list_ordered  per path scanned: mask 1; per ray listed: entry 4
+QUEUE_BYTES = {"raygen": 88, "sort_count": 37, "sort_scatter": 9}
 
 
 def parse():
@@ -72,10 +83,11 @@ def parse():
                     help="run only the batched job mix (per-job arm and engine arm) and print its JSON object")
     ap.add_argument("--engine-only", action="store_true", help="with --batch-only: skip the per-job arm and the served sweep")
     ap.add_argument("--no-autotune", action="store_true", help="engine arm with the default wavefront shape")
-    ap.add_argument("--large", action="store_true",
-                    help="also render the large scene (10M-triangle terrain, 50k blob instances, 4096x2048 image light, 3840x2160, 256 spp)")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large scene (10M-triangle terrain, 50k blob instances, 4096x2048 image light, 3840x2160)")
     ap.add_argument("--large-only", action="store_true", help="render only the large scene and print its JSON object")
-    ap.add_argument("--large-spp", type=int, default=256)
+    ap.add_argument("--large-spp", type=int, default=16,
+                    help="samples per pixel of the large scene (its stated workload is 256; the default run takes 16 to stay within minutes)")
     return ap.parse_args()
 
 
@@ -151,19 +163,37 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(compiled, spp_sample=1, rows=12, threads=None):
-    """Times the oracle (CPU restatement of CPURenderer) on a bounded row sample."""
+# The CPU sample: rows spread evenly over the whole image (every ROW_STRIDE-th
+# row from row ROW_OFFSET), 1 sample per pixel of the same job, so that its
+# mix of sky, terrain and sphere pixels is the image's own.  The 1-thread
+# figure uses every third row of that sample.
+ROW_STRIDE, ROW_OFFSET = 36, 18
+
+
+def cpu_baseline(compiled, threads=None, stride=ROW_STRIDE, offset=ROW_OFFSET):
+    """Times the oracle (the CPU restatement of CPURenderer) on a strided row sample of the job."""
     from oracle import dfo
     threads = threads or os.cpu_count() or 1
     o = dfo.OracleScene(compiled)
-    H = o.height
-    r0 = H // 2 - rows // 2
+    rows = len(range(offset, o.height, stride))
     t0 = time.perf_counter()
-    res = o.render(2, spp=spp_sample, max_bounce=CONFIG["max_bounce"], min_rr=CONFIG["min_rr"], rows=(r0, r0 + rows), threads=threads)
+    res = o.render(2, spp=1, max_bounce=CONFIG["max_bounce"], min_rr=CONFIG["min_rr"], rows=(offset, o.height), row_step=stride,
+                   threads=threads)
     dt = time.perf_counter() - t0
-    paths = o.width * rows * spp_sample
-    return {"value": paths / dt, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": "%d rows x %d px x %d spp of the same job (%d paths, %.1f s, %d rays)" % (rows, o.width, spp_sample, paths, dt, res["rays"])}
+    paths = o.width * rows
+    return {"value": paths / dt, "unit": METRIC, "cores": threads, "kind": "port", "rays_per_s": res["rays"] / dt,
+            "seconds": dt, "paths": paths, "rays": res["rays"],
+            "sample": "%d rows (every %dth from row %d) x %d px x 1 spp of the same job: %d paths, %d rays, %.1f s on %d threads"
+                      % (rows, stride, offset, o.width, paths, res["rays"], dt, threads)}
+
+
+def cpu_baselines(compiled):
+    """All host threads on the strided sample, and one thread on every third row of it
+    (the reference CPURenderer renders on one thread, AbstractCPURenderer.java:215-246)."""
+    b = cpu_baseline(compiled)
+    one = cpu_baseline(compiled, threads=1, stride=3 * ROW_STRIDE)
+    b["one_thread"] = {k: one[k] for k in ("value", "rays_per_s", "seconds", "paths", "rays", "sample")}
+    return b
 
 
 def batched_and_served(args, device=0):
@@ -326,19 +356,26 @@ def large_scene_run(args, device=0):
 
 
 def run_reference(args, rank):
+    """The reference arm: the CPU restatement of CPURenderer on all host threads.
+    One step is the strided row sample of the job (the same sample as the
+    cpu_baseline of the GPU arm); value = its paths over its time."""
     if rank != 0:
         return
     compiled = build_scene(args.cells)
     res = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(compiled, rows=24)
+        r = cpu_baseline(compiled)
         if i >= args.warmup:
             res.append(r)
-    v = statistics.median(x["value"] for x in res)
+    paths = sum(x["paths"] for x in res)
+    secs = sum(x["seconds"] for x in res)
+    v = paths / secs
     line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * CONFIG["resolution"][0] * CONFIG["resolution"][1] * args.spp / v, "higher_is_better": True,
+            "ms_per_step": 1000.0 * secs / len(res), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG, "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": METRIC, "cores": res[0]["cores"], "kind": "port", "sample": res[0]["sample"]},
+            "rays_per_s": sum(x["rays"] for x in res) / secs,
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": res[0]["cores"], "kind": "port", "sample": res[0]["sample"],
+                             "step": "one step = the row sample above (not the whole 64-spp job)"},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -397,13 +434,16 @@ def main():
     ms = []
     rays = 0
     launches = 0
-    trace_ms = 0.0
+    kstats = {}
     for _ in range(args.steps):
         ms.append(step())
         c = r.getCounters()
         rays += c["rays"]
         launches += c["launches"]
-        trace_ms += r.stageMillis()["trace"]
+        for k, v in r.kernelStats().items():  # per kernel kind: device ms, launches (this call), items (since clear)
+            a = kstats.setdefault(k, {"ms": 0.0, "launches": 0, "items": 0})
+            for f in a:
+                a[f] += v[f]
     torch.cuda.synchronize()
     clk = clocks.stop()
     paths_per_step = W * H * args.spp
@@ -448,31 +488,57 @@ def main():
 
     if rank == 0:
         peak, peak_kind = peaks()
-        trace_launches = args.steps * args.spp * (CONFIG["max_bounce"] + 4)
-        rays_per_launch = rays / trace_launches
-        launch_ms = trace_ms / trace_launches
-        achieved = rays_per_launch * TRACE_RECORD_BYTES / (launch_ms / 1000.0) / 1e9
+        tr = kstats["trace"]
+        rays_per_launch = tr["items"] / tr["launches"]
+        launch_ms = tr["ms"] / tr["launches"]
+        hbm_achieved = rays_per_launch * TRACE_RECORD_BYTES / (launch_ms / 1000.0) / 1e9
+        # issue-slot roofline of the traversal at the SM clock measured during the timed steps
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        f_hz = (clk["sm_mhz"] or 1965.0) * 1e6
+        issue_peak = ISSUE_SLOTS_PER_SM_CYCLE * sms * f_hz / 1e9
+        issue_achieved = rays_per_launch * TRACE_WARP_INST_PER_RAY / (launch_ms / 1000.0) / 1e9
+
+        def queue(name, nbytes):
+            k = kstats[name]
+            if not k["launches"] or k["ms"] <= 0.0:
+                return None
+            gbs = nbytes / (k["ms"] / 1000.0) / 1e9
+            return {"achieved": gbs, "unit": "GB/s", "frac": gbs / peak, "launches": k["launches"], "ms": k["ms"],
+                    "items": k["items"], "bytes": nbytes, "share": k["ms"] / total_ms}
+
+        rl = kstats["ray_list"]
+        stages = {n: queue(n, kstats[n]["items"] * QUEUE_BYTES[n]) for n in ("raygen", "sort_count", "sort_scatter")}
+        stages["ray_list"] = queue("ray_list", rl["launches"] * W * H + 4 * rl["items"])
+        stages["shade"] = {"ms": kstats["shade"]["ms"], "launches": kstats["shade"]["launches"], "items": kstats["shade"]["items"],
+                           "share": kstats["shade"]["ms"] / total_ms}
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded heightfield + spheres, no dataset)", "config": dict(CONFIG, spp=args.spp), "bvh_builder": args.bvh_builder,
             "rays_per_s": rays_all / (total_ms / 1000.0), "rays_per_path": rays / (paths_per_step * args.steps),
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None if TRACE_DRAM_BYTES_PER_RAY is None else rays_per_launch * TRACE_DRAM_BYTES_PER_RAY, "peak_kind": peak_kind,
-                         "kernel": "k_trace", "launches": trace_launches, "launch_ms": launch_ms, "rays_per_launch": rays_per_launch,
-                         "algorithmic_bytes_per_ray": TRACE_RECORD_BYTES, "trace_share": trace_ms / total_ms,
-                         "traffic_source": TRACE_TRAFFIC_SOURCE},
+            "roofline": {"bound": "issue", "kernel": "k_trace", "achieved": issue_achieved, "peak": issue_peak, "unit": "G warp-instructions/s",
+                         "frac": issue_achieved / issue_peak,
+                         "peak_kind": "%d issue slots x %d SMs x %.0f MHz (median SM clock of the timed steps)" % (ISSUE_SLOTS_PER_SM_CYCLE, sms, f_hz / 1e6),
+                         "warp_inst_per_ray": TRACE_WARP_INST_PER_RAY,
+                         "traffic": rays_per_launch * TRACE_DRAM_BYTES_PER_RAY,
+                         "traffic_source": "DRAM bytes per traced ray (%.0f) and warp instructions per ray from the ncu capture of one 1-spp pass "
+                                           "in %s, scaled by the rays of a launch; not measured in this run" % (TRACE_DRAM_BYTES_PER_RAY, TRACE_PROFILE),
+                         "hbm": {"achieved": hbm_achieved, "peak": peak, "unit": "GB/s", "frac": hbm_achieved / peak, "peak_kind": peak_kind,
+                                 "algorithmic_bytes_per_ray": TRACE_RECORD_BYTES},
+                         "launches": tr["launches"], "launch_ms": launch_ms, "rays_per_launch": rays_per_launch,
+                         "trace_share": tr["ms"] / total_ms},
+            "queue_stages": stages,
             "clocks": clk,
             "e2e": e2e,
         }
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(compiled, rows=144)
+            line["cpu_baseline"] = cpu_baselines(compiled)
     r.dispose()
     if rank == 0:
         if world == 1 and not args.no_batch:
             line["batched"], line["served"] = batched_and_served(args, local)
-        if world == 1 and args.large:
+        if world == 1 and not args.no_large:
             line["large"] = large_scene_run(args, local)
         print(json.dumps(line), flush=True)
     if world > 1:

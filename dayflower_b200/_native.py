@@ -35,6 +35,8 @@ SIGNATURES = [
     ("dfc_set_stage_timing", _c_int, [_c_p, _c_int]),
     ("dfc_setup", _c_int, [_c_p]),
     ("dfc_render", _c_int, [_c_p, _c_int, ctypes.POINTER(_c_int)]),
+    ("dfc_render_observed", _c_int, [_c_p, _c_int, _c_p, _c_p, ctypes.POINTER(_c_int)]),
+    ("dfc_read_kernel_stats", _c_int, [_c_p, _c_p, _c_p, _c_p, _c_int]),
     ("dfc_render_shutdown", _c_int, [_c_p]),
     ("dfc_clear", _c_int, [_c_p]),
     ("dfc_update_camera", _c_int, [_c_p, _c_p]),
@@ -72,6 +74,15 @@ SIGNATURES = [
     ("dfc_engine_stop", _c_int, [_c_p]),
     ("dfc_engine_get_stats", _c_int, [_c_p, _c_p]),
 ]
+
+
+class PassEvent(ctypes.Structure):
+    """``dfc_pass_event`` of ``dfc_render_observed``."""
+    _fields_ = [("event", _c_int), ("render_pass", _c_int), ("progress", ctypes.c_double), ("millis", ctypes.c_double),
+                ("rgba", ctypes.POINTER(ctypes.c_uint8)), ("width", _c_int), ("height", _c_int)]
+
+
+OBSERVER_FN = ctypes.CFUNCTYPE(None, _c_p, ctypes.POINTER(PassEvent))
 
 
 def load_renderer(build: bool = True) -> ctypes.CDLL:

@@ -57,7 +57,13 @@ struct dfc_renderer {
   DevBuf d_sort_keys, d_sort_bins, d_sorted;
   DevBuf d_ao_o, d_ao_d, d_ao_v;
   int64_t pass = 0, total_paths = 0, launches = 0;
-  float last_ms[5] = {0, 0, 0, 0, 0};
+  // device milliseconds and launches of the last render call: [0] whole call, then per kernel kind
+  // (DFC_KERNEL_*; filled while stage timing is on)
+  float last_ms[DFC_KERNEL_KINDS] = {};
+  int64_t last_launches[DFC_KERNEL_KINDS] = {};
+  // observed renders: pinned host copy of the RGBA8 image handed to the observer
+  uint8_t* h_rgba = nullptr;
+  size_t h_rgba_bytes = 0;
   float commit_ms[4] = {0, 0, 0, 0};  // last dfc_scene_commit: ingest, of which BLAS, TLAS builds; upload
   // optional per-stage timing: event pairs around every launch of a render call
   int stage_timing = 0;
@@ -73,25 +79,39 @@ int fail(dfc_renderer* r, int code, const std::string& msg) {
   if (r) r->err = msg;
   return code;
 }
+
+// The handle whose render observer this thread is running (dfc_render_observed
+// holds the handle's lock during the callback, so a call back into the same
+// handle is refused instead of deadlocking).
+thread_local const dfc_renderer* t_observing = nullptr;
 int cuda_fail(dfc_renderer* r, cudaError_t e, const char* what) {
   int code = (e == cudaErrorMemoryAllocation) ? DFC_E_OOM : DFC_E_CUDA;
   return fail(r, code, std::string(what) + ": " + cudaGetErrorString(e));
 }
+// Entry points that take the handle's lock.  A call from inside the handle's
+// own render observer (same thread, lock held) is refused.
+#define DFC_LOCK(r)                                                                                       \
+  if (t_observing == (r)) return fail((r), DFC_E_STATE, "called from inside the handle's render observer"); \
+  std::lock_guard<std::mutex> lk((r)->mu)
+
 #define DFC_CK(expr, what)                             \
   do {                                                 \
     cudaError_t e_ = (expr);                           \
     if (e_ != cudaSuccess) return cuda_fail(r, e_, what); \
   } while (0)
 
+// Per-pass totals: [0] rays traced, [1] shade work items, [2] camera rays (the rays of step 0).
 __global__ void k_sum_counts(const unsigned* counts, int steps, unsigned long long* total) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    unsigned long long s = 0;
-    for (int i = 0; i < steps; ++i) s += counts[4 * i];
-    *total += s;
+    unsigned long long s = 0, w = 0;
+    for (int i = 0; i < steps; ++i) { s += counts[4 * i]; w += counts[4 * i + 1]; }
+    total[0] += s;
+    total[1] += w;
+    total[2] += counts[0];
   }
 }
 
-// Stage ids for dfc_read_stage_times: 1 ray generation, 2 traversal, 3 shading.
+// Stage ids are the DFC_KERNEL_* kinds.
 int stage_begin(dfc_renderer* r, int stage) {
   if (!r->stage_timing) return -1;
   const size_t need = r->ev_marks.size() * 2 + 2;
@@ -109,10 +129,11 @@ void stage_end(dfc_renderer* r, int i) {
   if (i >= 0) cudaEventRecord(r->ev_pool[i + 1], r->stream);
 }
 void collect_stages(dfc_renderer* r) {
-  for (int k = 1; k < 5; ++k) r->last_ms[k] = 0.0f;
+  for (int k = 1; k < DFC_KERNEL_KINDS; ++k) { r->last_ms[k] = 0.0f; r->last_launches[k] = 0; }
   for (auto& m : r->ev_marks) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, r->ev_pool[m.second], r->ev_pool[m.second + 1]) == cudaSuccess) r->last_ms[m.first] += ms;
+    r->last_launches[m.first] += 1;
   }
   r->ev_marks.clear();
 }
@@ -172,7 +193,7 @@ int alloc_wavefront(dfc_renderer* r) {
     DFC_CK(r->d_work_list[k].ensure(P * 4), "work list");
   }
   DFC_CK(r->d_overflow.ensure(16), "counters");
-  DFC_CK(r->d_ray_total.ensure(16), "counters");
+  DFC_CK(r->d_ray_total.ensure(32), "counters");
   DFC_CK(r->d_sort_keys.ensure(P), "sort");
   DFC_CK(r->d_sorted.ensure(P * 4), "sort");
   DFC_CK(r->d_ray_mask.ensure(P), "ray mask");
@@ -192,7 +213,7 @@ int clear_film(dfc_renderer* r) {
   DFC_CK(cudaMemsetAsync(r->d_primary_prim.p, 0xff, P * 4, r->stream), "clear");
   DFC_CK(cudaMemsetAsync(r->d_primary_t.p, 0, P * 4, r->stream), "clear");
   DFC_CK(cudaMemsetAsync(r->d_overflow.p, 0, 16, r->stream), "clear");
-  DFC_CK(cudaMemsetAsync(r->d_ray_total.p, 0, 16, r->stream), "clear");
+  DFC_CK(cudaMemsetAsync(r->d_ray_total.p, 0, 32, r->stream), "clear");
   r->pass = 0;
   r->total_paths = 0;
   r->launches = 0;
@@ -284,7 +305,7 @@ int enqueue_pass(dfc_renderer* r) {
   g.ray_count = counts;
   g.work_list = r->d_work_list[0].as<unsigned>();
   g.work_count = counts + 1;
-  int ev = stage_begin(r, 1);
+  int ev = stage_begin(r, DFC_KERNEL_RAYGEN);
   k_raygen<<<(r->paths + 255) / 256, 256, 0, r->stream>>>(g);
   stage_end(r, ev);
   r->launches++;
@@ -295,7 +316,7 @@ int enqueue_pass(dfc_renderer* r) {
     DFC_CK(r->d_sort_bins.ensure(bins_bytes), "sort");
     DFC_CK(cudaMemsetAsync(r->d_sort_bins.p, 0, bins_bytes, r->stream), "sort");
     for (int s = 0; s < steps; ++s) {
-      ev = stage_begin(r, 2);
+      ev = stage_begin(r, DFC_KERNEL_TRACE);
       trace_kernel(r)<<<trace_grid, kTraceThreads, 0, r->stream>>>(trace_args(r, s));
       stage_end(r, ev);
       ShadeArgs a = shade_args(r, s);
@@ -310,21 +331,27 @@ int enqueue_pass(dfc_renderer* r) {
       so.keys = r->d_sort_keys.as<unsigned char>();
       so.bins = r->d_sort_bins.as<unsigned>() + (size_t)s * 2 * kSortBins;
       so.sorted = r->d_sorted.as<unsigned>();
-      ev = stage_begin(r, 3);
+      ev = stage_begin(r, DFC_KERNEL_SORT_COUNT);
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
+      stage_end(r, ev);
+      ev = stage_begin(r, DFC_KERNEL_SORT_SCATTER);
       k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
+      stage_end(r, ev);
       a.work_list = so.sorted;
       // path-ordered ray lists pay for their extra launch only on large passes; small ones stay launch-bound
       a.ray_mask = r->paths >= kOrderedRayListMinPaths ? r->d_ray_mask.as<unsigned char>() : nullptr;
+      ev = stage_begin(r, DFC_KERNEL_SHADE);
       (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
           <<<shade_grid, 256, 0, r->stream>>>(a);
+      stage_end(r, ev);
       r->launches += 4;
       if (a.ray_mask && s < steps - 1) {  // the next step's ray list, in path order
+        ev = stage_begin(r, DFC_KERNEL_RAY_LIST);
         k_ray_list_ordered<<<(r->paths + kRayListBlock - 1) / kRayListBlock, kRayListBlock, 0, r->stream>>>(
             a.ray_mask, r->paths, a.next_ray_list, a.next_ray_count);
+        stage_end(r, ev);
         r->launches += 1;
       }
-      stage_end(r, ev);
     }
   } else if (algo == DFC_RAY_TRACING) {
     ShadeArgs a = shade_args(r, 0);
@@ -400,12 +427,13 @@ int dfc_create(int device, dfc_renderer** out) {
 int dfc_destroy(dfc_renderer* r) {
   if (!r) return DFC_E_INVALID_ARG;
   {
-    std::lock_guard<std::mutex> lk(r->mu);
+    DFC_LOCK(r);
     cudaSetDevice(r->device);
     cudaStreamSynchronize(r->stream);
   }
   cudaEventDestroy(r->ev0);
   cudaEventDestroy(r->ev1);
+  if (r->h_rgba) cudaFreeHost(r->h_rgba);
   for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
   cudaStream_t s = r->stream;
   delete r;  // DevBuf destructors free device memory
@@ -417,7 +445,7 @@ const char* dfc_last_error(const dfc_renderer* r) { return r ? r->err.c_str() : 
 
 int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t count, int type) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!name) return fail(r, DFC_E_INVALID_ARG, "name == null");
   if (count < 0 || (count > 0 && !data)) return fail(r, DFC_E_INVALID_ARG, "data == null or negative count");
   if (type == DFC_F32) {
@@ -434,7 +462,7 @@ int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t c
 
 int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   RecycleOnExit recycle{r->staged};
   cudaSetDevice(r->device);
   HostScene hs;
@@ -459,7 +487,7 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
 
 int dfc_set_image(dfc_renderer* r, int width, int height) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (width == 0 && height == 0) {
     r->image_from_camera = 1;
     if (r->have_scene) { r->width = (int)r->scene.host.camera[17]; r->height = (int)r->scene.host.camera[18]; }
@@ -476,7 +504,7 @@ int dfc_set_image(dfc_renderer* r, int width, int height) {
 #define DFC_SETTER(fn, field, lo, hi, msg)                                            \
   int fn(dfc_renderer* r, int v) {                                                    \
     if (!valid(r)) return DFC_E_INVALID_ARG;                                          \
-    std::lock_guard<std::mutex> lk(r->mu);                                            \
+    DFC_LOCK(r);                                            \
     if (v < (lo) || v > (hi)) return fail(r, DFC_E_INVALID_ARG, msg);                 \
     r->field = v;                                                                     \
     return DFC_OK;                                                                    \
@@ -490,7 +518,7 @@ DFC_SETTER(dfc_set_preview_mode, preview, 0, 1, "preview mode is 0 or 1")
 
 int dfc_set_maximum_distance(dfc_renderer* r, float v) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!std::isfinite(v)) return fail(r, DFC_E_INVALID_ARG, "maximumDistance must be finite");
   r->max_distance = v;
   return DFC_OK;
@@ -498,21 +526,21 @@ int dfc_set_maximum_distance(dfc_renderer* r, float v) {
 
 int dfc_set_stage_timing(dfc_renderer* r, int on) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   r->stage_timing = on ? 1 : 0;
   return DFC_OK;
 }
 
 int dfc_set_seed(dfc_renderer* r, uint32_t seed) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   r->seed = seed;
   return DFC_OK;
 }
 
 int dfc_setup(dfc_renderer* r) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->have_scene) return fail(r, DFC_E_STATE, "setup() before setScene()");
   cudaSetDevice(r->device);
   int rc = alloc_wavefront(r);
@@ -523,10 +551,58 @@ int dfc_setup(dfc_renderer* r) {
   return DFC_OK;
 }
 
-int dfc_render(dfc_renderer* r, int passes, int* completed) {
-  if (completed) *completed = 0;
-  if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+}  // extern "C"
+
+namespace {
+
+// Resolves the film into the RGBA8 image on the handle's stream
+// (renderer/gpu/AbstractImageKernel.java:1104-1325; the tone mapper applies to
+// PATH_TRACING only, GPURenderer.java:108-110, :312-335).
+void enqueue_resolve(dfc_renderer* r) {
+  const int tm = r->algorithm == DFC_PATH_TRACING ? r->tone_mapper : DFC_TONE_MAPPER_NONE;
+  k_resolve_rgba8<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->d_film_sum.as<float4>(), (int)r->pixels, tm, 1.0f, r->d_rgba.as<uchar4>(),
+                                                                  r->film_filter == 1 ? r->d_film_consts.as<float>() : nullptr);
+}
+
+// Calls the observer with the handle marked as observing on this thread.
+void notify(dfc_renderer* r, dfc_observer_fn fn, void* user, int event, int pass, double progress, double millis, bool image) {
+  dfc_pass_event ev{};
+  ev.event = event;
+  ev.render_pass = pass;
+  ev.progress = progress;
+  ev.millis = millis;
+  ev.rgba = image ? r->h_rgba : nullptr;
+  ev.width = r->width;
+  ev.height = r->height;
+  t_observing = r;
+  fn(user, &ev);
+  t_observing = nullptr;
+}
+
+// The image after the last pass into the pinned host copy handed to observers
+// (AbstractGPURenderer.doUpdateImageF, :668-712).
+int update_host_image(dfc_renderer* r) {
+  const size_t bytes = (size_t)r->pixels * 4;
+  if (r->h_rgba_bytes < bytes) {
+    if (r->h_rgba) cudaFreeHost(r->h_rgba);
+    r->h_rgba = nullptr;
+    r->h_rgba_bytes = 0;
+    DFC_CK(cudaMallocHost(reinterpret_cast<void**>(&r->h_rgba), bytes), "observer image");
+    r->h_rgba_bytes = bytes;
+  }
+  enqueue_resolve(r);
+  DFC_CK(cudaMemcpyAsync(r->h_rgba, r->d_rgba.p, bytes, cudaMemcpyDeviceToHost, r->stream), "observer image");
+  DFC_CK(cudaStreamSynchronize(r->stream), "observer image");
+  return DFC_OK;
+}
+
+// render(renderPasses) with the lock held.  Without an observer the passes are
+// enqueued back to back and the host waits once; with one, every pass follows
+// AbstractGPURenderer.render() (:231-297): onRenderDisplay of the cleared image
+// on the first pass after a clear, onRenderPassProgress(0.0), the pass, the
+// image update, onRenderPassProgress(1.0), onRenderDisplay and
+// onRenderPassComplete(millis), the host waiting for each pass.
+int render_locked(dfc_renderer* r, int passes, dfc_observer_fn fn, void* user, int* completed) {
   if (passes < 1) return fail(r, DFC_E_INVALID_ARG, "renderPasses < 1");  // AbstractGPURenderer.java:323
   if (!r->set_up) return fail(r, DFC_E_STATE, "render() before setup()");
   cudaSetDevice(r->device);
@@ -541,9 +617,25 @@ int dfc_render(dfc_renderer* r, int passes, int* completed) {
   int done = 0;
   for (int k = 0; k < passes; ++k) {
     if (r->stop.load()) break;
-    int rc = enqueue_pass(r);
-    if (rc) return rc;
-    ++done;
+    if (fn) {
+      if (r->pass == 0) {  // a cleared film: the observer sees the cleared image first
+        if (int rc = update_host_image(r)) return rc;
+        notify(r, fn, user, DFC_OBSERVE_DISPLAY, 0, 0.0, 0.0, true);
+      }
+      const int pass_no = (int)r->pass + 1;
+      notify(r, fn, user, DFC_OBSERVE_PASS_PROGRESS, pass_no, 0.0, 0.0, false);
+      const auto t0 = std::chrono::steady_clock::now();
+      if (int rc = enqueue_pass(r)) return rc;
+      if (int rc = update_host_image(r)) return rc;
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      ++done;
+      notify(r, fn, user, DFC_OBSERVE_PASS_PROGRESS, pass_no, 1.0, 0.0, false);
+      notify(r, fn, user, DFC_OBSERVE_DISPLAY, pass_no, 1.0, 0.0, true);
+      notify(r, fn, user, DFC_OBSERVE_PASS_COMPLETE, pass_no, 1.0, ms, false);
+    } else {
+      if (int rc = enqueue_pass(r)) return rc;
+      ++done;
+    }
   }
   DFC_CK(cudaEventRecord(r->ev1, r->stream), "event");
   DFC_CK(cudaEventSynchronize(r->ev1), "render");
@@ -560,6 +652,25 @@ int dfc_render(dfc_renderer* r, int passes, int* completed) {
   return DFC_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int dfc_render(dfc_renderer* r, int passes, int* completed) {
+  if (completed) *completed = 0;
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  DFC_LOCK(r);
+  return render_locked(r, passes, nullptr, nullptr, completed);
+}
+
+int dfc_render_observed(dfc_renderer* r, int passes, dfc_observer_fn fn, void* user, int* completed) {
+  if (completed) *completed = 0;
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  DFC_LOCK(r);
+  if (!fn) return fail(r, DFC_E_INVALID_ARG, "observer == null");
+  return render_locked(r, passes, fn, user, completed);
+}
+
 int dfc_render_shutdown(dfc_renderer* r) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
   r->stop.store(true);
@@ -568,7 +679,7 @@ int dfc_render_shutdown(dfc_renderer* r) {
 
 int dfc_clear(dfc_renderer* r) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->set_up) return DFC_OK;
   cudaSetDevice(r->device);
   return clear_film(r);
@@ -576,7 +687,7 @@ int dfc_clear(dfc_renderer* r) {
 
 int dfc_update_camera(dfc_renderer* r, const float* camera19) {
   if (!valid(r) || !camera19) return fail(r, DFC_E_INVALID_ARG, "camera == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->have_scene) return fail(r, DFC_E_STATE, "updateCamera() before setScene()");
   std::memcpy(r->scene.host.camera, camera19, 19 * sizeof(float));
   DFC_CK(cudaMemcpyAsync(r->scene.camera.p, camera19, 19 * sizeof(float), cudaMemcpyHostToDevice, r->stream), "camera");
@@ -586,7 +697,7 @@ int dfc_update_camera(dfc_renderer* r, const float* camera19) {
 
 int dfc_update_matrices(dfc_renderer* r, const float* m, int64_t n) {
   if (!valid(r) || !m) return fail(r, DFC_E_INVALID_ARG, "matrices == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->have_scene) return fail(r, DFC_E_STATE, "updateMatrix44Fs() before setScene()");
   if (n != (int64_t)r->scene.host.prims.size()) return fail(r, DFC_E_INVALID_ARG, "matrix count differs from the primitive count");
   // The top level is built over compiled bounding volumes; moving primitives
@@ -607,14 +718,10 @@ int dfc_update_matrices(dfc_renderer* r, const float* m, int64_t n) {
 
 int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t cap) {
   if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
   if (cap < (int64_t)r->pixels * 4) return fail(r, DFC_E_INVALID_ARG, "destination too small");
-  // the tone mapper applies to PATH_TRACING only; the other algorithms are gamma-encoded as they are
-  // (renderer/gpu/GPURenderer.java:108-110, :312-335)
-  const int tm = r->algorithm == DFC_PATH_TRACING ? r->tone_mapper : DFC_TONE_MAPPER_NONE;
-  k_resolve_rgba8<<<(r->pixels + 255) / 256, 256, 0, r->stream>>>(r->d_film_sum.as<float4>(), (int)r->pixels, tm, 1.0f, r->d_rgba.as<uchar4>(),
-                                                                  r->film_filter == 1 ? r->d_film_consts.as<float>() : nullptr);
+  enqueue_resolve(r);
   DFC_CK(cudaMemcpyAsync(dst, r->d_rgba.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
   DFC_CK(cudaStreamSynchronize(r->stream), "readback");
   return DFC_OK;
@@ -622,7 +729,7 @@ int dfc_read_image_rgba8(dfc_renderer* r, uint8_t* dst, int64_t cap) {
 
 int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
   if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
   if (r->film_filter != 0) return fail(r, DFC_E_STATE, "the film is the Gaussian pixel film: read it with dfc_read_pixel_film");
   const size_t P = r->pixels;
@@ -641,7 +748,7 @@ int dfc_read_film(dfc_renderer* r, float* dst, int64_t cap) {
 
 int dfc_set_bvh_builder(dfc_renderer* r, int builder) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (builder != DFC_BVH_HOST && builder != DFC_BVH_DEVICE) return fail(r, DFC_E_INVALID_ARG, "builder is DFC_BVH_HOST or DFC_BVH_DEVICE");
   r->bvh_builder = builder;
   return DFC_OK;
@@ -649,7 +756,7 @@ int dfc_set_bvh_builder(dfc_renderer* r, int builder) {
 
 int dfc_set_film_filter(dfc_renderer* r, int filter) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (filter != 0 && filter != 1) return fail(r, DFC_E_INVALID_ARG, "film filter is 0 (box) or 1 (Gaussian pixel film)");
   r->film_filter = filter;
   r->set_up = false;  // a new film: call setup() again
@@ -658,7 +765,7 @@ int dfc_set_film_filter(dfc_renderer* r, int filter) {
 
 int dfc_read_pixel_film(dfc_renderer* r, float* dst, int64_t cap) {
   if (!valid(r) || !dst) return fail(r, DFC_E_INVALID_ARG, "dst == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
   if (r->film_filter != 1) return fail(r, DFC_E_STATE, "the film is the box film: read it with dfc_read_film");
   if (cap < (int64_t)r->pixels * 4) return fail(r, DFC_E_INVALID_ARG, "destination too small");
@@ -669,7 +776,7 @@ int dfc_read_pixel_film(dfc_renderer* r, float* dst, int64_t cap) {
 
 int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t cap) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (!r->set_up) return fail(r, DFC_E_STATE, "no film");
   if (cap < (int64_t)r->pixels) return fail(r, DFC_E_INVALID_ARG, "destination too small");
   if (prim) DFC_CK(cudaMemcpyAsync(prim, r->d_primary_prim.p, (size_t)r->pixels * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
@@ -680,7 +787,7 @@ int dfc_read_primary_hits(dfc_renderer* r, int32_t* prim, float* t, int64_t cap)
 
 int dfc_read_counters(dfc_renderer* r, int64_t* out4) {
   if (!valid(r) || !out4) return fail(r, DFC_E_INVALID_ARG, "out == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   unsigned long long rays = 0;
   if (r->set_up) {
     DFC_CK(cudaMemcpyAsync(&rays, r->d_ray_total.p, 8, cudaMemcpyDeviceToHost, r->stream), "readback");
@@ -695,15 +802,43 @@ int dfc_read_counters(dfc_renderer* r, int64_t* out4) {
 
 int dfc_read_commit_times(dfc_renderer* r, float* out4) {
   if (!valid(r) || !out4) return fail(r, DFC_E_INVALID_ARG, "out == null");
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   std::memcpy(out4, r->commit_ms, sizeof r->commit_ms);
   return DFC_OK;
 }
 
 int dfc_read_stage_times(dfc_renderer* r, float* out5) {
   if (!valid(r) || !out5) return fail(r, DFC_E_INVALID_ARG, "out == null");
-  std::lock_guard<std::mutex> lk(r->mu);
-  std::memcpy(out5, r->last_ms, sizeof r->last_ms);
+  DFC_LOCK(r);
+  const float* m = r->last_ms;
+  out5[0] = m[0];
+  out5[1] = m[DFC_KERNEL_RAYGEN];
+  out5[2] = m[DFC_KERNEL_TRACE];
+  out5[3] = m[DFC_KERNEL_SHADE] + m[DFC_KERNEL_SORT_COUNT] + m[DFC_KERNEL_SORT_SCATTER] + m[DFC_KERNEL_RAY_LIST];
+  out5[4] = m[DFC_KERNEL_FILM];
+  return DFC_OK;
+}
+
+int dfc_read_kernel_stats(dfc_renderer* r, float* ms, int64_t* launches, int64_t* items, int n) {
+  if (!valid(r)) return DFC_E_INVALID_ARG;
+  DFC_LOCK(r);
+  if (n < 1 || n > DFC_KERNEL_KINDS) return fail(r, DFC_E_INVALID_ARG, "n must be 1 .. DFC_KERNEL_KINDS");
+  unsigned long long tot[4] = {0, 0, 0, 0};
+  if (r->set_up) {
+    DFC_CK(cudaMemcpyAsync(tot, r->d_ray_total.p, sizeof tot, cudaMemcpyDeviceToHost, r->stream), "readback");
+    DFC_CK(cudaStreamSynchronize(r->stream), "readback");
+  }
+  int64_t it[DFC_KERNEL_KINDS] = {};
+  it[0] = r->total_paths;
+  it[DFC_KERNEL_RAYGEN] = r->total_paths;
+  it[DFC_KERNEL_TRACE] = (int64_t)tot[0];
+  it[DFC_KERNEL_SHADE] = it[DFC_KERNEL_SORT_COUNT] = it[DFC_KERNEL_SORT_SCATTER] = (int64_t)tot[1];
+  it[DFC_KERNEL_RAY_LIST] = (int64_t)(tot[0] - tot[2]);
+  for (int k = 0; k < n; ++k) {
+    if (ms) ms[k] = r->last_ms[k];
+    if (launches) launches[k] = k == 0 ? r->launches : r->last_launches[k];
+    if (items) items[k] = it[k];
+  }
   return DFC_OK;
 }
 
@@ -774,7 +909,7 @@ bool device_pointer_on(const void* p, int device) {
 extern "C" int dfc_trace_rays_noalloc(dfc_renderer* r, const float* d_origins, const float* d_directions, float* d_hits,
                                       int64_t count) {
   if (!valid(r)) return DFC_E_INVALID_ARG;
-  std::lock_guard<std::mutex> lk(r->mu);
+  DFC_LOCK(r);
   if (count < 0) return fail(r, DFC_E_INVALID_ARG, "count < 0");
   if (count > kNoAllocMaxRays)
     return fail(r, DFC_E_INVALID_ARG, "count " + std::to_string(count) + " exceeds the " + std::to_string(kNoAllocMaxRays) +

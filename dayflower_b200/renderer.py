@@ -152,14 +152,40 @@ class GPURenderer:
             self.setScene(cs)
             self.setup()
         done = ctypes.c_int(0)
-        rc = self._lib.dfc_render(self._h, n, ctypes.byref(done))
+        if self._observer is None:
+            rc = self._lib.dfc_render(self._h, n, ctypes.byref(done))
+        else:
+            # every pass notifies the observer as AbstractGPURenderer.render() does (:277-291)
+            errors = []
+
+            def on_event(_user, ev_p):
+                ev = ev_p.contents
+                try:
+                    if ev.event == 0:
+                        self._notify("onRenderPassProgress", ev.render_pass, ev.progress)
+                    elif ev.event == 1:
+                        img = np.ctypeslib.as_array(ev.rgba, shape=(ev.height, ev.width, 4)).copy()
+                        self._notify("onRenderDisplay", img)
+                    else:
+                        self._notify("onRenderPassComplete", ev.render_pass, ev.millis)
+                except BaseException as e:  # an exception must not unwind through the C frames
+                    errors.append(e)
+                    self._lib.dfc_render_shutdown(self._h)
+
+            cb = _native.OBSERVER_FN(on_event)
+            rc = self._lib.dfc_render_observed(self._h, n, cb, None, ctypes.byref(done))
+            if errors:
+                raise errors[0]
         self._render_pass += done.value
         if rc == DFC_E_STOPPED:
             return False
         self._check(rc)
-        if self._observer is not None and hasattr(self._observer, "onRenderPassComplete"):
-            self._observer.onRenderPassComplete(self, self._render_pass, self.lastRenderMillis())
         return True
+
+    def _notify(self, method, *args):
+        fn = getattr(self._observer, method, None)
+        if fn is not None:
+            fn(self, *args)
 
     def renderShutdown(self):
         if self._h is not None:
@@ -237,10 +263,32 @@ class GPURenderer:
     def traceRaysNoAlloc(self, d_origins: int, d_directions: int, d_hits: int, count: int):
         """Closest hits of ``count`` rays held in device memory (addresses of
         float4 arrays: origins, directions with tmax in w, hits out), with no
-        device allocation by the library; at most 1,048,576 rays per call."""
+        device allocation by the library; at most 1,048,576 rays per call.
+
+        It traces the scene of the last ``setScene``.  Edits made since then
+        with a ``CompiledSceneModifier`` raise :class:`RenderError`
+        (``DFC_E_STATE``): uploading them would allocate device memory, so the
+        caller commits them first with ``setScene``."""
         self._alive()
+        cs = self._scene
+        if cs is not None and getattr(cs, "version", 0) != getattr(self, "_scene_version", 0):
+            raise RenderError(DFC_E_STATE, "the compiled scene changed after setScene(); commit it with setScene() before "
+                                           "traceRaysNoAlloc (which uploads nothing)")
         self._check(self._lib.dfc_trace_rays_noalloc(self._h, ctypes.c_void_p(d_origins), ctypes.c_void_p(d_directions),
                                                      ctypes.c_void_p(d_hits), int(count)))
+
+    KERNELS = ("call", "raygen", "trace", "shade", "film", "sort_count", "sort_scatter", "ray_list")
+
+    def kernelStats(self):
+        """Per kernel kind: device milliseconds and launches of the last render call (with stage timing
+        on) and the items processed since setup/clear (paths, rays, shade work items, listed rays)."""
+        n = len(self.KERNELS)
+        ms = np.zeros(n, dtype=np.float32)
+        launches = np.zeros(n, dtype=np.int64)
+        items = np.zeros(n, dtype=np.int64)
+        self._check(self._lib.dfc_read_kernel_stats(self._h, ms.ctypes.data_as(ctypes.c_void_p), launches.ctypes.data_as(ctypes.c_void_p),
+                                                    items.ctypes.data_as(ctypes.c_void_p), n))
+        return {k: {"ms": float(ms[i]), "launches": int(launches[i]), "items": int(items[i])} for i, k in enumerate(self.KERNELS)}
 
     def lastRenderMillis(self) -> float:
         return self.stageMillis()["total"]

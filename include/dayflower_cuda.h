@@ -4,8 +4,7 @@
  *
  * Every entry point takes plain pointers and sizes.  Each one names the member
  * of the reference's GPURenderer API (org.dayflower.renderer.gpu, paths are
- * relative to src/main/java/org/dayflower/) that it replaces; INTEGRATION.md
- * shows the Java, ctypes and C bindings.
+ * relative to src/main/java/org/dayflower/) that it replaces.
  *
  * Ownership: the caller owns every host array it passes; the library copies
  * what it keeps before returning.  The library owns all device memory.
@@ -122,6 +121,41 @@ int dfc_setup(dfc_renderer* r);
  * Returns DFC_E_STOPPED if dfc_render_shutdown() interrupted it. */
 int dfc_render(dfc_renderer* r, int render_passes, int* completed);
 
+/* render(renderPasses) with a RendererObserver, AbstractGPURenderer.java:231-297
+ * and :322-332 (render(int) is a loop of render()).  Each pass calls fn, on the
+ * caller's thread, as the reference notifies its observer:
+ *   DFC_OBSERVE_PASS_PROGRESS (progress 0.0)   onRenderPassProgress(renderer, renderPass, 0.0)
+ *   ... the pass, then the image update (doUpdateImageF, :668-712) ...
+ *   DFC_OBSERVE_PASS_PROGRESS (progress 1.0)   onRenderPassProgress(renderer, renderPass, 1.0)
+ *   DFC_OBSERVE_DISPLAY (rgba = the image)     onRenderDisplay(renderer, image)
+ *   DFC_OBSERVE_PASS_COMPLETE (millis)         onRenderPassComplete(renderer, renderPass, elapsedTimeMillis)
+ * and the first pass after dfc_setup/dfc_clear starts with DFC_OBSERVE_DISPLAY
+ * of the cleared image (render_pass 0), as render() does after filmClear.
+ * render_pass counts from 1 after a clear.  The host waits for every pass, so
+ * an observed render is slower than dfc_render by one RGBA8 resolve and
+ * read-back per pass.  fn runs with the handle locked: it may call
+ * dfc_render_shutdown, and any other call on the same handle returns
+ * DFC_E_STATE.  rgba (width * height * 4 bytes, rows top to bottom) is valid
+ * only during the call. */
+typedef enum dfc_observe_event {
+  DFC_OBSERVE_PASS_PROGRESS = 0,
+  DFC_OBSERVE_DISPLAY = 1,
+  DFC_OBSERVE_PASS_COMPLETE = 2
+} dfc_observe_event;
+
+typedef struct dfc_pass_event {
+  int event;             /* dfc_observe_event */
+  int render_pass;
+  double progress;       /* PASS_PROGRESS: 0.0 before the pass, 1.0 after it */
+  double millis;         /* PASS_COMPLETE: host milliseconds of the pass and its image update */
+  const uint8_t* rgba;   /* DISPLAY: the RGBA8 image (tone mapped, sRGB) */
+  int width, height;
+} dfc_pass_event;
+
+typedef void (*dfc_observer_fn)(void* user, const dfc_pass_event* event);
+
+int dfc_render_observed(dfc_renderer* r, int render_passes, dfc_observer_fn fn, void* user, int* completed);
+
 /* renderShutdown(), AbstractGPURenderer.java:342: asynchronous stop request. */
 int dfc_render_shutdown(dfc_renderer* r);
 
@@ -179,6 +213,30 @@ int dfc_read_counters(dfc_renderer* r, int64_t* out4);
  * out[0] total, [1] ray generation, [2] traversal, [3] shading, [4] film.
  * Stages [1]-[4] are filled only while dfc_set_stage_timing is on. */
 int dfc_read_stage_times(dfc_renderer* r, float* out5);
+
+/* Per-kernel device time of the last dfc_render call (while dfc_set_stage_timing
+ * is on; CUDA events around every launch), launches, and the work items those
+ * kernels processed since the last dfc_setup/dfc_clear; index 0 is the whole
+ * call (its time, all launches, paths).  Kernel kinds and their items:
+ *   DFC_KERNEL_RAYGEN        camera paths started
+ *   DFC_KERNEL_TRACE         rays traced
+ *   DFC_KERNEL_SHADE         shade work items (also the two sort kernels')
+ *   DFC_KERNEL_FILM          (resolves; no items)
+ *   DFC_KERNEL_SORT_COUNT, DFC_KERNEL_SORT_SCATTER  material sort of the work items
+ *   DFC_KERNEL_RAY_LIST      rays listed in path order (all but the camera rays)
+ * ms, launches, items: n entries each (any may be NULL), n <= DFC_KERNEL_KINDS.
+ * No counterpart in the reference (it times whole passes only). */
+enum {
+  DFC_KERNEL_RAYGEN = 1,
+  DFC_KERNEL_TRACE = 2,
+  DFC_KERNEL_SHADE = 3,
+  DFC_KERNEL_FILM = 4,
+  DFC_KERNEL_SORT_COUNT = 5,
+  DFC_KERNEL_SORT_SCATTER = 6,
+  DFC_KERNEL_RAY_LIST = 7,
+  DFC_KERNEL_KINDS = 8
+};
+int dfc_read_kernel_stats(dfc_renderer* r, float* ms, int64_t* launches, int64_t* items, int n);
 
 /* Host wall time of the last dfc_scene_commit in milliseconds: out[0] decode
  * and acceleration builds, [1] of which bottom-level (mesh) builds, [2] of

@@ -2256,6 +2256,7 @@ struct Params {
   int preview;
   uint32_t seed;
   int row_begin, row_end;
+  int row_step;  // render rows row_begin, row_begin + row_step, ... below row_end (0 or 1: every row)
 };
 
 // scene/Scene.java:451 radiancePathTracer
@@ -2502,9 +2503,11 @@ typedef struct dfo_params {
   int preview;
   unsigned int seed;
   int row_begin, row_end;
+  int row_step;
 } dfo_params;
 
-// Renders rows [row_begin, row_end) with spp samples per pixel (samples
+// Renders rows row_begin, row_begin + row_step, ... below row_end (every row
+// of [row_begin, row_end) when row_step <= 1) with spp samples per pixel (samples
 // sample_base .. sample_base + spp - 1).  Outputs (any may be NULL), each
 // W*H entries, only the rendered rows written:
 //   sum_rgb   sum of the accepted samples (AbstractCPURenderer.java:231 guard)
@@ -2617,8 +2620,9 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
   std::memcpy(&P, pp, sizeof P);
   if (P.width <= 0 || P.height <= 0 || P.spp < 0) return -1;
   int rb = std::max(0, P.row_begin), re = std::min(P.height, P.row_end <= 0 ? P.height : P.row_end);
+  const int step = std::max(1, P.row_step);
   if (threads < 1) threads = 1;
-  std::atomic<int> next_row(rb);
+  std::atomic<int> next_row(0);
   std::atomic<long long> rays(0);
   std::atomic<int> unsupported(0);
   std::atomic<int> rt_overflow(0);
@@ -2626,7 +2630,7 @@ long long dfo_render(void* s, const dfo_params* pp, float* sum_rgb, float* sumsq
     RayStats st;
     bool unsup = false;
     for (;;) {
-      int y = next_row.fetch_add(1);
+      const int y = rb + next_row.fetch_add(1) * step;
       if (y >= re) break;
       for (int x = 0; x < P.width; ++x) {
         const size_t pix = (size_t)y * P.width + x;
@@ -2751,6 +2755,30 @@ int dfo_primary_ray(void* s, float ix, float iy, float px, float py, float* out6
   Ray r;
   if (!primary_ray(sc->cam, ix, iy, px, py, 0.5f, 0.5f, &r)) return 0;
   out6[0] = r.o.x; out6[1] = r.o.y; out6[2] = r.o.z; out6[3] = r.d.x; out6[4] = r.d.y; out6[5] = r.d.z;
+  return 1;
+}
+// One candidate of a primary hit, for the near-tie check of hit-id mismatches:
+// the primary ray of pixel (x, y), sample 0 of `seed` on a film `width` pixels
+// wide (the render's jitter, moved by (dpx, dpy) pixels), tested against
+// primitive `prim` alone in its object space (no bounding volume, no drift).
+// Returns 1 with the world t of a hit in (tMinimum, tMaximum), 0 on a miss,
+// -1 for bad arguments.
+int dfo_primary_prim_t(void* s, unsigned int seed, int width, int x, int y, float dpx, float dpy, int prim, float* t_out) {
+  Scene* sc = (Scene*)s;
+  if (!sc || !t_out || prim < 0 || prim >= sc->prim_count || width <= 0 || x < 0 || y < 0) return -1;
+  const uint32_t key = rng_path_key(seed, (uint32_t)((size_t)y * width + x), 0u);
+  Ray r;
+  if (!primary_ray(sc->cam, (float)x, (float)y, rng_uniform(key, kDimPixelX) + dpx, rng_uniform(key, kDimPixelY) + dpy,
+                   rng_uniform(key, kDimLensU), rng_uniform(key, kDimLensV), &r))
+    return 0;
+  const int32_t* P = sc->prims.data() + (size_t)prim * 8;
+  const Ray ro = transform_ray(sc->w2o[prim], r);
+  int aux = -1;
+  const float tmaxo = transform_t(sc->w2o[prim], r, ro, kTMaximum);
+  const float th = shape_t(*sc, P[6], P[7], ro, kTMinimum, tmaxo, &aux);
+  if (std::isnan(th) || !(th > kTMinimum) || !(th < tmaxo)) return 0;
+  const Ray rw = transform_ray(sc->o2w[prim], ro);
+  *t_out = transform_t(sc->o2w[prim], ro, rw, th);
   return 1;
 }
 // noise/PerlinNoiseF.java, noise/SimplexNoiseF.java

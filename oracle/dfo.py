@@ -27,7 +27,7 @@ _c_p, _c_f, _c_i, _c_u = ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c
 class Params(ctypes.Structure):
     _fields_ = [("algo", _c_i), ("width", _c_i), ("height", _c_i), ("spp", _c_i), ("sample_base", _c_i),
                 ("max_bounce", _c_i), ("min_rr", _c_i), ("ao_samples", _c_i), ("ao_distance", _c_f), ("preview", _c_i),
-                ("seed", _c_u), ("row_begin", _c_i), ("row_end", _c_i)]
+                ("seed", _c_u), ("row_begin", _c_i), ("row_end", _c_i), ("row_step", _c_i)]
 
 
 _lib = None
@@ -78,6 +78,7 @@ def lib() -> ctypes.CDLL:
         L.dfo_rng_uniform.restype = _c_f
         L.dfo_rng_uniform.argtypes = [_c_u, _c_u]
         L.dfo_primary_ray.argtypes = [_c_p, _c_f, _c_f, _c_f, _c_f, _c_p]
+        L.dfo_primary_prim_t.argtypes = [_c_p, _c_u, _c_i, _c_i, _c_i, _c_f, _c_f, _c_i, ctypes.POINTER(_c_f)]
         for n, args in (("dfo_perlin", [_c_f] * 3), ("dfo_simplex", [_c_f] * 3), ("dfo_perlin_turbulence", [_c_f] * 3 + [_c_i]),
                         ("dfo_simplex_fbm", [_c_f] * 7 + [_c_i])):
             getattr(L, n).restype = _c_f
@@ -120,12 +121,13 @@ class OracleScene:
 
     def render(self, algorithm: int, spp: int = 1, sample_base: int = 0, max_bounce: int = 20, min_rr: int = 5,
                ao_samples: int = 10, ao_distance: float = 20.0, seed: int = 0x5EED1234, rows=None, threads: int = 1,
-               preview: bool = False):
-        """Returns dict(sum, sumsq, count, prim, t, rays) over rows [r0, r1)."""
+               preview: bool = False, row_step: int = 1):
+        """Returns dict(sum, sumsq, count, prim, t, rays) over rows r0, r0 + row_step, ... below r1
+        (rows = (r0, r1), default the whole image); rows not rendered are left empty."""
         W, H = self.width, self.height
         r0, r1 = (0, H) if rows is None else rows
         p = Params(int(algorithm), W, H, int(spp), int(sample_base), int(max_bounce), int(min_rr), int(ao_samples),
-                   float(ao_distance), 1 if preview else 0, int(seed) & 0xFFFFFFFF, int(r0), int(r1))
+                   float(ao_distance), 1 if preview else 0, int(seed) & 0xFFFFFFFF, int(r0), int(r1), int(row_step))
         s = np.zeros((H, W, 3), np.float32)
         q = np.zeros((H, W, 3), np.float32)
         n = np.zeros((H, W), np.int32)
@@ -136,12 +138,22 @@ class OracleScene:
             raise RuntimeError("oracle render failed (%d): the scene uses features the oracle does not restate" % rays)
         return {"sum": s, "sumsq": q, "count": n, "prim": prim, "t": t, "rays": int(rays)}
 
+    def primary_prim_t(self, seed: int, x: int, y: int, prim: int, dpx: float = 0.0, dpy: float = 0.0):
+        """World t at which pixel (x, y)'s first primary ray (its jitter moved by
+        (dpx, dpy) pixels) hits primitive ``prim`` alone, or None on a miss."""
+        t = _c_f(0.0)
+        rc = lib().dfo_primary_prim_t(self._s, int(seed) & 0xFFFFFFFF, self.width, int(x), int(y), float(dpx), float(dpy), int(prim),
+                                      ctypes.byref(t))
+        if rc < 0:
+            raise ValueError("bad primitive or pixel")
+        return float(t.value) if rc == 1 else None
+
     def render_pixel_film(self, algorithm: int, spp: int = 1, sample_base: int = 0, max_bounce: int = 20, min_rr: int = 5,
                           ao_samples: int = 10, ao_distance: float = 20.0, seed: int = 0x5EED1234, threads: int = 1):
         """The CPU renderer's Gaussian XYZ film (PixelImageF): per pixel X, Y, Z sums and the filter weight sum, (H, W, 4)."""
         W, H = self.width, self.height
         p = Params(int(algorithm), W, H, int(spp), int(sample_base), int(max_bounce), int(min_rr), int(ao_samples),
-                   float(ao_distance), 0, int(seed) & 0xFFFFFFFF, 0, H)
+                   float(ao_distance), 0, int(seed) & 0xFFFFFFFF, 0, H, 1)
         out = np.zeros((H, W, 4), np.float32)
         rays = lib().dfo_render_pixel_film(self._s, ctypes.byref(p), ptr(out), int(threads))
         if rays < 0:

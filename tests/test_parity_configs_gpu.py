@@ -1,0 +1,115 @@
+"""Parity on the stated workloads at their own sizes.
+
+* The benchmark scene (a 1024x1024-cell fractal heightfield of 2,097,152
+  triangles, 2,000 spheres, Perez sky, 1920x1080): RAY_CASTING hit ids on the
+  whole frame against the oracle's ray caster (scene/Scene.java:675-701),
+  every mismatch a near tie; PATH_TRACING at 4 spp, bounce 8, Russian
+  roulette from 5, on a strided sample of 40 rows spread over the image (the
+  oracle's linear primitive loop makes a whole frame too slow for a test).
+* The Cornell box at 512x512: RAY_CASTING hit ids on the whole frame;
+  PATH_TRACING at 16 spp, bounce 20, Russian roulette from 5 (3-sigma and
+  image mean, and the RMSE against a converged 16,384-spp image); AMBIENT_OCCLUSION
+  with 64 samples at distance 200 (scene/Scene.java:272-313).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from dayflower_b200 import RenderingAlgorithm as RA
+from dayflower_b200.scene import generators as G
+from dayflower_b200.scene.compiler import compile_scene
+from oracle import dfo
+
+from . import parity as PT
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 8
+SEED = 0x5EED1234
+
+
+@pytest.fixture(scope="module")
+def terrain_full():
+    return compile_scene(G.terrain_spheres(cells=1024, n_spheres=2000, resolution=(1920, 1080), seed=2), layout_version=2)
+
+
+@pytest.fixture(scope="module")
+def cornell_512():
+    return compile_scene(G.cornell_box(resolution=(512, 512)))
+
+
+def _ray_casting(cs):
+    g = PT.render_gpu(cs, RA.RAY_CASTING, seed=SEED)
+    osc = dfo.OracleScene(cs)
+    o = osc.render(RA.RAY_CASTING, spp=1, seed=SEED, threads=THREADS)
+    L = dfo.lib()
+    L.dfo_set_no_drift(1)
+    try:
+        o_nd = osc.render(RA.RAY_CASTING, spp=1, seed=SEED, threads=THREADS)
+    finally:
+        L.dfo_set_no_drift(0)
+    frac, _, q = PT.check_primary(g, o, o_nd)
+    # every mismatch against the drift-free oracle (the arithmetic the device follows) is a near tie;
+    # against the faithful oracle the 99.99% bound above holds, its extra mismatches being the
+    # reference's own drift (the faithful and drift-free oracles differ on ~0.009% of this scene's pixels)
+    ties, edges, bad = PT.mismatch_near_ties(g, osc, o_nd, SEED)
+    assert not bad, "hit-id mismatches that are not near ties: %d (first %s)" % (len(bad), bad[:5])
+    mg = g["sum"] / np.maximum(g["count"], 1)[..., None]
+    mo = o_nd["sum"] / np.maximum(o_nd["count"], 1)[..., None]
+    assert np.mean(np.all(np.abs(mg - mo) <= 1e-4, axis=-1)) >= 0.999
+    return frac, q
+
+
+def test_benchmark_scene_ray_casting_full_frame(terrain_full):
+    frac, q = _ray_casting(terrain_full)
+    assert frac >= PT.HIT_ID_AGREEMENT and q <= PT.DEPTH_RTOL
+
+
+def test_benchmark_scene_path_tracing_row_sample(terrain_full):
+    g = PT.render_gpu(terrain_full, RA.PATH_TRACING, spp=4, max_bounce=8, min_rr=5, seed=SEED)
+    o = dfo.OracleScene(terrain_full).render(RA.PATH_TRACING, spp=4, max_bounce=8, min_rr=5, seed=SEED, threads=THREADS,
+                                              rows=(13, 1080), row_step=27)
+    rows = np.arange(13, 1080, 27)
+    assert rows.size == 40
+    gs = {k: g[k][rows] for k in ("sum", "sumsq", "count")}
+    os_ = {k: o[k][rows] for k in ("sum", "sumsq", "count")}
+    ok, mg, mo = PT.sigma_test(gs, os_)
+    assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
+    assert abs(mg.mean() - mo.mean()) <= 0.02 * mo.mean()
+
+
+def test_cornell_512_ray_casting(cornell_512):
+    _ray_casting(cornell_512)
+
+
+def test_cornell_512_path_tracing_16spp(cornell_512):
+    g = PT.render_gpu(cornell_512, RA.PATH_TRACING, spp=16, max_bounce=20, min_rr=5, seed=SEED)
+    o = PT.render_oracle(cornell_512, RA.PATH_TRACING, spp=16, max_bounce=20, min_rr=5, seed=SEED, threads=THREADS)
+    ok, mg, mo = PT.sigma_test(g, o)
+    assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
+    assert abs(mg.mean() - mo.mean()) <= 0.02 * mo.mean()
+
+
+def test_cornell_512_rmse_against_converged(cornell_512):
+    # RMSE of 16-spp images against a converged 16,384-spp device image (independent seed), as the
+    # root of the mean squared error over four seeds; device within 2% of the drift-free oracle
+    conv = PT.render_gpu(cornell_512, RA.PATH_TRACING, spp=16384, max_bounce=20, min_rr=5, seed=0xC0FFEE)
+    ref = conv["sum"] / np.maximum(conv["count"], 1)[..., None]
+    mse_g, mse_o = [], []
+    for s in range(4):
+        seed = SEED + 7919 * s
+        g = PT.render_gpu(cornell_512, RA.PATH_TRACING, spp=16, max_bounce=20, min_rr=5, seed=seed)
+        o = PT.render_oracle_no_drift(cornell_512, RA.PATH_TRACING, spp=16, max_bounce=20, min_rr=5, seed=seed, threads=THREADS)
+        mse_g.append(np.mean((g["sum"] / np.maximum(g["count"], 1)[..., None] - ref) ** 2))
+        mse_o.append(np.mean((o["sum"] / np.maximum(o["count"], 1)[..., None] - ref) ** 2))
+    rmse_g, rmse_o = float(np.sqrt(np.mean(mse_g))), float(np.sqrt(np.mean(mse_o)))
+    assert abs(rmse_g - rmse_o) <= 0.02 * rmse_o, "RMSE device %.5f oracle %.5f" % (rmse_g, rmse_o)
+
+
+def test_cornell_512_ambient_occlusion_64_samples(cornell_512):
+    g = PT.render_gpu(cornell_512, RA.AMBIENT_OCCLUSION, spp=4, ao_samples=64, ao_distance=200.0, seed=SEED)
+    o = PT.render_oracle(cornell_512, RA.AMBIENT_OCCLUSION, spp=4, ao_samples=64, ao_distance=200.0, seed=SEED, threads=THREADS)
+    ok, mg, mo = PT.sigma_test(g, o)
+    assert ok >= PT.PIXEL_PASS, "3-sigma pass rate %.4f" % ok
+    assert abs(mg.mean() - mo.mean()) <= 0.02 * mo.mean()

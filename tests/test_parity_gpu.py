@@ -65,6 +65,9 @@ def test_ray_casting_hit_ids(scene_name, request):
     o = PT.render_oracle(cs, RA.RAY_CASTING)
     o_nd = PT.render_oracle_no_drift(cs, RA.RAY_CASTING)
     PT.check_primary(g, o, o_nd)
+    from oracle import dfo
+    _, _, bad = PT.mismatch_near_ties(g, dfo.OracleScene(cs), o_nd, 0x5EED1234)
+    assert not bad, "hit-id mismatches that are not near ties: %s" % bad[:5]
     # shading 0.5 |n_s . d| (Scene.java:675): absolute agreement with the drift-free oracle
     mg = g["sum"] / np.maximum(g["count"], 1)[..., None]
     mo = o_nd["sum"] / np.maximum(o_nd["count"], 1)[..., None]

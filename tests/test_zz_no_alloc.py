@@ -116,5 +116,16 @@ def test_noalloc_rejects_oversized_and_host_buffers():
         with pytest.raises(ValueError, match="aligned|device memory"):
             p = host.ctypes.data
             r.traceRaysNoAlloc(p, p, p, 4)
+        # an edit made after setScene is not traced silently: the caller must commit it first
+        from dayflower_b200.renderer import DFC_E_STATE, RenderError
+        from dayflower_b200.scene import model as M
+        from dayflower_b200.scene.compiler import CompiledSceneModifier
+        assert CompiledSceneModifier(compiled).add_primitive(
+            M.Primitive(M.Sphere(), M.Matte(kd=(0.5, 0.5, 0.5)), M.Transform.translate_scale((0.0, 10.0, 0.0), 2.0)))
+        with pytest.raises(RenderError) as e:
+            r.traceRaysNoAlloc(0, 0, 0, 0)
+        assert e.value.code == DFC_E_STATE
+        r.setScene(compiled)
+        r.traceRaysNoAlloc(0, 0, 0, 0)
     finally:
         r.dispose()
