@@ -209,10 +209,10 @@ def batched_and_served(args, device=0):
     image read back to the host.
 
     Served: Poisson arrival streams of the same jobs at rates 10 .. 500 jobs/s
-    into the running engine (round-robin segments); latency is submit to done
-    at the job's own spp.  The per-job comparison is the latency of one
-    renderer serving the same arrivals one job at a time in arrival order,
-    from the measured per-job render times of (a).
+    into the running engine, with round-robin and with shortest-first segment
+    order; latency is submit to done at the job's own spp, reported for all
+    jobs and for the 64-spp ones.  The per-job comparison serves the same
+    arrivals live with one renderer, one job at a time in arrival order.
     """
     import numpy as np
     from dayflower_b200 import GPURenderer, RenderEngine
@@ -291,24 +291,69 @@ def batched_and_served(args, device=0):
         }
         if args.engine_only or args.batch_only:
             return batched, None
-        # served
-        eng.configure(**dict(tuned, policy=0))
-        eng.start()
+        # served: Poisson arrivals into the running engine, round-robin and shortest-first segment
+        # orders, against one per-job renderer serving the same arrivals live
         served = []
-        for lam in (10, 25, 50, 100, 250, 500):
-            n = min(len(jobs), max(16, int(4 * lam)))
-            arr = SV.poisson_arrivals(lam, n, seed=lam)
-            sub = [jobs[i % len(jobs)] for i in range(n)]
-            r = SV.run_served(eng, sub, arr)
-            p = SV.percentiles(r["latency_s"])
-            f = SV.percentiles(SV.fifo_latencies([service[i % len(jobs)] for i in range(n)], arr))
-            served.append({"lambda_per_s": lam, "jobs": n, "p50_s": p["p50_s"], "p99_s": p["p99_s"], "paths_per_s": r["paths_per_s"],
-                           "plain_per_job_p50_s": f["p50_s"], "plain_per_job_p99_s": f["p99_s"], "states": r["states"]})
-        eng.stop()
+        lams = (10, 25, 50, 100, 250, 500)
+        arrivals = {lam: SV.poisson_arrivals(lam, min(len(jobs), max(16, int(4 * lam))), seed=lam) for lam in lams}
+        subsets = {lam: [jobs[i % len(jobs)] for i in range(len(arrivals[lam]))] for lam in lams}
+
+        def pct(lat, sub, only64):
+            sel = np.array([(j["samples"] == 64 and j["width"] * j["height"] <= 1024 * 1024) for j in sub]) if only64 else None
+            x = lat[sel] if only64 else lat
+            return SV.percentiles(x) if len(x) else None
+
+        for policy, lookahead in ((0, 0), (2, int(tuned["capacity"]))):
+            eng.configure(**dict(tuned, policy=policy, lookahead_paths=lookahead))
+            eng.start()
+            for lam in lams:
+                sub, arr = subsets[lam], arrivals[lam]
+                r = SV.run_served(eng, sub, arr)
+                p_all, p64 = pct(r["latency_s"], sub, False), pct(r["latency_s"], sub, True)
+                served.append({"policy": "round_robin" if policy == 0 else "shortest_first", "lambda_per_s": lam, "jobs": len(sub),
+                               "p50_s": p_all["p50_s"], "p99_s": p_all["p99_s"],
+                               "spp64_jobs": int(sum(j["samples"] == 64 for j in sub)),
+                               "spp64_p50_s": p64["p50_s"] if p64 else None, "spp64_p99_s": p64["p99_s"] if p64 else None,
+                               "paths_per_s": r["paths_per_s"], "states": r["states"]})
+            eng.stop()
     finally:
         eng.close()
-    return batched, {"policy": "round_robin", "latency": "submit -> done at the job's spp (engine clock)",
-                     "plain_per_job": "one job at a time in arrival order, measured per-job render times", "sweep": served}
+    # the per-job comparison, live: one GPURenderer per scene, one job at a time in arrival order
+    live = []
+    if not args.engine_only:
+        handles = []
+        for cs in scenes:
+            h = GPURenderer(device=device)
+            h.setScene(cs)
+            handles.append(h)
+
+        def render_one(j):
+            h = handles[j["scene"]]
+            c = cams[j["scene"]].copy()
+            c[17], c[18] = j["width"], j["height"]
+            h.updateCamera(c)
+            h.setImage(j["width"], j["height"])
+            h.setMaximumBounce(j["maximum_bounce"])
+            h.setSeed(j["seed"])
+            h.setup()
+            h.render(j["samples"])
+            h.getImage()
+
+        render_one(jobs[0])
+        for lam in lams:
+            sub, arr = subsets[lam], arrivals[lam]
+            lat = SV.run_per_job_served(render_one, sub, arr)
+            p_all, p64 = pct(lat, sub, False), pct(lat, sub, True)
+            live.append({"lambda_per_s": lam, "jobs": len(sub), "p50_s": p_all["p50_s"], "p99_s": p_all["p99_s"],
+                         "spp64_p50_s": p64["p50_s"] if p64 else None, "spp64_p99_s": p64["p99_s"] if p64 else None})
+        for h in handles:
+            h.dispose()
+    return batched, {"latency": "submit -> done at the job's spp (engine clock); spp64: the 64-spp jobs (all <= 1024^2)",
+                     "round_robin": "every admitted job one 64K-path segment in turn, lookahead 8 x capacity",
+                     "shortest_first": "the next segment to the admitted job with the fewest paths left, lookahead 1 x capacity",
+                     "sweep": served,
+                     "plain_per_job_live": {"how": "one GPURenderer serving the same arrivals one job at a time in arrival order, "
+                                                   "latency arrival -> RGBA8 image on the host", "sweep": live}}
 
 
 def large_scene_run(args, device=0):

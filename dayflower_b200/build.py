@@ -18,9 +18,10 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 ROOT = os.path.dirname(HERE)
 
-CUDA_SOURCES = ["dfc_api.cu", "dfc_engine.cu", "dfc_kernels.cu", "dfc_ingest.cpp", "dfc_bvh.cpp", "dfc_devscene.cpp", "dfc_blas.cu"]
+CUDA_SOURCES = ["dfc_api.cu", "dfc_engine.cu", "dfc_kernels.cu", "dfc_trace.cu", "dfc_shade.cu", "dfc_shade_simple.cu", "dfc_raytrace.cu",
+                "dfc_ingest.cpp", "dfc_bvh.cpp", "dfc_devscene.cpp", "dfc_blas.cu"]
 CUDA_HEADERS = ["dfc_scene.h", "dfc_device.cuh", "dfc_shapes.cuh", "dfc_kernels.h", "dfc_ingest.h", "dfc_bvh.h", "dfc_devscene.h",
-                "dfc_blas.h", "dfc_texture.cuh", "dfc_matderive.h"]
+                "dfc_blas.h", "dfc_texture.cuh", "dfc_matderive.h", "dfc_trav.cuh", "dfc_shade.cuh"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -61,8 +62,12 @@ def build_cuda(force: bool = False, verbose: bool = False, extra=()) -> str:
         return out
     obj_dir = os.path.join(LIB, "_obj")
     os.makedirs(obj_dir, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [os.path.join(ROOT, "include", "dayflower_cuda.h")]
+
     def compile_one(s):
         o = os.path.join(obj_dir, s + ".o")
+        if not force and not extra and not _stale(o, [os.path.join(CSRC, s)] + headers):
+            return o, ""  # this source and every header are older than its object
         # -fmad=false: every float operation is rounded on its own, as in the
         # reference (Java float arithmetic has no contraction); the traversal's
         # box tests use explicit fmaf where the rounding does not matter.

@@ -70,6 +70,7 @@ struct dfc_renderer {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, int>> ev_marks;  // (stage, index of the start event)
   int sm_count = 148;
+  bool full_bsdf = false;  // the committed scene has materials of more than two lobes (or evaluated per hit)
   int trace_blocks = 6, ao_blocks = 5, rt_blocks = 4;  // resident blocks per SM of k_trace / k_trace_ao / k_ray_trace
 };
 
@@ -311,6 +312,7 @@ int enqueue_pass(dfc_renderer* r) {
   r->launches++;
   const int trace_grid = r->sm_count * r->trace_blocks;
   const int shade_grid = r->sm_count * 8;
+  const int sort_grid = r->sm_count * 4;  // the scatter: fewer blocks, fewer bin scans and cursor atomics per launch
   if (algo == DFC_PATH_TRACING) {
     const size_t bins_bytes = (size_t)steps * 2 * kSortBins * sizeof(unsigned);
     DFC_CK(r->d_sort_bins.ensure(bins_bytes), "sort");
@@ -335,14 +337,29 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       stage_end(r, ev);
       ev = stage_begin(r, DFC_KERNEL_SORT_SCATTER);
-      k_sort_scatter<<<shade_grid, 256, 0, r->stream>>>(so);
+      k_sort_scatter<<<sort_grid, 256, 0, r->stream>>>(so);
       stage_end(r, ev);
       a.work_list = so.sorted;
       // path-ordered ray lists pay for their extra launch only on large passes; small ones stay launch-bound
       a.ray_mask = r->paths >= kOrderedRayListMinPaths ? r->d_ray_mask.as<unsigned char>() : nullptr;
+      // the two-lobe kernel shades the matte ... plastic hits, misses and light-ray-only paths; the general
+      // kernel the other materials, when the scene has any
+      ShadeArgs simple = a;
+      if (r->full_bsdf) {
+        simple.range_bins = so.bins;
+        simple.range_lo = 0;
+        simple.range_hi = kSimpleBins;
+      }
       ev = stage_begin(r, DFC_KERNEL_SHADE);
-      (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
-          <<<shade_grid, 256, 0, r->stream>>>(a);
+      (r->scene.host.record_shapes ? k_shade_path_simple_records : k_shade_path_simple)<<<shade_grid, 256, 0, r->stream>>>(simple);
+      if (r->full_bsdf) {
+        a.range_bins = so.bins;
+        a.range_lo = kSimpleBins;
+        a.range_hi = kKeyInline;
+        (r->scene.host.textured() ? k_shade_path_textured : r->scene.host.record_shapes ? k_shade_path_records : k_shade_path)
+            <<<shade_grid, 256, 0, r->stream>>>(a);
+        r->launches += 1;
+      }
       stage_end(r, ev);
       r->launches += 4;
       if (a.ray_mask && s < steps - 1) {  // the next step's ray list, in path order
@@ -477,6 +494,8 @@ int dfc_scene_commit(dfc_renderer* r, int layout_version) {
   DFC_CK(upload_scene(std::move(hs), r->stream, &r->scene), "scene upload");
   r->commit_ms[3] = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t1).count();
   r->have_scene = true;
+  r->full_bsdf = r->scene.host.textured();
+  for (const DMaterial& m : r->scene.host.materials) r->full_bsdf = r->full_bsdf || m.kind >= kSimpleKinds;
   if (r->image_from_camera) {
     r->width = (int)r->scene.host.camera[17];
     r->height = (int)r->scene.host.camera[18];

@@ -136,7 +136,7 @@ DFC_D float gamma_n(int n) { const float e = 5.9604645e-8f; return (n * e) / (1.
 
 // Double-precision edge functions (Triangle3F.java:537-546), taken only when a
 // float edge function is exactly zero; kept out of line to keep the hot loop small.
-__device__ __noinline__ void tri_edges_fp64(float x0, float y0, float x1, float y1, float x2, float y2, float* e0, float* e1, float* e2) {
+static __device__ __noinline__ void tri_edges_fp64(float x0, float y0, float x1, float y1, float x2, float y2, float* e0, float* e1, float* e2) {
   *e0 = (float)((double)y2 * (double)x1 - (double)x2 * (double)y1);
   *e1 = (float)((double)y0 * (double)x2 - (double)x0 * (double)y2);
   *e2 = (float)((double)y1 * (double)x0 - (double)x1 * (double)y0);
@@ -252,7 +252,7 @@ DFC_D EF ef_div(EF a, EF b) {
   return {v, ndn(fminf(fminf(d0, d1), fminf(d2, d3))), nup(fmaxf(fmaxf(d0, d1), fmaxf(d2, d3)))};
 }
 // geometry/shape/Sphere3F.java:507, unit sphere; returns -1 on a miss.
-__device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax);
+static __device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax);
 // A float pre-test that only rejects rays that clearly miss (the closest
 // approach of the line is outside the sphere by a margin far above rounding),
 // so that most candidate spheres never reach the interval-arithmetic test.
@@ -264,7 +264,7 @@ DFC_D float sphere_t(V3 o, V3 d, float tmin, float tmax) {
   if (disc < -1.0e-5f * (1.0f + oo)) return -1.0f;
   return sphere_t_exact(o, d, tmin, tmax);
 }
-__device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax) {
+static __device__ __noinline__ float sphere_t_exact(V3 o, V3 d, float tmin, float tmax) {
   EF ox = ef(o.x), oy = ef(o.y), oz = ef(o.z), dx = ef(d.x), dy = ef(d.y), dz = ef(d.z);
   EF a = ef_add(ef_add(ef_mul(dx, dx), ef_mul(dy, dy)), ef_mul(dz, dz));
   EF b = ef_mul(ef(2.0f), ef_add(ef_add(ef_mul(dx, ox), ef_mul(dy, oy)), ef_mul(dz, oz)));
@@ -413,9 +413,14 @@ struct Lobe {
   V3 scale;
   float p0, p1;  // Oren-Nayar A, B | microfacet alpha x, y | Disney roughness | clear coat alpha, weight | specular BTDF etaA, etaB
 };
-struct Bsdf {
+// A BSDF of at most N lobes.  The matte, mirror, glass, metal and plastic
+// materials need at most two (kSimpleLobes): their shading kernel holds the
+// lobes in registers and compiles none of the other materials' lobe code.
+template <int N>
+struct BsdfN {
+  static constexpr int kN = N;
   int n;
-  Lobe l[kMaxLobes];
+  Lobe l[N];
   float eta;            // BSDF.getEta
   float fr_i, fr_t;     // dielectric Fresnel of reflection lobes (Disney: etaT)
   float bt_a, bt_b;     // etaA, etaB of transmission lobes
@@ -424,6 +429,11 @@ struct Bsdf {
   ONB s;
   V3 ng, wo_w, wo;
 };
+using Bsdf = BsdfN<kMaxLobes>;
+constexpr int kSimpleLobes = 2;
+using SimpleBsdf = BsdfN<kSimpleLobes>;
+// Every lobe kind and Fresnel term (false: only those of the matte, mirror, glass, metal and plastic materials).
+template <class BT> constexpr bool kAllLobes = BT::kN >= kMaxLobes;
 
 DFC_D float fr_dielectric(float cosi, float etaI, float etaT) {  // scene/fresnel/DielectricFresnel.java
   float c = clampf(cosi, -1.0f, 1.0f);
@@ -450,16 +460,19 @@ DFC_D float fr_conductor1(float c, float eta, float k) {  // scene/fresnel/Condu
 }
 DFC_D float schlick_w(float c) { float m = clampf(1.0f - c, 0.0f, 1.0f); return (m * m) * (m * m) * m; }  // Schlick.java:104
 DFC_D float lerpf(float a, float b, float t) { return (1.0f - t) * a + t * b; }  // utility/Floats.java:591
-DFC_D V3 fresnel(const Bsdf& B, const Lobe& L, float cosi) {
+template <class BT>
+DFC_D V3 fresnel(const BT& B, const Lobe& L, float cosi) {
   if (L.fresnel == kFresDielectric) { float f = fr_dielectric(cosi, B.fr_i, B.fr_t); return {f, f, f}; }
   if (L.fresnel == kFresConductor) {
     float c = fabsf(cosi);
     return {fr_conductor1(c, B.ca.x, B.cb.x), fr_conductor1(c, B.ca.y, B.cb.y), fr_conductor1(c, B.ca.z, B.cb.z)};
   }
-  if (L.fresnel == kFresDisney) {  // scene/fresnel/DisneyFresnel.java
-    const float d = fr_dielectric(cosi, 1.0f, B.fr_t), w = schlick_w(cosi);
-    return {lerpf(d, lerpf(B.ca.x, 1.0f, w), B.metallic), lerpf(d, lerpf(B.ca.y, 1.0f, w), B.metallic),
-            lerpf(d, lerpf(B.ca.z, 1.0f, w), B.metallic)};
+  if constexpr (kAllLobes<BT>) {
+    if (L.fresnel == kFresDisney) {  // scene/fresnel/DisneyFresnel.java
+      const float d = fr_dielectric(cosi, 1.0f, B.fr_t), w = schlick_w(cosi);
+      return {lerpf(d, lerpf(B.ca.x, 1.0f, w), B.metallic), lerpf(d, lerpf(B.ca.y, 1.0f, w), B.metallic),
+              lerpf(d, lerpf(B.ca.z, 1.0f, w), B.metallic)};
+    }
   }
   return {1, 1, 1};
 }
@@ -537,7 +550,8 @@ DFC_D float smith_ggx(float ct, float alpha) {
   return 1.0f / (ct + sqrtf(a + b - a * b));
 }
 
-DFC_D V3 lobe_f(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
+template <class BT>
+DFC_D V3 lobe_f(const BT& B, const Lobe& L, V3 wo, V3 wi) {
   switch (L.kind) {
     case kLambert: case kLambertBTDF: return L.scale * (1.0f / kPi);
     case kOrenNayar: {
@@ -569,6 +583,9 @@ DFC_D V3 lobe_f(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
       float k = fabsf(tr_D(L, h) * tr_G(L, wo, wi) * eta * eta * fabsf(ih) * fabsf(oh) * b * b / (wi.z * wo.z * a * a));
       return L.scale * ((1.0f - F) * k);
     }
+    default: break;
+  }
+  if constexpr (kAllLobes<BT>) switch (L.kind) {
     case kFresnelBlend: {  // FresnelBlendBRDF.java (scale: diffuse, Bsdf.ca: specular)
       V3 h = wo + wi;
       if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return {0, 0, 0};
@@ -611,12 +628,14 @@ DFC_D V3 lobe_f(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
       const float ss = 1.25f * (fss * (1.0f / (co + ci) - 0.5f) + 0.5f);
       return V3{L.scale.x * (1.0f / kPi) * ss, L.scale.y * (1.0f / kPi) * ss, L.scale.z * (1.0f / kPi) * ss};
     }
-    default: return {0, 0, 0};
+    default: break;
   }
+  return {0, 0, 0};
 }
-DFC_D float lobe_pdf(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
-  switch (L.kind) {
-    case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
+template <class BT>
+DFC_D float lobe_pdf(const BT& B, const Lobe& L, V3 wo, V3 wi) {
+  if constexpr (kAllLobes<BT>) switch (L.kind) {
+    case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
       return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
     case kLambertBTDF: return same_hemi(wo, wi) ? 0.0f : fabsf(wi.z) * (1.0f / kPi);
     case kFresnelBlend: {
@@ -624,6 +643,19 @@ DFC_D float lobe_pdf(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
       const V3 h = normalize(wo + wi);
       return 0.5f * (fabsf(wi.z) * (1.0f / kPi) + tr_pdf(L, wo, h) / (4.0f * dot(wo, h)));
     }
+    case kDisneyClearCoat: {
+      if (!same_hemi(wo, wi)) return 0.0f;
+      V3 h = wi + wo;
+      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return 0.0f;
+      h = normalize(h);
+      const float ch = fabsf(h.z);
+      return gtr1(ch, L.p0) * ch / (4.0f * dot(wo, h));
+    }
+    default: break;
+  }
+  switch (L.kind) {
+    case kLambert: case kOrenNayar:
+      return same_hemi(wo, wi) ? fabsf(wi.z) * (1.0f / kPi) : 0.0f;
     case kTSBRDF: {
       if (!same_hemi(wo, wi)) return 0.0f;
       V3 h = normalize(wo + wi);
@@ -638,20 +670,41 @@ DFC_D float lobe_pdf(const Bsdf& B, const Lobe& L, V3 wo, V3 wi) {
       float a = oh + eta * ih;
       return tr_pdf(L, wo, h) * fabsf((eta * eta * ih) / (a * a));
     }
-    case kDisneyClearCoat: {
-      if (!same_hemi(wo, wi)) return 0.0f;
-      V3 h = wi + wo;
-      if (h.x == 0.0f && h.y == 0.0f && h.z == 0.0f) return 0.0f;
-      h = normalize(h);
-      const float ch = fabsf(h.z);
-      return gtr1(ch, L.p0) * ch / (4.0f * dot(wo, h));
-    }
     default: return 0.0f;
   }
 }
 struct LSample { V3 f, wi; float pdf; int type; };
-DFC_D bool lobe_sample(const Bsdf& B, const Lobe& L, V3 wo, float u, float v, LSample* s) {
+template <class BT>
+DFC_D bool lobe_sample(const BT& B, const Lobe& L, V3 wo, float u, float v, LSample* s) {
   s->type = L.type;
+  if constexpr (kAllLobes<BT>) switch (L.kind) {
+    case kFresnelBlend: {  // FresnelBlendBRDF.java:sampleDistributionFunction
+      V3 wi;
+      if (u < 0.5f) {
+        wi = cosine_hemisphere(fminf(2.0f * u, 0.99999994f), v);
+        if (wo.z < 0.0f) wi.z = -wi.z;
+      } else {
+        const V3 h = tr_sample_h(L, wo, fminf(2.0f * (u - 0.5f), 0.99999994f), v);
+        wi = h * (dot(wo, h) * 2.0f) - wo;
+        if (!same_hemi(wo, wi)) return false;
+      }
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
+    }
+    case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
+      if (wo.z == 0.0f) return false;
+      const float a2 = L.p0 * L.p0;
+      const float ct = sqrtf(fmaxf(0.0f, (1.0f - powf(a2, 1.0f - u)) / (1.0f - a2)));
+      const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+      float sp, cp;
+      sincosf(2.0f * kPi * v, &sp, &cp);
+      V3 h = {st * cp, st * sp, ct};
+      if (!same_hemi(wo, h)) h = -h;
+      const V3 wi = h * (dot(wo, h) * 2.0f) - wo;
+      if (!same_hemi(wo, wi)) return false;
+      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
+    }
+    default: break;
+  }
   switch (L.kind) {
     case kLambert: case kOrenNayar: case kDisneyDiffuse: case kDisneyFakeSS: case kDisneyRetro: case kDisneySheen:
     case kLambertBTDF: {
@@ -701,31 +754,7 @@ DFC_D bool lobe_sample(const Bsdf& B, const Lobe& L, V3 wo, float u, float v, LS
       if (!refract(wo, h, eta, &wi)) return false;
       s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
     }
-    case kFresnelBlend: {  // FresnelBlendBRDF.java:sampleDistributionFunction
-      V3 wi;
-      if (u < 0.5f) {
-        wi = cosine_hemisphere(fminf(2.0f * u, 0.99999994f), v);
-        if (wo.z < 0.0f) wi.z = -wi.z;
-      } else {
-        const V3 h = tr_sample_h(L, wo, fminf(2.0f * (u - 0.5f), 0.99999994f), v);
-        wi = h * (dot(wo, h) * 2.0f) - wo;
-        if (!same_hemi(wo, wi)) return false;
-      }
-      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
-    }
-    case kDisneyClearCoat: {  // DisneyClearCoatBRDF.java:sampleDistributionFunction
-      if (wo.z == 0.0f) return false;
-      const float a2 = L.p0 * L.p0;
-      const float ct = sqrtf(fmaxf(0.0f, (1.0f - powf(a2, 1.0f - u)) / (1.0f - a2)));
-      const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-      float sp, cp;
-      sincosf(2.0f * kPi * v, &sp, &cp);
-      V3 h = {st * cp, st * sp, ct};
-      if (!same_hemi(wo, h)) h = -h;
-      const V3 wi = h * (dot(wo, h) * 2.0f) - wo;
-      if (!same_hemi(wo, wi)) return false;
-      s->wi = wi; s->f = lobe_f(B, L, wo, wi); s->pdf = lobe_pdf(B, L, wo, wi); return true;
-    }
+    default: break;
   }
   return false;
 }
@@ -739,6 +768,20 @@ DFC_D Lobe make_lobe(int kind, int type, V3 scale, float p0 = 0.0f, float p1 = 0
   return L;
 }
 DFC_D Lobe tr_lobe(int kind, int type, V3 scale, float ax, float ay) { return make_lobe(kind, type, scale, fmaxf(ax, 0.001f), fmaxf(ay, 0.001f)); }
+
+// Appends a lobe.  The two-lobe form writes its slots by selects, so that no
+// indexed store moves its lobes to local memory.
+template <int N>
+DFC_D void push_lobe(BsdfN<N>* B, const Lobe& L) {
+  if constexpr (N <= kSimpleLobes) {
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      if (B->n == k) B->l[k] = L;
+  } else {
+    B->l[B->n] = L;
+  }
+  ++B->n;
+}
 
 // DisneyMaterial.computeScatteringFunctions (scene/material/DisneyMaterial.java:1121-1210)
 // from the per-material quantities ingest computed (DMaterial comments).
@@ -782,95 +825,107 @@ DFC_D void build_disney(const DMaterial& m, Bsdf* B) {
 // Returns false when the material gives no BSDF (the ray passes through).
 // multi = isAllowingMultipleLobes: false (the ray tracer) builds smooth glass
 // as separate specular reflection and transmission lobes (GlassMaterial.java:520).
-DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_material, Bsdf* B, bool multi = true) {
+// With fewer than kMaxLobes lobes (SimpleBsdf) only the matte, mirror, glass,
+// metal and plastic kinds are built; the shading kernels route the others to
+// the full Bsdf by the material sort.
+template <int N>
+DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_material, BsdfN<N>* B, bool multi = true) {
   B->n = 0; B->eta = 1.0f;
   B->fr_i = 1.0f; B->fr_t = 1.0f; B->bt_a = 1.0f; B->bt_b = 1.0f; B->metallic = 0.0f;
   B->ca = V3{0, 0, 0}; B->cb = V3{0, 0, 0};
   switch (m.kind) {
     case kMatLambert: case kMatOrenNayar:
-      B->l[B->n++] = make_lobe(m.kind == kMatLambert ? kLambert : kOrenNayar, kRefl | kDiffuse, ld3(m.c0), m.on_a, m.on_b);
+      push_lobe(B, make_lobe(m.kind == kMatLambert ? kLambert : kOrenNayar, kRefl | kDiffuse, ld3(m.c0), m.on_a, m.on_b));
       break;
     case kMatMirror:
-      B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0));
+      push_lobe(B, make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0)));
       break;
     case kMatGlassSpec:
       if (multi) {
-        B->l[B->n++] = make_lobe(kFresnelSpec, kRefl | kTrans | kSpecular, ld3(m.c0));
+        push_lobe(B, make_lobe(kFresnelSpec, kRefl | kTrans | kSpecular, ld3(m.c0)));
         B->ca = ld3(m.c1);
       } else {
-        if (m.has_kr) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0)); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
-        if (m.has_kt) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c1), 1.0f, m.eta);
+        if (m.has_kr) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c0)); L.fresnel = kFresDielectric; push_lobe(B, L); }
+        if (m.has_kt) push_lobe(B, make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c1), 1.0f, m.eta));
         B->fr_i = 1.0f; B->fr_t = m.eta;
       }
       B->bt_a = 1.0f; B->bt_b = m.eta; B->eta = m.eta;
       break;
     case kMatGlassRough: {
-      if (m.has_kr) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
-      if (m.has_kt) B->l[B->n++] = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c1), m.ax, m.ay);
+      if (m.has_kr) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay); L.fresnel = kFresDielectric; push_lobe(B, L); }
+      if (m.has_kt) push_lobe(B, tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c1), m.ax, m.ay));
       B->fr_i = 1.0f; B->fr_t = m.eta; B->bt_a = 1.0f; B->bt_b = m.eta; B->eta = m.eta;
       break;
     }
     case kMatMetal: {
       Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, V3{1, 1, 1}, m.ax, m.ay);
       L.fresnel = kFresConductor;
-      B->l[B->n++] = L;
+      push_lobe(B, L);
       B->ca = ld3(m.c1); B->cb = ld3(m.c2);
       break;
     }
     case kMatPlastic: {
-      if (m.has_kr) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
-      if (m.has_kt) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
+      if (m.has_kr) push_lobe(B, make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0)));
+      if (m.has_kt) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; push_lobe(B, L); }
       B->fr_i = 1.5f; B->fr_t = 1.0f;
       break;
     }
-    case kMatDisney: build_disney(m, B); break;
-    case kMatClearCoat: {  // ClearCoatMaterial.java:computeScatteringFunctions
-      const V3 n = sf.s.w;
-      const V3 nco = dot(n, ray_d) > 0.0f ? -n : n;  // Intersection.getSurfaceNormalSCorrectlyOriented
-      const bool entering = dot(n, nco) > 0.0f;
-      const float etaI = entering ? 1.0f : 1.5f, etaT = entering ? 1.5f : 1.0f;
-      V3 refr;
-      if (refract(ray_d, nco, etaI / etaT, &refr)) {  // Vector3F.refraction(direction, normal, eta)
-        const float cosi = dot(ray_d, nco);
-        const float R = fr_dielectric(entering ? -cosi : dot(refr, n), 1.0f, 1.5f), T = 1.0f - R;
-        const float p = 0.25f + 0.5f * R;
-        if (u_material < p) B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1) * (R / p));
-        else B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0) * (T / (1.0f - p)));
+    default:
+      if constexpr (N >= kMaxLobes) {
+        switch (m.kind) {
+        case kMatDisney: build_disney(m, B); break;
+        case kMatClearCoat: {  // ClearCoatMaterial.java:computeScatteringFunctions
+          const V3 n = sf.s.w;
+          const V3 nco = dot(n, ray_d) > 0.0f ? -n : n;  // Intersection.getSurfaceNormalSCorrectlyOriented
+          const bool entering = dot(n, nco) > 0.0f;
+          const float etaI = entering ? 1.0f : 1.5f, etaT = entering ? 1.5f : 1.0f;
+          V3 refr;
+          if (refract(ray_d, nco, etaI / etaT, &refr)) {  // Vector3F.refraction(direction, normal, eta)
+            const float cosi = dot(ray_d, nco);
+            const float R = fr_dielectric(entering ? -cosi : dot(refr, n), 1.0f, 1.5f), T = 1.0f - R;
+            const float p = 0.25f + 0.5f * R;
+            if (u_material < p) push_lobe(B, make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1) * (R / p)));
+            else push_lobe(B, make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0) * (T / (1.0f - p))));
+          } else {
+            push_lobe(B, make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1)));
+          }
+          break;
+        }
+        case kMatGlossy: {
+          Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay);
+          L.fresnel = kFresConductor;
+          push_lobe(B, L);
+          B->ca = ld3(m.c1); B->cb = ld3(m.c2);
+          break;
+        }
+        case kMatSubstrate:
+          push_lobe(B, tr_lobe(kFresnelBlend, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay));
+          B->ca = ld3(m.c1);
+          break;
+        case kMatTranslucent: {
+          if (m.flags & 1) push_lobe(B, make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0)));
+          if (m.flags & 2) push_lobe(B, make_lobe(kLambertBTDF, kTrans | kDiffuse, ld3(m.c1)));
+          if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c2), m.ax, m.ay); L.fresnel = kFresDielectric; push_lobe(B, L); }
+          if (m.flags & 8) push_lobe(B, tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c3), m.ax, m.ay));
+          B->fr_i = 1.0f; B->fr_t = 1.5f; B->bt_a = 1.0f; B->bt_b = 1.5f;
+          break;
+        }
+        case kMatUber: {
+          if (m.flags & 1) push_lobe(B, make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c4), 1.0f, 1.0f));
+          if (m.flags & 2) push_lobe(B, make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0)));
+          if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; push_lobe(B, L); }
+          if (m.flags & 8) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c2)); L.fresnel = kFresDielectric; push_lobe(B, L); }
+          if (m.flags & 16) push_lobe(B, make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c3), 1.0f, m.eta));
+          B->fr_i = 1.0f; B->fr_t = m.eta;
+          B->eta = (m.flags & 1) ? 1.0f : m.eta;
+          break;
+        }
+        default: return false;
+        }
+        break;
       } else {
-        B->l[B->n++] = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c1));
+        return false;
       }
-      break;
-    }
-    case kMatGlossy: {
-      Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay);
-      L.fresnel = kFresConductor;
-      B->l[B->n++] = L;
-      B->ca = ld3(m.c1); B->cb = ld3(m.c2);
-      break;
-    }
-    case kMatSubstrate:
-      B->l[B->n++] = tr_lobe(kFresnelBlend, kRefl | kGlossy, ld3(m.c0), m.ax, m.ay);
-      B->ca = ld3(m.c1);
-      break;
-    case kMatTranslucent: {
-      if (m.flags & 1) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
-      if (m.flags & 2) B->l[B->n++] = make_lobe(kLambertBTDF, kTrans | kDiffuse, ld3(m.c1));
-      if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c2), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
-      if (m.flags & 8) B->l[B->n++] = tr_lobe(kTSBTDF, kTrans | kGlossy, ld3(m.c3), m.ax, m.ay);
-      B->fr_i = 1.0f; B->fr_t = 1.5f; B->bt_a = 1.0f; B->bt_b = 1.5f;
-      break;
-    }
-    case kMatUber: {
-      if (m.flags & 1) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c4), 1.0f, 1.0f);
-      if (m.flags & 2) B->l[B->n++] = make_lobe(kLambert, kRefl | kDiffuse, ld3(m.c0));
-      if (m.flags & 4) { Lobe L = tr_lobe(kTSBRDF, kRefl | kGlossy, ld3(m.c1), m.ax, m.ay); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
-      if (m.flags & 8) { Lobe L = make_lobe(kSpecBRDF, kRefl | kSpecular, ld3(m.c2)); L.fresnel = kFresDielectric; B->l[B->n++] = L; }
-      if (m.flags & 16) B->l[B->n++] = make_lobe(kSpecBTDF, kTrans | kSpecular, ld3(m.c3), 1.0f, m.eta);
-      B->fr_i = 1.0f; B->fr_t = m.eta;
-      B->eta = (m.flags & 1) ? 1.0f : m.eta;
-      break;
-    }
-    default: return false;
   }
   B->s = sf.s;
   B->ng = sf.g.w;
@@ -878,37 +933,62 @@ DFC_D bool build_bsdf(const DMaterial& m, const Surface& sf, V3 ray_d, float u_m
   B->wo = normalize(to_local(B->wo_w, B->s));
   return B->n > 0 || m.kind == kMatUber;  // UberMaterial gives a BSDF even without lobes: the path ends there
 }
-DFC_D V3 bsdf_f(const Bsdf& B, int flags, V3 wi_w) {
+// The lobe loops run over the N slots of the BSDF, unrolled for the two-lobe
+// form so that its lobes stay in registers.
+template <int N>
+DFC_D V3 bsdf_f(const BsdfN<N>& B, int flags, V3 wi_w) {
   V3 wi = normalize(to_local(wi_w, B.s));
   bool refl = dot(wi_w, B.ng) * dot(B.wo_w, B.ng) > 0.0f;
   V3 r = {0, 0, 0};
-  for (int k = 0; k < B.n; ++k) {
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+  for (int k = 0; k < N; ++k) {
+    if (k >= B.n) break;
     const Lobe& L = B.l[k];
     if (type_match(L.type, flags) && ((refl && (L.type & kRefl)) || (!refl && (L.type & kTrans)))) r = r + lobe_f(B, L, B.wo, wi);
   }
   return r;
 }
-DFC_D float bsdf_pdf(const Bsdf& B, int flags, V3 wi_w) {
+template <int N>
+DFC_D float bsdf_pdf(const BsdfN<N>& B, int flags, V3 wi_w) {
   if (B.n == 0 || B.wo.z == 0.0f) return 0.0f;
   V3 wi = normalize(to_local(wi_w, B.s));
   float p = 0.0f;
   int m = 0;
-  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) { ++m; p += lobe_pdf(B, B.l[k], B.wo, wi); }
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+  for (int k = 0; k < N; ++k) {
+    if (k >= B.n) break;
+    if (type_match(B.l[k].type, flags)) { ++m; p += lobe_pdf(B, B.l[k], B.wo, wi); }
+  }
   return m > 1 ? p / m : p;
 }
 struct BSample { V3 f, wi; float pdf; int type; };
 // scene/BSDF.java:323 sampleDistributionFunction
-DFC_D bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BSample* out) {
+template <int N>
+DFC_D bool bsdf_sample(const BsdfN<N>& B, int flags, float u, float v, BSample* out) {
   if (B.wo.z == 0.0f) return false;
   int m = 0, match_k = -1;
-  for (int k = 0; k < B.n; ++k) if (type_match(B.l[k].type, flags)) ++m;
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+  for (int k = 0; k < N; ++k) {
+    if (k >= B.n) break;
+    if (type_match(B.l[k].type, flags)) ++m;
+  }
   if (m == 0) return false;
   const int match = min((int)floorf(u * m), m - 1);
-  for (int k = 0, j = 0; k < B.n; ++k) {
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+  for (int k = 0, j = 0; k < N; ++k) {
+    if (k >= B.n) break;
     if (!type_match(B.l[k].type, flags)) continue;
     if (j++ == match) { match_k = k; break; }
   }
-  const Lobe& L = B.l[match_k];
+  Lobe L;
+  if constexpr (N <= kSimpleLobes) {  // a select, not an indexed (local-memory) read
+    L = B.l[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k)
+      if (match_k == k) L = B.l[k];
+  } else {
+    L = B.l[match_k];
+  }
   LSample s;
   if (!lobe_sample(B, L, B.wo, fminf(u * m - match, 0.99999994f), v, &s)) return false;
   V3 wiw = normalize(to_world(s.wi, B.s));
@@ -917,7 +997,9 @@ DFC_D bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BSample* out)
   if (!is_spec(L.type)) {
     bool refl = dot(wiw, B.ng) * dot(B.wo_w, B.ng) > 0.0f;
     f = {0, 0, 0};
-    for (int k = 0; k < B.n; ++k) {
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+    for (int k = 0; k < N; ++k) {
+      if (k >= B.n) break;
       const Lobe& O = B.l[k];
       if (!type_match(O.type, flags)) continue;
       if (k != match_k) pdf += lobe_pdf(B, O, B.wo, s.wi);
@@ -928,7 +1010,16 @@ DFC_D bool bsdf_sample(const Bsdf& B, int flags, float u, float v, BSample* out)
   out->f = f; out->wi = wiw; out->pdf = pdf; out->type = s.type;
   return true;
 }
-DFC_D int bsdf_nonspec(const Bsdf& B) { int c = 0; for (int k = 0; k < B.n; ++k) c += is_spec(B.l[k].type) ? 0 : 1; return c; }
+template <int N>
+DFC_D int bsdf_nonspec(const BsdfN<N>& B) {
+  int c = 0;
+#pragma unroll(N <= kSimpleLobes ? N : 1)
+  for (int k = 0; k < N; ++k) {
+    if (k >= B.n) break;
+    c += is_spec(B.l[k].type) ? 0 : 1;
+  }
+  return c;
+}
 
 // ---------------------------------------------------------------- lights --
 // sampler/Distribution1F.java + Distribution2F.java over the packed array form.

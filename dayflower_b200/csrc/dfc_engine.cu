@@ -4,7 +4,8 @@
 // Device side (dfc_kernels.cu): a fixed pool of `capacity` path slots.  One
 // bounce iteration is
 //   k_batch_plan -> k_batch_regen -> k_trace_batch -> k_sort_count_batch
-//   -> k_sort_scatter -> k_shade_path_batch
+//   -> k_sort_scatter -> k_shade_path_batch_simple -> k_shade_path_batch
+//   -> k_shade_inline_batch (AMBIENT_OCCLUSION and RAY_TRACING jobs)
 // Regen starts new paths of admitted jobs in the slots the previous shade
 // retired, so jobs that arrive while others run join the wavefront at the
 // next iteration.  Every count the kernels need lives in device memory, so
@@ -21,6 +22,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -44,7 +46,8 @@ using namespace dfc;
 namespace {
 
 constexpr int kMaxScenes = 64;
-static_assert(kJobPathTracing == DFC_JOB_PATH_TRACING && kJobRayCasting == DFC_JOB_RAY_CASTING && kJobDepthCamera == DFC_JOB_DEPTH_CAMERA,
+static_assert(kJobPathTracing == DFC_JOB_PATH_TRACING && kJobRayCasting == DFC_JOB_RAY_CASTING && kJobDepthCamera == DFC_JOB_DEPTH_CAMERA &&
+                  kJobAmbientOcclusion == DFC_JOB_AMBIENT_OCCLUSION && kJobRayTracing == DFC_JOB_RAY_TRACING,
               "job kinds of the kernels and of the C ABI");
 constexpr unsigned kJobRing = 4096;    // job records on the device (power of two)
 constexpr unsigned kSegRing = 65536;   // segment records on the device (power of two)
@@ -83,6 +86,7 @@ struct dfc_engine {
   int bvh_builder = DFC_BVH_DEVICE;  // mesh hierarchies of later scene commits
   int sm_count = 148;
   int max_trace_blocks = 6;
+  int inline_blocks = 2;  // resident blocks per SM of k_shade_inline_batch
   cudaStream_t stream = nullptr, upload_stream = nullptr, read_stream = nullptr;
   cudaEvent_t ev_order = nullptr;
   // `mu` guards all host state and every enqueue on `stream`; nothing waits
@@ -180,7 +184,7 @@ dfc_engine_config resolved(const dfc_engine* e, dfc_engine_config c) {
   if (c.shade_threads != 128) c.shade_threads = 256;
   if (c.iterations_per_launch <= 0) c.iterations_per_launch = 4;
   c.iterations_per_launch += c.iterations_per_launch & 1;  // even: the graph ends on the parity it started with
-  if (c.policy != DFC_SCHEDULE_FIFO) c.policy = DFC_SCHEDULE_ROUND_ROBIN;
+  if (c.policy != DFC_SCHEDULE_FIFO && c.policy != DFC_SCHEDULE_SHORTEST_FIRST) c.policy = DFC_SCHEDULE_ROUND_ROBIN;
   c.reserved = 0;
   if (c.segment_paths <= 0) c.segment_paths = kDefaultSegment;
   if (c.lookahead_paths <= 0) c.lookahead_paths = 8 * c.capacity;
@@ -257,6 +261,7 @@ void iteration_args(dfc_engine* e, int b, BatchArgs* ba, TraceArgs* ta, SortArgs
   sa->state = st;
   sa->paths = P;
   sa->pixels = 0;
+  sa->overflow = e->d_overflow.as<unsigned>();
   sa->work_list = so->sorted;
   sa->work_count = so->work_count;
   sa->next_work_list = e->d_work_list[b ^ 1].as<unsigned>();
@@ -273,7 +278,7 @@ void iteration_args(dfc_engine* e, int b, BatchArgs* ba, TraceArgs* ta, SortArgs
   sa->pend_mis = e->d_pend_m.as<float4>();
 }
 
-constexpr int kKernelsPerIteration = 6;
+constexpr int kKernelsPerIteration = 8;
 
 void enqueue_iteration(dfc_engine* e, int b, int variant) {
   BatchArgs ba;
@@ -288,8 +293,23 @@ void enqueue_iteration(dfc_engine* e, int b, int variant) {
   (variant >= 1 ? k_trace_batch_records : k_trace_batch)<<<e->sm_count * c.trace_blocks_per_sm, kTraceThreads, 0, e->stream>>>(ta);
   k_sort_count_batch<<<shade_grid, 256, 0, e->stream>>>(so);
   k_sort_scatter<<<shade_grid, 256, 0, e->stream>>>(so);
+  // the two-lobe kernel over the matte ... plastic hits, misses and light-ray-only paths, the general one over the rest
+  ShadeArgs simple = sa;
+  simple.range_bins = so.bins;
+  simple.range_lo = 0;
+  simple.range_hi = kSimpleBins;
+  (variant >= 1 ? k_shade_path_batch_simple_records : k_shade_path_batch_simple)<<<shade_grid, 256, 0, e->stream>>>(simple);
+  ShadeArgs full = sa;
+  full.range_bins = so.bins;
+  full.range_lo = kSimpleBins;
+  full.range_hi = kKeyInline;
   (variant == 2 ? k_shade_path_batch_textured : variant == 1 ? k_shade_path_batch_records : k_shade_path_batch)
-      <<<shade_grid, c.shade_threads, 0, e->stream>>>(sa);
+      <<<shade_grid, c.shade_threads, 0, e->stream>>>(full);
+  // AMBIENT_OCCLUSION and RAY_TRACING paths finish in one step, tracing their rays on their own threads
+  sa.range_bins = so.bins;
+  sa.range_lo = kKeyInline;
+  sa.range_hi = kSortBins;
+  k_shade_inline_batch<<<e->sm_count * e->inline_blocks, kTraceThreads, 0, e->stream>>>(sa);
 }
 
 // Captures iterations_per_launch iterations (alternating parity) into the graph.
@@ -460,6 +480,8 @@ int service(dfc_engine* e, bool idle_device) {
     dj.min_rr = J.d.minimum_bounce_russian_roulette;
     dj.seed = J.d.seed;
     dj.kind = J.d.kind;
+    dj.ao_samples = J.d.ambient_occlusion_samples;
+    dj.ao_distance = J.d.maximum_distance;
     dj.cancelled = 0;
     dj.film_sum = static_cast<float4*>(film);
     dj.film_sq = static_cast<float4*>(film) + pixels;
@@ -489,7 +511,15 @@ int service(dfc_engine* e, bool idle_device) {
     while (backlog < (unsigned long long)c.lookahead_paths && !e->sched.empty() &&
            e->seg_next + (unsigned)add.size() - e->seg_lo < kSegRing) {
       if (e->rr >= e->sched.size()) e->rr = 0;
-      const size_t pick = c.policy == DFC_SCHEDULE_FIFO ? 0 : e->rr;
+      size_t pick = c.policy == DFC_SCHEDULE_FIFO ? 0 : e->rr;
+      if (c.policy == DFC_SCHEDULE_SHORTEST_FIRST) {  // the admitted job with the fewest paths left to hand out
+        unsigned long long best = ~0ull;
+        for (size_t q = 0; q < e->sched.size(); ++q) {
+          auto jt = e->jobs.find(e->sched[q]);
+          const unsigned long long left = jt == e->jobs.end() ? 0ull : jt->second.paths - std::min(jt->second.appended, jt->second.paths);
+          if (left < best) { best = left; pick = q; }
+        }
+      }
       const int64_t id = e->sched[pick];
       auto it = e->jobs.find(id);
       if (it == e->jobs.end() || it->second.state != DFC_JOB_RUNNING || it->second.cancel_req ||
@@ -509,7 +539,7 @@ int service(dfc_engine* e, bool idle_device) {
       e->admitted_paths += n;
       backlog += n;
       if (J.appended >= J.paths) e->sched.erase(e->sched.begin() + (long)pick);
-      else if (c.policy != DFC_SCHEDULE_FIFO) e->rr = pick + 1;
+      else if (c.policy == DFC_SCHEDULE_ROUND_ROBIN) e->rr = pick + 1;
     }
     // one copy per contiguous run of ring slots
     size_t k = 0;
@@ -734,6 +764,8 @@ int dfc_engine_create(int device, int64_t budget, dfc_engine** out) {
   nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_batch_records, kTraceThreads, 0) == cudaSuccess && nb > 0)
     e->max_trace_blocks = std::min(e->max_trace_blocks, nb);
+  nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade_inline_batch, kTraceThreads, 0) == cudaSuccess && nb > 0) e->inline_blocks = nb;
   cudaGetLastError();
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return DFC_E_CUDA;
@@ -909,8 +941,12 @@ int dfc_job_submit(dfc_engine* e, const dfc_job_desc* d, int64_t* job_id) {
   if (d->samples < 1) return efail(e, DFC_E_INVALID_ARG, "renderPasses < 1");  // AbstractGPURenderer.java:323
   if (d->maximum_bounce < 0 || d->maximum_bounce > 4096) return efail(e, DFC_E_INVALID_ARG, "maximumBounce out of range");
   if (d->minimum_bounce_russian_roulette < 0) return efail(e, DFC_E_INVALID_ARG, "minimumBounceRussianRoulette out of range");
-  if (d->kind != DFC_JOB_PATH_TRACING && d->kind != DFC_JOB_RAY_CASTING && d->kind != DFC_JOB_DEPTH_CAMERA)
-    return efail(e, DFC_E_UNSUPPORTED, "engine jobs are PATH_TRACING, RAY_CASTING or DEPTH_CAMERA");
+  if (d->kind < DFC_JOB_PATH_TRACING || d->kind > DFC_JOB_RAY_TRACING) return efail(e, DFC_E_INVALID_ARG, "unknown job kind");
+  if (d->kind == DFC_JOB_AMBIENT_OCCLUSION) {
+    if (d->ambient_occlusion_samples < 1 || d->ambient_occlusion_samples > 4096)
+      return efail(e, DFC_E_INVALID_ARG, "samples out of range");  // setSamples, AbstractGPURenderer.java:515
+    if (!std::isfinite(d->maximum_distance)) return efail(e, DFC_E_INVALID_ARG, "maximumDistance must be finite");
+  }
   const int64_t id = e->next_id++;
   JobRec J;
   J.d = *d;

@@ -9,7 +9,7 @@ namespace dfc {
 
 enum { DFC_ALGO_AO = 0, DFC_ALGO_DEPTH = 1, DFC_ALGO_PATH = 2, DFC_ALGO_RAY_CASTING = 3, DFC_ALGO_RAY_TRACING = 4 };
 // DJob::kind (the C ABI's DFC_JOB_* values)
-enum : int { kJobPathTracing = 0, kJobRayCasting = 1, kJobDepthCamera = 2 };
+enum : int { kJobPathTracing = 0, kJobRayCasting = 1, kJobDepthCamera = 2, kJobAmbientOcclusion = 3, kJobRayTracing = 4 };
 
 // Path flags (PathMeta.w)
 enum : unsigned { kFlagAlive = 1u, kFlagSpecular = 2u, kFlagPendShadow = 4u, kFlagPendMis = 8u, kFlagShadowAny = 16u, kFlagNoSample = 32u };
@@ -24,7 +24,9 @@ struct DJob {
   unsigned width, pixels;
   int max_bounce, min_rr;
   uint32_t seed;
-  int kind;                  // kJobPathTracing, kJobRayCasting or kJobDepthCamera
+  int kind;                  // kJob*
+  int ao_samples;            // AMBIENT_OCCLUSION: rays per camera sample
+  float ao_distance;         //                    maximum distance (<= 0: occlusion only)
   unsigned cancelled;        // 1: start no more paths of this job (the plan skips them)
   float4* film_sum;          // per pixel: sum of accepted samples (xyz), count (w)
   float4* film_sq;           // per pixel: sum of squares (xyz)
@@ -111,6 +113,12 @@ struct ShadeArgs {
   int max_bounce, min_rr, preview, last_step, record_primary, ao_samples;
   const unsigned* work_list;
   const unsigned* work_count;
+  // When set, the kernel shades only the work items of sort keys
+  // [range_lo, range_hi): a range of the sorted work list found from these
+  // bin counts (SortArgs::bins of this step).
+  const unsigned* range_bins;
+  int range_lo, range_hi;
+  unsigned* overflow;  // batch engine: traversal stack bound exceeded (the inline AO and ray-tracing kernel)
   unsigned* next_work_list;
   unsigned* next_work_count;
   unsigned* next_ray_list;
@@ -147,10 +155,19 @@ struct AoArgs {
   unsigned* overflow;
 };
 
-// Material sort of a shade work list: key = material kind of the extension
-// hit (0 .. kMatKinds-1), kMatKinds for a miss, kMatKinds + 1 for a path with
-// nothing left to shade (pending light rays only).
-constexpr int kSortBins = kMatKinds + 2;
+// Material sort of a shade work list by the material kind of the extension
+// hit.  The keys put the kinds whose BSDF has at most two lobes (no BSDF,
+// matte, mirror, glass, metal, plastic: kinds 0 .. kSimpleKinds - 1) first,
+// then a miss, then a path with nothing left to shade (pending light rays
+// only), then the other kinds; the first kSimpleBins keys are shaded by the
+// two-lobe kernel, the rest by the general one.
+constexpr int kSortBins = kMatKinds + 3;
+constexpr int kKeyInline = kMatKinds + 2;  // batch engine: AMBIENT_OCCLUSION and RAY_TRACING paths (k_shade_inline_batch)
+constexpr int kSimpleKinds = kMatPlastic + 1;
+constexpr int kKeyMiss = kSimpleKinds;
+constexpr int kKeyNothing = kSimpleKinds + 1;
+constexpr int kSimpleBins = kSimpleKinds + 2;
+__host__ __device__ inline int material_sort_key(int kind) { return kind < kSimpleKinds ? kind : kind + 2; }
 struct SortArgs {
   SceneView scene;
   const SceneView* scenes;  // batch engine only (see TraceArgs)
@@ -207,6 +224,11 @@ __global__ void k_trace_batch(TraceArgs a);          // batch engine: scene per 
 __global__ void k_trace_batch_records(TraceArgs a);
 __global__ void k_shade_path(ShadeArgs a);
 __global__ void k_shade_path_records(ShadeArgs a);  // with the disk ... torus surfaces
+// two-lobe BSDFs only (the material kinds below kSimpleKinds), in registers, at four blocks per SM
+__global__ void k_shade_path_simple(ShadeArgs a);
+__global__ void k_shade_path_simple_records(ShadeArgs a);
+__global__ void k_shade_path_batch_simple(ShadeArgs a);
+__global__ void k_shade_path_batch_simple_records(ShadeArgs a);
 __global__ void k_shade_path_batch(ShadeArgs a);     // batch engine: scene, film and limits per path from the job table
 __global__ void k_shade_path_batch_records(ShadeArgs a);
 // with record shapes and materials evaluated per hit (textures, modifiers, composite materials)
@@ -222,6 +244,8 @@ __global__ void k_trace_ao(AoArgs a);
 // sample walks the sample's specular reflection/transmission tree depth first.
 __global__ void k_ray_trace(ShadeArgs a, unsigned* overflow, unsigned long long* rays);
 __global__ void k_ao_resolve(ShadeArgs a, const float* ao_value, int samples);
+// Batch engine: AMBIENT_OCCLUSION and RAY_TRACING paths, finished in one step (sort key kKeyInline).
+__global__ void k_shade_inline_batch(ShadeArgs a);
 // film_consts: nullptr for the box film (mean, tone mapper, sRGB); else the
 // PixelImageF resolve (filmRender: XYZ -> RGB over the weight sum, negative
 // parts dropped, sRGB) with the XYZ -> sRGB matrix at film_consts[265, 274).

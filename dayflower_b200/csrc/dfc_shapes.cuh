@@ -258,7 +258,7 @@ DFC_D float polygon_t(const float* q, V3 o, V3 d, float tmin, float tmax) {  // 
 
 // Object-space t of one record shape; -1 on a miss.  Out of line, so that
 // its double-precision torus solve stays out of the traversal loop's frame.
-__device__ __noinline__ float record_shape_t(int shape, const float* q, V3 o, V3 d, float tmin, float tmax) {
+static __device__ __noinline__ float record_shape_t(int shape, const float* q, V3 o, V3 d, float tmin, float tmax) {
   switch (shape) {
     case kShapeDisk: return disk_t(q, o, d, tmin, tmax);
     case kShapeCuboid: return cuboid_t(q, o, d, tmin, tmax);
@@ -280,7 +280,7 @@ DFC_D ONB uv_frame(V3 u, V3 v) {
 
 // Surface of a record shape at object-space distance t (doCreateSurfaceIntersection
 // of each shape class).  Out of line: shading reaches it only for these shapes.
-__device__ __noinline__ Surface record_shape_surface(int shape, const float* q, V3 o, V3 d, float t) {
+static __device__ __noinline__ Surface record_shape_surface(int shape, const float* q, V3 o, V3 d, float t) {
   Surface s;
   V3 p = point_at(o, d, t);
   const V3 pu = {-q[0] * p.y, q[0] * p.x, 0.0f};

@@ -151,7 +151,7 @@ DFC_D V3 tx_texel(const unsigned* px, int rx, int ry, int x, int y) {
 // Texture.getColor for one node; pattern textures walk to the chosen child,
 // BlendTexture evaluates both children (nesting bounded by D).
 template <int D>
-__device__ __noinline__ V3 tex_eval(const SceneView& S, int node, const TexCtx& c) {
+static __device__ __noinline__ V3 tex_eval(const SceneView& S, int node, const TexCtx& c) {
   for (int guard = 0; guard < 64 && node >= 0; ++guard) {
     const DTexture& t = S.textures[node];
     switch (t.kind) {
@@ -269,7 +269,7 @@ DFC_D V3 object_point(const DPrim& pr, const Surface& sf) { return pr.identity ?
 // Material.computeScatteringFunctions up to the BSDF build for a kMatTextured
 // material: modifier (changes the hit's shading frame for the rest of the
 // bounce), texture evaluation at the modified hit, derivation of the constants.
-__device__ __noinline__ void eval_textured(const SceneView& S, int tm_index, V3 p_obj, V3 ray_d, Surface* sf, DMaterial* out) {
+static __device__ __noinline__ void eval_textured(const SceneView& S, int tm_index, V3 p_obj, V3 ray_d, Surface* sf, DMaterial* out) {
   const DTexMaterial& tm = S.texmats[tm_index];
   if (tm.modifier >= 0) apply_modifier(S, tm.modifier, sf);
   const TexCtx c{sf->p, p_obj, sf->s.w, ray_d, sf->tu, sf->tv};
@@ -288,7 +288,7 @@ __device__ __noinline__ void eval_textured(const SceneView& S, int tm_index, V3 
 // change sf's shading frame, which the caller keeps for the rest of the
 // bounce).  Out of line, so that the shading kernels' common path (constant
 // materials, build_bsdf inline) keeps its register allocation.
-__device__ __noinline__ bool textured_bsdf(const SceneView& S, const DPrim& pr, V3 ray_d, float u_material, bool multi, Surface* sf,
+static __device__ __noinline__ bool textured_bsdf(const SceneView& S, const DPrim& pr, V3 ray_d, float u_material, bool multi, Surface* sf,
                                            Bsdf* B) {
   int mat = pr.material;
   const V3 p_obj = object_point(pr, *sf);
@@ -300,7 +300,7 @@ __device__ __noinline__ bool textured_bsdf(const SceneView& S, const DPrim& pr, 
 }
 
 // Material.emittance at this hit: the (picked) material's emission texture, on the unmodified hit.
-__device__ __noinline__ V3 hit_material_emission(const SceneView& S, const DPrim& pr, V3 ray_d, const Surface& sf) {
+static __device__ __noinline__ V3 hit_material_emission(const SceneView& S, const DPrim& pr, V3 ray_d, const Surface& sf) {
   int mat = pr.material;
   const V3 p_obj = object_point(pr, sf);
   if (S.materials[mat].kind == kMatComposite) mat = resolve_composite(S, mat, p_obj, sf.tu, sf.tv);

@@ -36,10 +36,12 @@ JOB_STATE_NAMES = {JOB_QUEUED: "queued", JOB_RUNNING: "running", JOB_DONE: "done
 class JobDesc(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_int32), ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("samples", ctypes.c_int32),
                 ("maximum_bounce", ctypes.c_int32), ("minimum_bounce_russian_roulette", ctypes.c_int32),
-                ("seed", ctypes.c_uint32), ("kind", ctypes.c_int32)]
+                ("seed", ctypes.c_uint32), ("kind", ctypes.c_int32), ("ambient_occlusion_samples", ctypes.c_int32),
+                ("maximum_distance", ctypes.c_float)]
 
 
-JOB_PATH_TRACING, JOB_RAY_CASTING, JOB_DEPTH_CAMERA = 0, 1, 2
+# dfc_job_desc.kind: the RenderingAlgorithm of the job (GPURenderer.run dispatches on it, GPURenderer.java:65-77)
+JOB_PATH_TRACING, JOB_RAY_CASTING, JOB_DEPTH_CAMERA, JOB_AMBIENT_OCCLUSION, JOB_RAY_TRACING = 0, 1, 2, 3, 4
 
 
 class JobInfo(ctypes.Structure):
@@ -47,7 +49,7 @@ class JobInfo(ctypes.Structure):
                 ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
 
 
-SCHEDULE_ROUND_ROBIN, SCHEDULE_FIFO = 0, 1
+SCHEDULE_ROUND_ROBIN, SCHEDULE_FIFO, SCHEDULE_SHORTEST_FIRST = 0, 1, 2
 
 
 class EngineConfig(ctypes.Structure):
@@ -163,14 +165,18 @@ class RenderEngine:
     # -- jobs ----------------------------------------------------------------------
     @staticmethod
     def _desc(scene, width, height, samples, maximum_bounce=20, minimum_bounce_russian_roulette=5, seed=0x5EED1234,
-              kind=JOB_PATH_TRACING):
+              kind=JOB_PATH_TRACING, ambient_occlusion_samples=10, maximum_distance=20.0):
         return JobDesc(int(scene), int(width), int(height), int(samples), int(maximum_bounce), int(minimum_bounce_russian_roulette),
-                       int(seed) & 0xFFFFFFFF, int(kind))
+                       int(seed) & 0xFFFFFFFF, int(kind), int(ambient_occlusion_samples), float(maximum_distance))
 
     def submit(self, scene: int, width: int, height: int, samples: int, maximum_bounce: int = 20,
-               minimum_bounce_russian_roulette: int = 5, seed: int = 0x5EED1234, kind: int = JOB_PATH_TRACING) -> int:
-        """Queues a job (PATH_TRACING, or RAY_CASTING / DEPTH_CAMERA with ``kind``); returns its id."""
-        d = self._desc(scene, width, height, samples, maximum_bounce, minimum_bounce_russian_roulette, seed, kind)
+               minimum_bounce_russian_roulette: int = 5, seed: int = 0x5EED1234, kind: int = JOB_PATH_TRACING,
+               ambient_occlusion_samples: int = 10, maximum_distance: float = 20.0) -> int:
+        """Queues a job of any rendering algorithm (``kind``: JOB_PATH_TRACING, JOB_RAY_CASTING,
+        JOB_DEPTH_CAMERA, JOB_AMBIENT_OCCLUSION with its samples and maximum distance, or
+        JOB_RAY_TRACING); returns its id.  ``samples`` is the render(samples) pass count."""
+        d = self._desc(scene, width, height, samples, maximum_bounce, minimum_bounce_russian_roulette, seed, kind,
+                       ambient_occlusion_samples, maximum_distance)
         jid = ctypes.c_int64(0)
         self._check(self._lib.dfc_job_submit(self._h, ctypes.byref(d), ctypes.byref(jid)))
         self._jobs[int(jid.value)] = (int(width), int(height))

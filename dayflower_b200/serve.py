@@ -3,11 +3,11 @@ jobs as they arrive while earlier ones are on the GPU, and the latency
 statistics of such a run.
 
 The engine admits each arrival into the running wavefront at the next bounce
-iteration (round-robin over admitted jobs by default), so a job's latency to
-its target spp is its queueing plus its share of the device.  For comparison,
-:func:`fifo_latencies` gives the latencies a single per-job renderer (one job
-on the GPU at a time, in arrival order) would have on the same arrivals, from
-measured per-job render times.
+iteration (round-robin or shortest-first over admitted jobs), so a job's
+latency to its target spp is its queueing plus its share of the device.  For
+comparison, :func:`run_per_job_served` serves the same arrivals live with one
+per-job renderer (one job on the GPU at a time, in arrival order), and
+:func:`fifo_latencies` computes that from measured per-job render times.
 """
 from __future__ import annotations
 
@@ -60,6 +60,38 @@ def run_served(engine, jobs: Sequence[dict], arrivals: Sequence[float], timeout_
     paths = float(sum(x["paths_total"] for x in infos))
     states = {x["state"] for x in infos}
     return {"latency_s": lat, "paths": paths, "wall_s": wall, "paths_per_s": paths / wall, "states": sorted(states)}
+
+
+def run_per_job_served(render_one, jobs: Sequence[dict], arrivals: Sequence[float]) -> np.ndarray:
+    """The per-job comparison, run live: a client thread delivers jobs[i] at
+    arrivals[i] into a queue, and one server (this thread, one GPURenderer
+    job at a time, as ``render_one(job)`` renders it to its RGBA8 image)
+    takes them in arrival order.  Returns each job's latency (arrival to its
+    image on the host), in seconds."""
+    import queue
+    q: "queue.Queue" = queue.Queue()
+    lat = np.zeros(len(jobs))
+    t0 = time.perf_counter()
+
+    def client():
+        for i, at in enumerate(arrivals):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            q.put((i, time.perf_counter()))
+        q.put(None)
+
+    th = threading.Thread(target=client)
+    th.start()
+    while True:
+        item = q.get()
+        if item is None:
+            break
+        i, t_arrival = item
+        render_one(jobs[i])
+        lat[i] = time.perf_counter() - t_arrival
+    th.join()
+    return lat
 
 
 def fifo_latencies(service_s: Sequence[float], arrivals: Sequence[float]) -> np.ndarray:

@@ -311,17 +311,24 @@ typedef struct dfc_job_desc {
   int32_t maximum_bounce;                   /* setMaximumBounce */
   int32_t minimum_bounce_russian_roulette;  /* setMinimumBounceRussianRoulette */
   uint32_t seed;                            /* seed of the counter-based random numbers (dfc_set_seed) */
-  int32_t kind;                             /* DFC_JOB_PATH_TRACING (0), DFC_JOB_RAY_CASTING or DFC_JOB_DEPTH_CAMERA */
+  int32_t kind;                             /* DFC_JOB_PATH_TRACING (0) or another DFC_JOB_* algorithm */
+  int32_t ambient_occlusion_samples;        /* AMBIENT_OCCLUSION: setSamples (rays per camera sample, 1 .. 4096) */
+  float maximum_distance;                   /* AMBIENT_OCCLUSION: setMaximumDistance (<= 0: occlusion only) */
 } dfc_job_desc;
 
-/* Rendering algorithm of an engine job (dfc_job_desc.kind): PATH_TRACING, or
- * the one-step RAY_CASTING and DEPTH_CAMERA of setRenderingAlgorithm
- * (renderer/gpu/AbstractGPURenderer.java:504), shaded as the per-job renderer
- * shades them.  AMBIENT_OCCLUSION and RAY_TRACING jobs run on a per-job
- * renderer (DFC_E_UNSUPPORTED here). */
+/* Rendering algorithm of an engine job (dfc_job_desc.kind), the
+ * RenderingAlgorithm of setRenderingAlgorithm (renderer/gpu/
+ * AbstractGPURenderer.java:504) that GPURenderer.run dispatches on
+ * (renderer/gpu/GPURenderer.java:65-77), each shaded as the per-job renderer
+ * shades it: PATH_TRACING in the bounce wavefront; RAY_CASTING and
+ * DEPTH_CAMERA end at their camera ray; AMBIENT_OCCLUSION and RAY_TRACING
+ * trace their camera ray in the wavefront and then their occlusion rays or
+ * their ray tree in one step on the path's thread. */
 #define DFC_JOB_PATH_TRACING 0
 #define DFC_JOB_RAY_CASTING 1
 #define DFC_JOB_DEPTH_CAMERA 2
+#define DFC_JOB_AMBIENT_OCCLUSION 3
+#define DFC_JOB_RAY_TRACING 4
 
 typedef struct dfc_job_info {
   int32_t state;                 /* DFC_JOB_* */
@@ -335,8 +342,11 @@ typedef struct dfc_job_info {
  * consecutive paths of one job, at most `lookahead_paths` ahead of the paths
  * started so far.  ROUND_ROBIN gives every admitted job one segment in turn
  * (processor sharing: small jobs finish early while large ones run); FIFO
- * finishes jobs in admission order. */
-enum { DFC_SCHEDULE_ROUND_ROBIN = 0, DFC_SCHEDULE_FIFO = 1 };
+ * finishes jobs in admission order; SHORTEST_FIRST gives the next segment to
+ * the admitted job with the fewest paths left to hand out (small jobs stay
+ * fast under overload, large ones wait; a small lookahead_paths lets new
+ * arrivals overtake sooner). */
+enum { DFC_SCHEDULE_ROUND_ROBIN = 0, DFC_SCHEDULE_FIFO = 1, DFC_SCHEDULE_SHORTEST_FIRST = 2 };
 
 typedef struct dfc_engine_config {
   int64_t capacity;              /* path slots of the wavefront (0: default 2^20) */

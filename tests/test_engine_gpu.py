@@ -76,17 +76,18 @@ def test_engine_job_matches_per_job_renderer(engine, scenes, name):
 
 
 @pytest.mark.parametrize("name", ["cornell", "mixed", "quadrics"])
-@pytest.mark.parametrize("kind,algorithm", [(1, RA.RAY_CASTING), (2, RA.DEPTH_CAMERA)])
+@pytest.mark.parametrize("kind,algorithm", [(1, RA.RAY_CASTING), (2, RA.DEPTH_CAMERA), (3, RA.AMBIENT_OCCLUSION), (4, RA.RAY_TRACING)])
 def test_engine_one_step_jobs_match_per_job_renderer(engine, scenes, name, kind, algorithm):
-    # RAY_CASTING and DEPTH_CAMERA jobs end at their camera ray; each sample is the per-job renderer's
-    from dayflower_b200.engine import JOB_DEPTH_CAMERA, JOB_RAY_CASTING
-    assert (JOB_RAY_CASTING, JOB_DEPTH_CAMERA) == (1, 2)
+    # RAY_CASTING and DEPTH_CAMERA jobs end at their camera ray; AMBIENT_OCCLUSION and RAY_TRACING trace their
+    # occlusion rays or ray tree in one step; each sample is the per-job renderer's (GPURenderer.java:65-77)
+    from dayflower_b200.engine import JOB_AMBIENT_OCCLUSION, JOB_DEPTH_CAMERA, JOB_RAY_CASTING, JOB_RAY_TRACING
+    assert (JOB_RAY_CASTING, JOB_DEPTH_CAMERA, JOB_AMBIENT_OCCLUSION, JOB_RAY_TRACING) == (1, 2, 3, 4)
     e, ids = engine
     cs = scenes[name]
     w, h = res_of(cs)
-    g = PT.render_gpu(cs, algorithm, spp=3, seed=91)
+    g = PT.render_gpu(cs, algorithm, spp=3, seed=91, max_bounce=8, ao_samples=12, ao_distance=30.0)
     others = [e.submit(ids["terrain"], 32, 24, 2, maximum_bounce=4, seed=5)]  # shares the wavefront with a path-traced job
-    j = e.submit(ids[name], w, h, 3, seed=91, kind=kind)
+    j = e.submit(ids[name], w, h, 3, seed=91, kind=kind, maximum_bounce=8, ambient_occlusion_samples=12, maximum_distance=30.0)
     e.run(timeout_s=120)
     assert e.info(j)["state"] == "done"
     f = e.film(j)
@@ -219,6 +220,7 @@ def test_engine_rejects_bad_jobs(engine):
         e.submit(ids["cornell"], 0, 8, 1)
     with pytest.raises(ValueError):
         e.submit(ids["cornell"], 8, 8, 0)
-    from dayflower_b200.renderer import UnsupportedSceneError
-    with pytest.raises(UnsupportedSceneError):
-        e.submit(ids["cornell"], 8, 8, 1, kind=3)  # AMBIENT_OCCLUSION / RAY_TRACING run on a per-job renderer
+    with pytest.raises(ValueError):
+        e.submit(ids["cornell"], 8, 8, 1, kind=5)  # no such rendering algorithm
+    with pytest.raises(ValueError):
+        e.submit(ids["cornell"], 8, 8, 1, kind=3, ambient_occlusion_samples=0)  # setSamples out of range

@@ -126,13 +126,17 @@ def test_path_tracing_rmse_against_converged(scene_name, request):
     # the root of the mean squared error over four 16-spp renders with
     # different seeds (an estimate of the expected error, not of one draw).
     #
-    # The oracle here runs without the reference's object-space drift: the
-    # reference carries each ray through every primitive's space in list
-    # order, which moves a secondary ray's origin by a few ulps and so decides
-    # whether a ray leaving a curved surface hits that surface again at
-    # t ~ 1e-6 (the near root wins when its lower bound is above 0,
-    # Sphere3F.java intersectionT).  A hierarchy cannot follow that order; per
-    # sample the device matches the drift-free oracle (as the depth check does).
+    # The oracle is the faithful one.  The reference carries each ray through
+    # every primitive's space in list order, which moves a secondary ray's
+    # origin by a few ulps and so decides whether a ray leaving a curved
+    # surface hits that surface again at t ~ 1e-6 (the near root wins when its
+    # lower bound is above 0, Sphere3F.java intersectionT).  A hierarchy cannot
+    # follow that order per sample (per sample the device matches the
+    # drift-free oracle, as the depth check shows), but in the aggregate the
+    # device's image statistics are the faithful oracle's: measured device /
+    # faithful RMSE 0.998-1.000 on these scenes, against 0.987-1.000 for the
+    # drift-free oracle, whose glass and mirror spheres never re-hit
+    # themselves.
     #
     # The Disney and materials scenes are not cases: their 16-spp error is
     # dominated by rare caustic paths (thin, glass and translucent spheres
@@ -147,7 +151,7 @@ def test_path_tracing_rmse_against_converged(scene_name, request):
     for s in range(4):
         seed = 0x5EED1234 + 7919 * s
         g = PT.render_gpu(cs, RA.PATH_TRACING, spp=16, max_bounce=8, seed=seed)
-        o = PT.render_oracle_no_drift(cs, RA.PATH_TRACING, spp=16, max_bounce=8, seed=seed)
+        o = PT.render_oracle(cs, RA.PATH_TRACING, spp=16, max_bounce=8, seed=seed)
         mse_g.append(np.mean((g["sum"] / np.maximum(g["count"], 1)[..., None] - ref) ** 2))
         mse_o.append(np.mean((o["sum"] / np.maximum(o["count"], 1)[..., None] - ref) ** 2))
     rmse_g, rmse_o = float(np.sqrt(np.mean(mse_g))), float(np.sqrt(np.mean(mse_o)))

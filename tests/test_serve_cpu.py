@@ -46,3 +46,15 @@ def test_job_mix_scene_sizes():
     sc = G.job_mix_scene(2)
     kinds = {type(l).__name__ for l in sc.lights}
     assert kinds == {"PointLight", "SpotLight", "DiffuseAreaLight"}
+
+
+def test_live_per_job_server_matches_the_fifo_queue():
+    # the live comparison arm on a fake renderer: each job takes its service time, one at a time in arrival order
+    import time
+    service = [0.06, 0.01, 0.01, 0.05, 0.01]
+    arrivals = [0.0, 0.01, 0.02, 0.2, 0.21]
+    jobs = [{"service": s} for s in service]
+    lat = SV.run_per_job_served(lambda j: time.sleep(j["service"]), jobs, arrivals)
+    want = SV.fifo_latencies(service, arrivals)
+    assert np.all(lat >= want - 1e-3)
+    assert np.all(lat <= want + 0.03)
