@@ -298,23 +298,34 @@ def batched_and_served(args, device=0):
         arrivals = {lam: SV.poisson_arrivals(lam, min(len(jobs), max(16, int(4 * lam))), seed=lam) for lam in lams}
         subsets = {lam: [jobs[i % len(jobs)] for i in range(len(arrivals[lam]))] for lam in lams}
 
-        def pct(lat, sub, only64):
-            sel = np.array([(j["samples"] == 64 and j["width"] * j["height"] <= 1024 * 1024) for j in sub]) if only64 else None
-            x = lat[sel] if only64 else lat
-            return SV.percentiles(x) if len(x) else None
+        def pct(lat, sub, which):
+            """Latency percentiles of all jobs, the 64-spp jobs (all <= 1024^2) or the small ones (<= 256^2)."""
+            if which == "all":
+                x = lat
+            elif which == "spp64":
+                x = lat[np.array([j["samples"] == 64 and j["width"] * j["height"] <= 1024 * 1024 for j in sub])]
+            else:
+                x = lat[np.array([j["width"] * j["height"] <= 256 * 256 for j in sub])]
+            return SV.percentiles(x) if len(x) else {"p50_s": None, "p99_s": None}
 
-        for policy, lookahead in ((0, 0), (2, int(tuned["capacity"]))):
-            eng.configure(**dict(tuned, policy=policy, lookahead_paths=lookahead))
+        def row(lat, sub):
+            out = {}
+            for which in ("all", "spp64", "small"):
+                p = pct(lat, sub, which)
+                pre = "" if which == "all" else which + "_"
+                out[pre + "p50_s"], out[pre + "p99_s"] = p["p50_s"], p["p99_s"]
+            return out
+
+        for policy in (0, 2):
+            eng.configure(**dict(tuned, policy=policy))
             eng.start()
             for lam in lams:
                 sub, arr = subsets[lam], arrivals[lam]
                 r = SV.run_served(eng, sub, arr)
-                p_all, p64 = pct(r["latency_s"], sub, False), pct(r["latency_s"], sub, True)
-                served.append({"policy": "round_robin" if policy == 0 else "shortest_first", "lambda_per_s": lam, "jobs": len(sub),
-                               "p50_s": p_all["p50_s"], "p99_s": p_all["p99_s"],
-                               "spp64_jobs": int(sum(j["samples"] == 64 for j in sub)),
-                               "spp64_p50_s": p64["p50_s"] if p64 else None, "spp64_p99_s": p64["p99_s"] if p64 else None,
-                               "paths_per_s": r["paths_per_s"], "states": r["states"]})
+                served.append(dict({"policy": "round_robin" if policy == 0 else "shortest_first", "lambda_per_s": lam, "jobs": len(sub),
+                                    "spp64_jobs": int(sum(j["samples"] == 64 for j in sub)),
+                                    "small_jobs": int(sum(j["width"] * j["height"] <= 256 * 256 for j in sub)),
+                                    "paths_per_s": r["paths_per_s"], "states": r["states"]}, **row(r["latency_s"], sub)))
             eng.stop()
     finally:
         eng.close()
@@ -343,14 +354,13 @@ def batched_and_served(args, device=0):
         for lam in lams:
             sub, arr = subsets[lam], arrivals[lam]
             lat = SV.run_per_job_served(render_one, sub, arr)
-            p_all, p64 = pct(lat, sub, False), pct(lat, sub, True)
-            live.append({"lambda_per_s": lam, "jobs": len(sub), "p50_s": p_all["p50_s"], "p99_s": p_all["p99_s"],
-                         "spp64_p50_s": p64["p50_s"] if p64 else None, "spp64_p99_s": p64["p99_s"] if p64 else None})
+            live.append(dict({"lambda_per_s": lam, "jobs": len(sub)}, **row(lat, sub)))
         for h in handles:
             h.dispose()
-    return batched, {"latency": "submit -> done at the job's spp (engine clock); spp64: the 64-spp jobs (all <= 1024^2)",
-                     "round_robin": "every admitted job one 64K-path segment in turn, lookahead 8 x capacity",
-                     "shortest_first": "the next segment to the admitted job with the fewest paths left, lookahead 1 x capacity",
+    return batched, {"latency": "submit -> done at the job's spp (engine clock); spp64: the 64-spp jobs (all <= 1024^2); "
+                                "small: jobs of <= 256^2 pixels",
+                     "round_robin": "every admitted job one 64K-path segment in turn",
+                     "shortest_first": "the next segment to the admitted job with the fewest paths left",
                      "sweep": served,
                      "plain_per_job_live": {"how": "one GPURenderer serving the same arrivals one job at a time in arrival order, "
                                                    "latency arrival -> RGBA8 image on the host", "sweep": live}}

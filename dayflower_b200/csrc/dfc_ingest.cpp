@@ -694,6 +694,36 @@ struct Decoder {
       }
       hs.prims.push_back(pr);
     }
+    // Items whose box covers a large part of the scene (a terrain under
+    // everything else, the walls of a room) can be tested before the top
+    // level rather than inside it: their hit usually comes first along a ray
+    // and then culls most of the top level.  At most DFC_FIRST_ITEMS of them,
+    // each at least a fifth of the scene box's surface area, largest first.
+#ifndef DFC_FIRST_ITEMS
+#define DFC_FIRST_ITEMS 0
+#endif
+    constexpr size_t kFirstItems = DFC_FIRST_ITEMS;
+    constexpr float kFirstArea = 0.2f;
+    if (kFirstItems > 0 && tlas_boxes.size() > 1) {
+      Box scene_box;
+      for (const Box& b : tlas_boxes) scene_box.grow(b);
+      std::vector<size_t> big;
+      for (size_t k = 0; k < tlas_boxes.size(); ++k)
+        if (tlas_boxes[k].area() >= kFirstArea * scene_box.area()) big.push_back(k);
+      std::stable_sort(big.begin(), big.end(), [&](size_t a, size_t b) { return tlas_boxes[a].area() > tlas_boxes[b].area(); });
+      if (big.size() > kFirstItems) big.resize(kFirstItems);
+      if (big.size() < tlas_boxes.size()) {
+        std::vector<char> out(tlas_boxes.size(), 0);
+        for (size_t k : big) { hs.unbounded.push_back(tlas_prims[k]); out[k] = 1; }
+        size_t w = 0;
+        for (size_t k = 0; k < tlas_boxes.size(); ++k) {
+          if (out[k]) continue;
+          tlas_boxes[w] = tlas_boxes[k]; tlas_prims[w] = tlas_prims[k]; tlas_spheres[w] = tlas_spheres[k];
+          ++w;
+        }
+        tlas_boxes.resize(w); tlas_prims.resize(w); tlas_spheres.resize(w);
+      }
+    }
     if (!tlas_boxes.empty()) {
       const auto t_tlas = std::chrono::steady_clock::now();
       std::vector<int> order;

@@ -124,9 +124,16 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
   // (every bounding-volume and shape test compares false against NaN); here a
   // NaN would pass every slab test (fmaxf drops NaN), so stop it up front.
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) { out->t = tmax; return false; }
+  int sp = 0;
+  if (S.tlas_root >= 0) stack[(sp++) * kTraceBlock] = S.tlas_root;
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
+    if (pr.shape == kShapeMesh) {  // entered before the top level (pushed last, popped first)
+      if (sp < kStack) stack[(sp++) * kTraceBlock] = -2 - pi;
+      else atomicAdd(overflow, 1u);
+      continue;
+    }
     ObjRay r = obj_ray(pr, o, d);
     float to = prim_t<kRecords>(S, pr, r, best * r.s);
     if (to > kTMin) {  // SurfaceIntersector3F.intersection: t > tMinimum
@@ -137,10 +144,8 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
       }
     }
   }
-  if (S.tlas_root < 0) { out->t = best; return found; }
+  if (sp == 0) { out->t = best; return found; }
   const V3 winv = safe_inv(d);
-  int sp = 0;
-  stack[(sp++) * kTraceBlock] = S.tlas_root;
   bool in_blas = false;
   ObjRay br;
   br.s = 1.0f;
@@ -238,6 +243,13 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
 constexpr unsigned kAlive = kFlagAlive, kPendShadow = kFlagPendShadow, kPendMis = kFlagPendMis, kShadowAny = kFlagShadowAny,
                    kNoSample = kFlagNoSample;
 
+// Stack entries (32 bits):
+//   0x00000000 | node                 an interior node
+//   0x80000000 | first << 2 | (n - 1) a leaf of n items starting at `first`
+//   0xC0000000 | prim                 enter the bottom level of mesh primitive `prim`
+//   0xFFFFFFFF                        end of a bottom level (back to world space)
+constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0xC0000000u, kEndBlas = 0xFFFFFFFFu;
+
 // ---- persistent traversal with per-lane refill ---------------------------
 // The same walk as trace_ray, held in registers across iterations so that a
 // lane whose ray is done takes a new ray from the queue instead of idling
@@ -262,35 +274,34 @@ struct Trav {
 };
 
 template <bool kRecords>
-DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack) {
+DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack, unsigned* overflow) {
   T.o = o; T.d = d; T.co = o; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
   T.any = any; T.in_blas = false;
   T.sp = 0; T.bprim = -1;
   T.prim = -1; T.aux = -1; T.t_obj = 0.0f;
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
+  T.cinv = safe_inv(d);
+  if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
     const DPrim& pr = S.prims[pi];
+    if (pr.shape == kShapeMesh) {  // entered before the top level (pushed last, popped first)
+      if (T.sp < kStack) stack[(T.sp++) * kTraceBlock] = (int)(kTagMesh | (unsigned)pi);
+      else atomicAdd(overflow, 1u);
+      continue;
+    }
     ObjRay r = obj_ray(pr, o, d);
     const float to = prim_t<kRecords>(S, pr, r, T.cbest * r.s);
     if (to > kTMin) {
       const float tw = to / r.s;
       if (tw < T.cbest) {
         T.cbest = tw; T.prim = pi; T.aux = pr.data; T.t_obj = to;
-        if (any) return;
+        if (any) { T.sp = 0; return; }
       }
     }
   }
-  T.cinv = safe_inv(d);
-  if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
 }
 
-// Stack entries (32 bits):
-//   0x00000000 | node                 an interior node
-//   0x80000000 | first << 2 | (n - 1) a leaf of n items starting at `first`
-//   0xC0000000 | prim                 enter the bottom level of mesh primitive `prim`
-//   0xFFFFFFFF                        end of a bottom level (back to world space)
-constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0xC0000000u, kEndBlas = 0xFFFFFFFFu;
 
 #define DFC_CSWAP(ta, ea, tb, eb) \
   if (tb < ta) { const float tt_ = ta; ta = tb; tb = tt_; const unsigned ee_ = ea; ea = eb; eb = ee_; }
@@ -453,7 +464,7 @@ __device__ __forceinline__ void trace_rays(const TraceArgs& a) {
           slot = type * a.paths + p;
           if constexpr (kMulti) si = a.jobs[a.slot_job[p]].scene;
           const float4 ro = a.ray_o[slot], rd = a.ray_d[slot];
-          trav_init<kRecords>(scene_at<kMulti>(a, si), T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack);
+          trav_init<kRecords>(scene_at<kMulti>(a, si), T, V3{ro.x, ro.y, ro.z}, V3{rd.x, rd.y, rd.z}, rd.w, (ref & 4u) != 0u, stack, a.overflow);
           lf_cnt = 0;
         }
       }
