@@ -239,7 +239,30 @@ __global__ void k_blas_tri_pos(const float* tri_attr, const int* tri_index, cons
 template <typename T>
 cudaError_t alloc(T** p, size_t n, cudaStream_t s) { return cudaMallocAsync(reinterpret_cast<void**>(p), (n ? n : 1) * sizeof(T), s); }
 
+// Rewrites each node's child words as the traversal's stack entries, so that
+// a node visit loads one 16-byte word of children and pushes it as it is:
+// an interior child keeps its index (tag bits 00), a leaf becomes
+// 0x80000000 | first << 2 | (count - 1).  count[] is left as built.
+__global__ void k_encode_entries(BVH4Node* nodes, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int4* cp = reinterpret_cast<int4*>(nodes + i) + 6;
+  int4 c = cp[0];
+  const int4 k = cp[1];
+  auto enc = [](int child, int count) -> int {
+    if (child >= 0 || count <= 0) return child >= 0 ? child : 0;  // interior, or an empty slot (never hit)
+    return (int)(0x80000000u | ((unsigned)(~child) << 2) | (unsigned)(count - 1));
+  };
+  cp[0] = make_int4(enc(c.x, k.x), enc(c.y, k.y), enc(c.z, k.z), enc(c.w, k.w));
+}
+
 }  // namespace
+
+cudaError_t encode_node_entries(BVH4Node* nodes, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_encode_entries<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(nodes, n);
+  return cudaGetLastError();
+}
 
 int build_blas_device(const float* tri_attr, const int* tri_index, int n, BVH4Node* nodes_out, int node_base, int node_cap, F4* tri_pos,
                       int tri_first, cudaStream_t s, cudaError_t* err) {

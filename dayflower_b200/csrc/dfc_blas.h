@@ -18,6 +18,13 @@ namespace dfc {
 int build_blas_device(const float* tri_attr, const int* tri_index, int count, BVH4Node* nodes, int node_base, int node_cap,
                       F4* tri_pos, int tri_first, cudaStream_t stream, cudaError_t* err);
 
+// Rewrites the child words of `n` device nodes as traversal stack entries (an
+// interior child's index; 0x80000000 | first << 2 | (count - 1) for a leaf of
+// `count` items from `first`), once every level of the scene is in place.
+// Leaf ranges must start below 2^28.
+cudaError_t encode_node_entries(BVH4Node* nodes, size_t n, cudaStream_t stream);
+constexpr long long kMaxLeafFirst = 1ll << 28;
+
 // Nodes a mesh of `count` triangles may need (an upper bound).
 inline int blas_node_capacity(int count) { return count > 1 ? count : 1; }
 

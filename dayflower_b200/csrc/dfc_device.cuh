@@ -1059,8 +1059,21 @@ DFC_D float d2_pdf(const float* a, float su, float sv) {
   return a[offC + 4 + iC + (int)a[offC + 1]] / a[offM + 3];
 }
 
+// The sky models and the light sampling and pdf routines below are large
+// (perez_sky alone evaluates 15 exponentials) and are reached from several
+// places of a shading kernel; compiled out of line they are held once in the
+// instruction cache instead of once per call site.
+#ifndef DFC_LIGHT_NOINLINE
+#define DFC_LIGHT_NOINLINE 1
+#endif
+#if DFC_LIGHT_NOINLINE
+#define DFC_LIGHT_FN static __device__ __noinline__
+#else
+#define DFC_LIGHT_FN DFC_D
+#endif
+
 // scene/light/PerezLight.java doRadianceSky (renderer/gpu/AbstractLightKernel.java:1615 form).
-DFC_D V3 perez_sky(const float* q, V3 dir) {
+DFC_LIGHT_FN V3 perez_sky(const float* q, V3 dir) {
   if (dir.z < 0.0f) return {0, 0, 0};
   V3 ds = normalize(V3{dir.x, dir.y, fmaxf(dir.z, 0.001f)});
   const float T = q[41];
@@ -1091,7 +1104,7 @@ DFC_D V3 sat0(V3 c) { return {fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0
 // distribution +40, RGB image +2352): spherical texture coordinates, rotated
 // counterclockwise, scaled, mapped to pixels (Point2F.toImage) and read with
 // bilinear interpolation and wrap-around (ImageF.getColorRGB).
-DFC_D V3 image_sky(const float* q, V3 d) {
+DFC_LIGHT_FN V3 image_sky(const float* q, V3 d) {
   float phi = atan2f(d.y, d.x);
   if (phi < 0.0f) phi += 2.0f * kPi;
   const float theta = acosf(clampf(d.z, -1.0f, 1.0f));
@@ -1118,60 +1131,108 @@ DFC_D V3 image_sky(const float* q, V3 d) {
 
 struct LightS { V3 L, p, wi; float pdf; };
 
+// DiffuseAreaLight.sampleRadianceIncoming for a triangle or sphere shape.
+DFC_LIGHT_FN bool area_light_sample(const float* tri_attr, const DLight& lt, V3 p, float u, float v, LightS* o) {
+  V3 ref = xf_point(lt.w2o, p);
+  V3 sp, sn;
+  float pdf;
+  if (lt.shape == kShapeTriangle) {
+    // Triangle3F.sample(Point2F) + Shape3F.sample(sample, ref): the solid-angle
+    // pdf there is dist^2/|cos| (the area density of the point is not applied).
+    const float* q = tri_attr + (size_t)lt.shape_data * 24;
+    float su = sqrtf(u), b0 = 1.0f - su, b1 = v * su, b2 = 1.0f - b0 - b1;
+    V3 A = ld3(q), B = ld3(q + 3), C = ld3(q + 6);
+    sp = {A.x * b0 + B.x * b1 + C.x * b2, A.y * b0 + B.y * b1 + C.y * b2, A.z * b0 + B.z * b1 + C.z * b2};
+    sn = normalize(ld3(q + 15) * b0 + ld3(q + 18) * b1 + ld3(q + 21) * b2);
+    V3 inc = sp - ref;
+    if (dot(inc, inc) == 0.0f) return false;
+    V3 incn = normalize(inc);
+    pdf = dot(inc, inc) / fabsf(dot(sn, -incn));
+    if (isinf(pdf) || isnan(pdf)) return false;
+  } else if (lt.shape == kShapeSphere) {
+    if (dot(ref, ref) <= 1.0f) {
+      float ct = 1.0f - 2.0f * u, st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), s, c;
+      sincosf(v * 2.0f * kPi, &s, &c);
+      sp = {st * c, st * s, ct};
+      sn = normalize(sp);
+      V3 inc = sp - ref;
+      if (dot(inc, inc) == 0.0f) return false;
+      pdf = dot(inc, inc) / fabsf(dot(sn, -normalize(inc)));
+      if (isinf(pdf) || isnan(pdf)) return false;
+    } else {
+      float dist = len(ref), dr = 1.0f / dist;
+      V3 dc = (-ref) * dr;
+      ONB b = onb_w(dc);
+      float stm2 = dr * dr, stmr = dist;
+      float ctm = sqrtf(fmaxf(0.0f, 1.0f - stm2));
+      float ct = stm2 < 0.00068523f ? sqrtf(1.0f - stm2 * u) : (ctm - 1.0f) * u + 1.0f;
+      float st2 = stm2 < 0.00068523f ? stm2 * u : 1.0f - ct * ct;
+      float ca = st2 * stmr + ct * sqrtf(fmaxf(0.0f, 1.0f - st2 * stmr * stmr));
+      float sa = sqrtf(fmaxf(0.0f, 1.0f - ca * ca)), s, c;
+      sincosf(v * 2.0f * kPi, &s, &c);
+      V3 sd = (-b.u) * (sa * c) + (-b.v) * (sa * s) + (-b.w) * ca;
+      sp = sd; sn = normalize(sd); pdf = 1.0f / (2.0f * kPi * (1.0f - ctm));
+    }
+  } else {
+    return false;  // Shape3F.sample default: no sample for other shapes
+  }
+  V3 pw = xf_point(lt.o2w, sp);
+  V3 nw = normalize(xf_vec_t(lt.w2o, sn));
+  V3 wi = normalize(pw - p);
+  if (pdf > 0.0f && (lt.two_sided || dot(nw, -wi) > 0.0f)) { *o = LightS{ld3(lt.radiance), pw, wi, pdf}; return true; }
+  return false;
+}
+
+// PerezLight and ImageLight (scene/light/ImageLight.java:207) sampleRadianceIncoming;
+// q is the light's record in the sky pool, gw and sw the surface's geometric and
+// shading normals.
+DFC_LIGHT_FN bool sky_light_sample(const float* q, int type, V3 p, V3 gw, V3 sw, float u, float v, float sun_pick, LightS* o) {
+  if (type == kLightPerez) {
+    const float* dist = q + 48;
+    V3 sunW = ld3(q + 38), sunO = ld3(q + 35);
+    if (dot(sunW, gw) > sun_pick && dot(sunW, sw) > sun_pick) {
+      float st = sint(sunO);
+      if (st != 0.0f) {
+        float phi = atan2f(sunO.y, sunO.x);
+        if (phi < 0.0f) phi += 2.0f * kPi;
+        float pdf = d2_pdf(dist, phi * (1.0f / (2.0f * kPi)), acosf(clampf(sunO.z, -1.0f, 1.0f)) * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
+        if (pdf != 0.0f) { *o = LightS{ld3(q + 32), p + sunW * (2.0f * q[45]), sunW, pdf}; return true; }
+      }
+    }
+    float ru, rv;
+    d2_remap(dist, u, v, &ru, &rv);
+    float pr = d2_pdf(dist, ru, rv);
+    if (pr == 0.0f) return false;
+    float sth, cth, sph, cph;
+    sincosf(rv * kPi, &sth, &cth);
+    sincosf(ru * 2.0f * kPi, &sph, &cph);
+    V3 dobj = {sth * cph, sth * sph, cth};
+    V3 dw = normalize(xf_vec(q, dobj));
+    float st = sint(dobj);
+    if (st == 0.0f) return false;
+    *o = LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
+    return true;
+  }
+  float ru, rv;
+  d2_remap(q + 40, u, v, &ru, &rv);
+  const float pr = d2_pdf(q + 40, ru, rv);
+  if (pr == 0.0f) return false;
+  float sth, cth, sph, cph;
+  sincosf(rv * kPi, &sth, &cth);
+  sincosf(ru * 2.0f * kPi, &sph, &cph);
+  const V3 dobj = {sth * cph, sth * sph, cth};
+  const V3 dw = normalize(xf_vec(q, dobj));
+  const float st = sint(dobj);
+  if (st == 0.0f) return false;
+  *o = LightS{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
+  return true;
+}
+
 // Light.sampleRadianceIncoming for each supported light type.
 DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf, float u, float v, float sun_pick, LightS* o) {
   const V3 p = sf.p;
   switch (lt.type) {
-    case kLightDiffuseArea: {
-      V3 ref = xf_point(lt.w2o, p);
-      V3 sp, sn;
-      float pdf;
-      if (lt.shape == kShapeTriangle) {
-        // Triangle3F.sample(Point2F) + Shape3F.sample(sample, ref): the solid-angle
-        // pdf there is dist^2/|cos| (the area density of the point is not applied).
-        const float* q = S.tri_attr + (size_t)lt.shape_data * 24;
-        float su = sqrtf(u), b0 = 1.0f - su, b1 = v * su, b2 = 1.0f - b0 - b1;
-        V3 A = ld3(q), B = ld3(q + 3), C = ld3(q + 6);
-        sp = {A.x * b0 + B.x * b1 + C.x * b2, A.y * b0 + B.y * b1 + C.y * b2, A.z * b0 + B.z * b1 + C.z * b2};
-        sn = normalize(ld3(q + 15) * b0 + ld3(q + 18) * b1 + ld3(q + 21) * b2);
-        V3 inc = sp - ref;
-        if (dot(inc, inc) == 0.0f) return false;
-        V3 incn = normalize(inc);
-        pdf = dot(inc, inc) / fabsf(dot(sn, -incn));
-        if (isinf(pdf) || isnan(pdf)) return false;
-      } else if (lt.shape == kShapeSphere) {
-        if (dot(ref, ref) <= 1.0f) {
-          float ct = 1.0f - 2.0f * u, st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), s, c;
-          sincosf(v * 2.0f * kPi, &s, &c);
-          sp = {st * c, st * s, ct};
-          sn = normalize(sp);
-          V3 inc = sp - ref;
-          if (dot(inc, inc) == 0.0f) return false;
-          pdf = dot(inc, inc) / fabsf(dot(sn, -normalize(inc)));
-          if (isinf(pdf) || isnan(pdf)) return false;
-        } else {
-          float dist = len(ref), dr = 1.0f / dist;
-          V3 dc = (-ref) * dr;
-          ONB b = onb_w(dc);
-          float stm2 = dr * dr, stmr = dist;
-          float ctm = sqrtf(fmaxf(0.0f, 1.0f - stm2));
-          float ct = stm2 < 0.00068523f ? sqrtf(1.0f - stm2 * u) : (ctm - 1.0f) * u + 1.0f;
-          float st2 = stm2 < 0.00068523f ? stm2 * u : 1.0f - ct * ct;
-          float ca = st2 * stmr + ct * sqrtf(fmaxf(0.0f, 1.0f - st2 * stmr * stmr));
-          float sa = sqrtf(fmaxf(0.0f, 1.0f - ca * ca)), s, c;
-          sincosf(v * 2.0f * kPi, &s, &c);
-          V3 sd = (-b.u) * (sa * c) + (-b.v) * (sa * s) + (-b.w) * ca;
-          sp = sd; sn = normalize(sd); pdf = 1.0f / (2.0f * kPi * (1.0f - ctm));
-        }
-      } else {
-        return false;  // Shape3F.sample default: no sample for other shapes
-      }
-      V3 pw = xf_point(lt.o2w, sp);
-      V3 nw = normalize(xf_vec_t(lt.w2o, sn));
-      V3 wi = normalize(pw - p);
-      if (pdf > 0.0f && (lt.two_sided || dot(nw, -wi) > 0.0f)) { *o = LightS{ld3(lt.radiance), pw, wi, pdf}; return true; }
-      return false;
-    }
+    case kLightDiffuseArea: return area_light_sample(S.tri_attr, lt, p, u, v, o);
     case kLightPoint: {
       V3 pos = ld3(lt.pos);
       V3 d = pos - p;
@@ -1195,49 +1256,8 @@ DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf,
       *o = LightS{ld3(lt.radiance), p + d * (2.0f * lt.radius), d, 1.0f};
       return true;
     }
-    case kLightPerez: {
-      const float* q = S.perez + lt.perez;
-      const float* dist = q + 48;
-      V3 sunW = ld3(q + 38), sunO = ld3(q + 35);
-      if (dot(sunW, sf.g.w) > sun_pick && dot(sunW, sf.s.w) > sun_pick) {
-        float st = sint(sunO);
-        if (st != 0.0f) {
-          float phi = atan2f(sunO.y, sunO.x);
-          if (phi < 0.0f) phi += 2.0f * kPi;
-          float pdf = d2_pdf(dist, phi * (1.0f / (2.0f * kPi)), acosf(clampf(sunO.z, -1.0f, 1.0f)) * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
-          if (pdf != 0.0f) { *o = LightS{ld3(q + 32), p + sunW * (2.0f * q[45]), sunW, pdf}; return true; }
-        }
-      }
-      float ru, rv;
-      d2_remap(dist, u, v, &ru, &rv);
-      float pr = d2_pdf(dist, ru, rv);
-      if (pr == 0.0f) return false;
-      float sth, cth, sph, cph;
-      sincosf(rv * kPi, &sth, &cth);
-      sincosf(ru * 2.0f * kPi, &sph, &cph);
-      V3 dobj = {sth * cph, sth * sph, cth};
-      V3 dw = normalize(xf_vec(q, dobj));
-      float st = sint(dobj);
-      if (st == 0.0f) return false;
-      *o = LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
-      return true;
-    }
-    case kLightImage: {  // scene/light/ImageLight.java:207 sampleRadianceIncoming
-      const float* q = S.perez + lt.perez;
-      float ru, rv;
-      d2_remap(q + 40, u, v, &ru, &rv);
-      const float pr = d2_pdf(q + 40, ru, rv);
-      if (pr == 0.0f) return false;
-      float sth, cth, sph, cph;
-      sincosf(rv * kPi, &sth, &cth);
-      sincosf(ru * 2.0f * kPi, &sph, &cph);
-      const V3 dobj = {sth * cph, sth * sph, cth};
-      const V3 dw = normalize(xf_vec(q, dobj));
-      const float st = sint(dobj);
-      if (st == 0.0f) return false;
-      *o = LightS{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
-      return true;
-    }
+    case kLightPerez:
+    case kLightImage: return sky_light_sample(S.perez + lt.perez, lt.type, p, sf.g.w, sf.s.w, u, v, sun_pick, o);
   }
   return false;
 }
@@ -1254,15 +1274,15 @@ DFC_D V3 light_Le_miss(const SceneView& S, const DLight& lt, V3 d) {
 
 // Light.evaluateProbabilityDensityFunctionRadianceIncoming of the sky lights
 // (PerezLight, ImageLight.java:348); their distribution starts at +48 and +40.
-DFC_D float sky_pdf(const SceneView& S, const DLight& lt, V3 wi) {
-  const float* q = S.perez + lt.perez;
+DFC_LIGHT_FN float sky_pdf_q(const float* q, int type, V3 wi) {
   V3 d = normalize(xf_vec(q + 16, wi));
   float th = acosf(clampf(d.z, -1.0f, 1.0f));
   float st = sinf(th);
   if (st == 0.0f) return 0.0f;
   float phi = atan2f(d.y, d.x);
   if (phi < 0.0f) phi += 2.0f * kPi;
-  return d2_pdf(q + (lt.type == kLightPerez ? 48 : 40), phi * (1.0f / (2.0f * kPi)), th * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
+  return d2_pdf(q + (type == kLightPerez ? 48 : 40), phi * (1.0f / (2.0f * kPi)), th * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
 }
+DFC_D float sky_pdf(const SceneView& S, const DLight& lt, V3 wi) { return sky_pdf_q(S.perez + lt.perez, lt.type, wi); }
 
 }  // namespace dfc

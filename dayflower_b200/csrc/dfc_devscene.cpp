@@ -81,6 +81,11 @@ cudaError_t upload_scene(HostScene&& hs, cudaStream_t s, DeviceScene* ds) {
     if (e != cudaSuccess) return e;
     std::vector<int>().swap(hs.blas_tri_index);
   }
+  // leaf ranges (triangles, top-level items) must fit the 28 bits of a stack entry
+  if ((long long)tri_pos_count(hs) / 3 >= kMaxLeafFirst || (long long)hs.tlas_items.size() >= kMaxLeafFirst) return cudaErrorInvalidValue;
+  e = encode_node_entries(ds->nodes.as<BVH4Node>(), node_count(hs), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
   SceneView& v = ds->view;
   v.prims = ds->prims.as<DPrim>();
   v.prim_count = (int)hs.prims.size();

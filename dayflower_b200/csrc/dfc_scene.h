@@ -170,8 +170,13 @@ struct alignas(16) DLight {
 struct alignas(16) BVH4Node {
   float lox[4], loy[4], loz[4];
   float hix[4], hiy[4], hiz[4];
-  int child[4];   // >= 0 internal node, < 0 leaf whose first item is ~child
-  int count[4];   // items in a leaf (0 for internal or empty slots)
+  // As built: child >= 0 an internal node, < 0 a leaf whose first item is
+  // ~child, with count[] items (0 for internal or empty slots).  In device
+  // memory, once uploaded (encode_node_entries), child[] holds the traversal's
+  // stack entries instead: an internal node's index, or
+  // 0x80000000 | first << 2 | (count - 1) for a leaf.
+  int child[4];
+  int count[4];
 };
 static_assert(sizeof(BVH4Node) == 128, "BVH4Node is one 128-byte line");
 

@@ -38,11 +38,11 @@ DFC_D float world_t(const DPrim& pr, V3 o, const Surface& sf) {
 
 // Area-light pdf for a direction (Shape3F.evaluateProbabilityDensityFunction and
 // the Sphere3F override), in the light's object space.
-DFC_D float area_light_pdf(const SceneView& S, const DLight& lt, V3 p, V3 wi) {
+DFC_LIGHT_FN float area_light_pdf_t(const float* tri_attr, const DLight& lt, V3 p, V3 wi) {
   V3 ref = xf_point(lt.w2o, p);
   V3 w = normalize(xf_vec(lt.w2o, wi));
   if (lt.shape == kShapeTriangle) {
-    const float* q = S.tri_attr + (size_t)lt.shape_data * 24;
+    const float* q = tri_attr + (size_t)lt.shape_data * 24;
     float t = tri_t(ld3(q), ld3(q + 3), ld3(q + 6), ref, w, 0.001f, kFltMax);
     if (!(t > 0.0f)) return 0.0f;
     Surface s = triangle_surface(q, ref, w, t);
@@ -60,6 +60,7 @@ DFC_D float area_light_pdf(const SceneView& S, const DLight& lt, V3 p, V3 wi) {
   }
   return 0.0f;
 }
+DFC_D float area_light_pdf(const SceneView& S, const DLight& lt, V3 p, V3 wi) { return area_light_pdf_t(S.tri_attr, lt, p, wi); }
 
 DFC_D void film_add_to(float4* film_sum, float4* film_sq, unsigned pix, V3 L) {
   if (!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z))) return;  // AbstractCPURenderer.java:231
@@ -93,9 +94,25 @@ DFC_D void film_splat(const ShadeArgs& a, unsigned pix, uint32_t key, V3 L) {
     }
   }
 }
+// The per-job renderer's box film.  A render pass has one path per pixel and
+// its kernels run one after another on the renderer's stream, so every pixel
+// has a single writer per pass: the sums take a plain read-add-write (two
+// 16-byte loads and stores instead of seven atomics), in pass order, and a
+// render is bitwise the same on every run.  The batch engine, whose wavefront
+// can hold several samples of one pixel at once, adds with film_add_to.
+DFC_D void film_add_owned(float4* film_sum, float4* film_sq, unsigned pix, V3 L) {
+  if (!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z))) return;  // AbstractCPURenderer.java:231
+  if (luminance(L) < -1.0e-5f) return;
+  float4 s = film_sum[pix];
+  s.x += L.x; s.y += L.y; s.z += L.z; s.w += 1.0f;
+  film_sum[pix] = s;
+  float4 q = film_sq[pix];
+  q.x += L.x * L.x; q.y += L.y * L.y; q.z += L.z * L.z;
+  film_sq[pix] = q;
+}
 DFC_D void film_add(const ShadeArgs& a, unsigned pix, uint32_t key, V3 L) {
   if (a.pixel_film) film_splat(a, pix, key, L);
-  else film_add_to(a.film_sum, a.film_sq, pix, L);
+  else film_add_owned(a.film_sum, a.film_sq, pix, L);
 }
 
 // One shade step of the path tracer for every path on the work list.  In

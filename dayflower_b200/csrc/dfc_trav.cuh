@@ -91,11 +91,35 @@ DFC_D bool sphere_may_hit(float4 bs, V3 o, V3 d, float best) {
   return true;
 }
 
+// Three-operand min and max (one instruction each on sm_100).  Like fminf and
+// fmaxf they return the other operands' extreme when one operand is NaN.
+#ifndef DFC_MINMAX3
+#define DFC_MINMAX3 1
+#endif
+DFC_D float fmin3f(float a, float b, float c) {
+#if DFC_MINMAX3
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fminf(fminf(a, b), c);
+#endif
+}
+DFC_D float fmax3f(float a, float b, float c) {
+#if DFC_MINMAX3
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fmaxf(fmaxf(a, b), c);
+#endif
+}
+
 // 4 child slab tests of one node; returns a hit mask and the entry distances.
-DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin, float tmax, float tn[4]) {
+// (ox, oy, oz) = -origin * inverse direction, per axis.
+DFC_D unsigned node_hits_oi(const BVH4Node* nodes, int ni, float ox, float oy, float oz, V3 inv, float tmin, float tmax, float tn[4]) {
   const float4* p = reinterpret_cast<const float4*>(nodes + ni);
   const float4 lx = __ldg(p + 0), ly = __ldg(p + 1), lz = __ldg(p + 2), hx = __ldg(p + 3), hy = __ldg(p + 4), hz = __ldg(p + 5);
-  const float ox = -o.x * inv.x, oy = -o.y * inv.y, oz = -o.z * inv.z;
   const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
   const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
   unsigned mask = 0;
@@ -104,12 +128,15 @@ DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin
     float x0 = fmaf(lxa[k], inv.x, ox), x1 = fmaf(hxa[k], inv.x, ox);
     float y0 = fmaf(lya[k], inv.y, oy), y1 = fmaf(hya[k], inv.y, oy);
     float z0 = fmaf(lza[k], inv.z, oz), z1 = fmaf(hza[k], inv.z, oz);
-    float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-    float tfar = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax)) * 1.0000004f;
+    float tnear = fmax3f(fminf(x0, x1), fminf(y0, y1), fmaxf(fminf(z0, z1), tmin));
+    float tfar = fmin3f(fmaxf(x0, x1), fmaxf(y0, y1), fminf(fmaxf(z0, z1), tmax)) * 1.0000004f;
     tn[k] = tnear;
     if (tnear <= tfar && lxa[k] <= hxa[k]) mask |= 1u << k;
   }
   return mask;
+}
+DFC_D unsigned node_hits(const BVH4Node* nodes, int ni, V3 o, V3 inv, float tmin, float tmax, float tn[4]) {
+  return node_hits_oi(nodes, ni, -o.x * inv.x, -o.y * inv.y, -o.z * inv.z, inv, tmin, tmax, tn);
 }
 
 // Closest (or any) hit in (kTMin, tmax) along a world ray.  stack points at
@@ -172,9 +199,8 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
     float tn[4];
     const unsigned mask = in_blas ? node_hits(S.nodes, e, br.o, br.inv, 0.0f, bbest, tn) : node_hits(S.nodes, e, o, winv, 0.0f, best, tn);
     if (!mask) continue;
-    const int4* cp = reinterpret_cast<const int4*>(S.nodes + e) + 6;
-    const int4 ch = __ldg(cp), cn = __ldg(cp + 1);
-    const int cha[4] = {ch.x, ch.y, ch.z, ch.w}, cna[4] = {cn.x, cn.y, cn.z, cn.w};
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(S.nodes + e) + 6);  // stack entries (encode_node_entries)
+    const int cha[4] = {ch.x, ch.y, ch.z, ch.w};
     int ent[4];
     float entt[4];
     int nent = 0;
@@ -183,7 +209,7 @@ DFC_D bool trace_ray(const SceneView& S, V3 o, V3 d, float tmax, bool kAny, Hit*
       if (!(mask & (1u << k))) continue;
       const int c = cha[k];
       if (c >= 0) { ent[nent] = c; entt[nent] = tn[k]; ++nent; continue; }
-      const int first = ~c, cnt = cna[k];
+      const int first = (int)(((unsigned)c & 0x3FFFFFFFu) >> 2), cnt = (c & 3) + 1;
       if (in_blas) {
         for (int j = 0; j < cnt; ++j) {
           const int ti = first + j;
@@ -260,9 +286,15 @@ constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0x
 // (a lane that already holds one keeps walking nodes speculatively), then all
 // lanes test their leaves together, one item per iteration, so node and leaf
 // code do not interleave within a warp.
+#ifndef DFC_OINV
+#define DFC_OINV 0
+#endif
 struct Trav {
   V3 o, d;          // world ray
   V3 co, cinv;      // origin and inverse direction in the current space (world, or a mesh's object space)
+#if DFC_OINV
+  V3 coi;           // -co * cinv per axis (the slab test's offsets)
+#endif
   float cbest;      // closest hit so far in the current space
   float wbest;      // world closest hit, saved while in a bottom level
   float s;          // length of the object-space direction before normalisation
@@ -273,6 +305,14 @@ struct Trav {
   float t_obj;
 };
 
+DFC_D void set_offsets(Trav& T) {
+#if DFC_OINV
+  T.coi = V3{-T.co.x * T.cinv.x, -T.co.y * T.cinv.y, -T.co.z * T.cinv.z};
+#else
+  (void)T;
+#endif
+}
+
 template <bool kRecords>
 DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack, unsigned* overflow) {
   T.o = o; T.d = d; T.co = o; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
@@ -281,6 +321,7 @@ DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool a
   T.prim = -1; T.aux = -1; T.t_obj = 0.0f;
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
   T.cinv = safe_inv(d);
+  set_offsets(T);
   if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
@@ -318,14 +359,17 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   --T.sp;
   if (tag == 0u) {
     float tn[4];
+#if DFC_OINV
+    const unsigned mask = node_hits_oi(S.nodes, (int)e, T.coi.x, T.coi.y, T.coi.z, T.cinv, 0.0f, T.cbest, tn);
+#else
     const unsigned mask = node_hits(S.nodes, (int)e, T.co, T.cinv, 0.0f, T.cbest, tn);
+#endif
     if (!mask) return false;
-    const int4* cp = reinterpret_cast<const int4*>(S.nodes + e) + 6;
-    const int4 ch = __ldg(cp), cn = __ldg(cp + 1);
+    // the node's children, already in stack-entry form (encode_node_entries)
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(S.nodes + e) + 6);
     const float inf = __int_as_float(0x7f800000);
-    auto entry = [](int c, int n) -> unsigned { return c >= 0 ? (unsigned)c : (kTagLeaf | ((unsigned)(~c) << 2) | (unsigned)(n - 1)); };
     float t0 = (mask & 1u) ? tn[0] : inf, t1 = (mask & 2u) ? tn[1] : inf, t2 = (mask & 4u) ? tn[2] : inf, t3 = (mask & 8u) ? tn[3] : inf;
-    unsigned e0 = entry(ch.x, cn.x), e1 = entry(ch.y, cn.y), e2 = entry(ch.z, cn.z), e3 = entry(ch.w, cn.w);
+    unsigned e0 = (unsigned)ch.x, e1 = (unsigned)ch.y, e2 = (unsigned)ch.z, e3 = (unsigned)ch.w;
     DFC_CSWAP(t0, e0, t1, e1);
     DFC_CSWAP(t2, e2, t3, e3);
     DFC_CSWAP(t0, e0, t2, e2);
@@ -350,6 +394,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     T.cbest = fminf(T.wbest, T.cbest / T.s);
     T.co = T.o;
     T.cinv = safe_inv(T.d);
+    set_offsets(T);
     T.s = 1.0f;
     return false;
   }
@@ -359,6 +404,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   const DPrim& pm = S.prims[T.bprim];
   const ObjRay r = obj_ray(pm, T.o, T.d);
   T.co = r.o; T.cinv = r.inv; T.s = r.s;
+  set_offsets(T);
   T.wbest = T.cbest;
   T.cbest = T.wbest * r.s;
   T.sh = make_shear(r.d);
@@ -406,7 +452,10 @@ DFC_D void leaf_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
 }
 
 constexpr unsigned kNoRay = 0xffffffffu;
-constexpr int kRefill = 8;        // refill a warp's idle lanes once this many are idle
+#ifndef DFC_REFILL
+#define DFC_REFILL 8
+#endif
+constexpr int kRefill = DFC_REFILL;  // refill a warp's idle lanes once this many are idle
 // Node-phase bound and resident blocks, measured on the 2.1M-triangle benchmark
 // scene with device-built hierarchies and path-ordered ray lists: 4, 6, 8, 16, 32
 // steps gave 132.2, 134.1, 138.6, 133.8, 132.1M paths/s; 7 blocks (72 registers)
