@@ -60,21 +60,30 @@ DFC_D ObjRay obj_ray(const DPrim& pr, V3 o, V3 d) {
 
 // Object-space test of one analytic primitive; returns the object distance or -1.
 // Out of line: called at top-level leaves only, it keeps the traversal loop small.
-// kRecords adds disk ... torus (the double-precision torus solve enlarges the
-// call tree enough to cost the traversal loop registers, so scenes without
-// those shapes run the instantiation without them).
+// Its arguments are plain values (no references to the kernel's parameters or
+// to a ray struct), so a call passes them in registers and the caller keeps no
+// copy of the scene or the ray in local memory.  kRecords adds disk ... torus
+// (the double-precision torus solve enlarges the call tree enough to cost the
+// traversal loop registers, so scenes without those shapes run the
+// instantiation without them).
 template <bool kRecords>
-__device__ __noinline__ float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
-  switch (pr.shape) {
-    case kShapeSphere: return sphere_t(r.o, r.d, kTMin, tmax_obj);
+__device__ __noinline__ float prim_t_v(const float* tri_attr, const float* rects, const float* shapes, int shape, int data, float ox, float oy, float oz,
+               float dx, float dy, float dz, float tmax_obj) {
+  const V3 o = {ox, oy, oz}, d = {dx, dy, dz};
+  switch (shape) {
+    case kShapeSphere: return sphere_t(o, d, kTMin, tmax_obj);
     case kShapeTriangle: {
-      const float* q = S.tri_attr + (size_t)pr.data * 24;
-      return tri_t(ld3(q), ld3(q + 3), ld3(q + 6), r.o, r.d, kTMin, tmax_obj);
+      const float* q = tri_attr + (size_t)data * 24;
+      return tri_t(ld3(q), ld3(q + 3), ld3(q + 6), o, d, kTMin, tmax_obj);
     }
-    case kShapeRectangle: return rect_t(S.rects + (size_t)pr.data * 16, r.o, r.d, kTMin, tmax_obj);
-    case kShapePlane: return plane_t(r.o, r.d, kTMin, tmax_obj);
-    default: return kRecords ? record_shape_t(pr.shape, S.shapes + pr.data, r.o, r.d, kTMin, tmax_obj) : -1.0f;
+    case kShapeRectangle: return rect_t(rects + (size_t)data * 16, o, d, kTMin, tmax_obj);
+    case kShapePlane: return plane_t(o, d, kTMin, tmax_obj);
+    default: return kRecords ? record_shape_t(shape, shapes + data, o, d, kTMin, tmax_obj) : -1.0f;
   }
+}
+template <bool kRecords>
+DFC_D float prim_t(const SceneView& S, const DPrim& pr, const ObjRay& r, float tmax_obj) {
+  return prim_t_v<kRecords>(S.tri_attr, S.rects, S.shapes, pr.shape, pr.data, r.o.x, r.o.y, r.o.z, r.d.x, r.d.y, r.d.z, tmax_obj);
 }
 
 // Conservative world-space rejection of a top-level item by its bounding
@@ -93,26 +102,15 @@ DFC_D bool sphere_may_hit(float4 bs, V3 o, V3 d, float best) {
 
 // Three-operand min and max (one instruction each on sm_100).  Like fminf and
 // fmaxf they return the other operands' extreme when one operand is NaN.
-#ifndef DFC_MINMAX3
-#define DFC_MINMAX3 1
-#endif
 DFC_D float fmin3f(float a, float b, float c) {
-#if DFC_MINMAX3
   float r;
   asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
   return r;
-#else
-  return fminf(fminf(a, b), c);
-#endif
 }
 DFC_D float fmax3f(float a, float b, float c) {
-#if DFC_MINMAX3
   float r;
   asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
   return r;
-#else
-  return fmaxf(fmaxf(a, b), c);
-#endif
 }
 
 // 4 child slab tests of one node; returns a hit mask and the entry distances.
@@ -286,15 +284,9 @@ constexpr unsigned kTagMask = 0xC0000000u, kTagLeaf = 0x80000000u, kTagMesh = 0x
 // (a lane that already holds one keeps walking nodes speculatively), then all
 // lanes test their leaves together, one item per iteration, so node and leaf
 // code do not interleave within a warp.
-#ifndef DFC_OINV
-#define DFC_OINV 0
-#endif
 struct Trav {
   V3 o, d;          // world ray
   V3 co, cinv;      // origin and inverse direction in the current space (world, or a mesh's object space)
-#if DFC_OINV
-  V3 coi;           // -co * cinv per axis (the slab test's offsets)
-#endif
   float cbest;      // closest hit so far in the current space
   float wbest;      // world closest hit, saved while in a bottom level
   float s;          // length of the object-space direction before normalisation
@@ -305,14 +297,6 @@ struct Trav {
   float t_obj;
 };
 
-DFC_D void set_offsets(Trav& T) {
-#if DFC_OINV
-  T.coi = V3{-T.co.x * T.cinv.x, -T.co.y * T.cinv.y, -T.co.z * T.cinv.z};
-#else
-  (void)T;
-#endif
-}
-
 template <bool kRecords>
 DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool any, int* stack, unsigned* overflow) {
   T.o = o; T.d = d; T.co = o; T.cbest = tmax; T.wbest = tmax; T.s = 1.0f;
@@ -321,7 +305,6 @@ DFC_D void trav_init(const SceneView& S, Trav& T, V3 o, V3 d, float tmax, bool a
   T.prim = -1; T.aux = -1; T.t_obj = 0.0f;
   if (!isfinite(o.x + o.y + o.z + d.x + d.y + d.z)) return;  // misses everything (see trace_ray)
   T.cinv = safe_inv(d);
-  set_offsets(T);
   if (S.tlas_root >= 0) { stack[0] = S.tlas_root; T.sp = 1; }
   for (int u = 0; u < S.unbounded_count; ++u) {
     const int pi = S.unbounded[u];
@@ -359,11 +342,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   --T.sp;
   if (tag == 0u) {
     float tn[4];
-#if DFC_OINV
-    const unsigned mask = node_hits_oi(S.nodes, (int)e, T.coi.x, T.coi.y, T.coi.z, T.cinv, 0.0f, T.cbest, tn);
-#else
     const unsigned mask = node_hits(S.nodes, (int)e, T.co, T.cinv, 0.0f, T.cbest, tn);
-#endif
     if (!mask) return false;
     // the node's children, already in stack-entry form (encode_node_entries)
     const int4 ch = __ldg(reinterpret_cast<const int4*>(S.nodes + e) + 6);
@@ -394,8 +373,7 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     T.cbest = fminf(T.wbest, T.cbest / T.s);
     T.co = T.o;
     T.cinv = safe_inv(T.d);
-    set_offsets(T);
-    T.s = 1.0f;
+      T.s = 1.0f;
     return false;
   }
   // enter a mesh's bottom level
@@ -404,7 +382,6 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
   const DPrim& pm = S.prims[T.bprim];
   const ObjRay r = obj_ray(pm, T.o, T.d);
   T.co = r.o; T.cinv = r.inv; T.s = r.s;
-  set_offsets(T);
   T.wbest = T.cbest;
   T.cbest = T.wbest * r.s;
   T.sh = make_shear(r.d);
