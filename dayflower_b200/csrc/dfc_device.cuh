@@ -135,11 +135,13 @@ DFC_D bool camera_ray(const float* c, float ix, float iy, float px, float py, fl
 DFC_D float gamma_n(int n) { const float e = 5.9604645e-8f; return (n * e) / (1.0f - n * e); }
 
 // Double-precision edge functions (Triangle3F.java:537-546), taken only when a
-// float edge function is exactly zero; kept out of line to keep the hot loop small.
-static __device__ __noinline__ void tri_edges_fp64(float x0, float y0, float x1, float y1, float x2, float y2, float* e0, float* e1, float* e2) {
-  *e0 = (float)((double)y2 * (double)x1 - (double)x2 * (double)y1);
-  *e1 = (float)((double)y0 * (double)x2 - (double)x0 * (double)y2);
-  *e2 = (float)((double)y1 * (double)x0 - (double)x1 * (double)y0);
+// float edge function is exactly zero; kept out of line to keep the hot loop
+// small, and returned by value so that the caller's edge values stay in
+// registers (an address taken for an out-of-line call puts them in local memory).
+struct Edges { float e0, e1, e2; };
+static __device__ __noinline__ Edges tri_edges_fp64(float x0, float y0, float x1, float y1, float x2, float y2) {
+  return Edges{(float)((double)y2 * (double)x1 - (double)x2 * (double)y1), (float)((double)y0 * (double)x2 - (double)x0 * (double)y2),
+               (float)((double)y1 * (double)x0 - (double)x1 * (double)y0)};
 }
 
 // geometry/shape/Triangle3F.java:505 watertight test; returns -1 on a miss.
@@ -159,7 +161,7 @@ DFC_D float tri_t(V3 a, V3 b, V3 c, V3 o, V3 d, float tmin, float tmax) {
   float e0 = x1 * y2 - y1 * x2;
   float e1 = x2 * y0 - y2 * x0;
   float e2 = x0 * y1 - y0 * x1;
-  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) tri_edges_fp64(x0, y0, x1, y1, x2, y2, &e0, &e1, &e2);
+  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) { const Edges E = tri_edges_fp64(x0, y0, x1, y1, x2, y2); e0 = E.e0; e1 = E.e1; e2 = E.e2; }
   if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
   const float det = e0 + e1 + e2;
   if (det == 0.0f) return -1.0f;
@@ -211,7 +213,7 @@ DFC_D float tri_t_sheared(float4 A, float4 B, float4 C, V3 o, const Shear& sh, f
   float e0 = x1 * y2 - y1 * x2;
   float e1 = x2 * y0 - y2 * x0;
   float e2 = x0 * y1 - y0 * x1;
-  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) tri_edges_fp64(x0, y0, x1, y1, x2, y2, &e0, &e1, &e2);
+  if (e0 == 0.0f || e1 == 0.0f || e2 == 0.0f) { const Edges E = tri_edges_fp64(x0, y0, x1, y1, x2, y2); e0 = E.e0; e1 = E.e1; e2 = E.e2; }
   if ((e0 < 0.0f || e1 < 0.0f || e2 < 0.0f) && (e0 > 0.0f || e1 > 0.0f || e2 > 0.0f)) return -1.0f;
   const float det = e0 + e1 + e2;
   if (det == 0.0f) return -1.0f;
@@ -1129,10 +1131,12 @@ DFC_LIGHT_FN V3 image_sky(const float* q, V3 d) {
   return lerp3(lerp3(px(x0, y0), px(x1, y0), xf), lerp3(px(x0, y1), px(x1, y1), xf), yf);
 }
 
+// A light sample; the out-of-line samplers return pdf 0 for no sample (every
+// caller skips a sample whose pdf is not positive).
 struct LightS { V3 L, p, wi; float pdf; };
 
 // DiffuseAreaLight.sampleRadianceIncoming for a triangle or sphere shape.
-DFC_LIGHT_FN bool area_light_sample(const float* tri_attr, const DLight& lt, V3 p, float u, float v, LightS* o) {
+DFC_LIGHT_FN LightS area_light_sample(const float* tri_attr, const DLight& lt, V3 p, float u, float v) {
   V3 ref = xf_point(lt.w2o, p);
   V3 sp, sn;
   float pdf;
@@ -1145,10 +1149,10 @@ DFC_LIGHT_FN bool area_light_sample(const float* tri_attr, const DLight& lt, V3 
     sp = {A.x * b0 + B.x * b1 + C.x * b2, A.y * b0 + B.y * b1 + C.y * b2, A.z * b0 + B.z * b1 + C.z * b2};
     sn = normalize(ld3(q + 15) * b0 + ld3(q + 18) * b1 + ld3(q + 21) * b2);
     V3 inc = sp - ref;
-    if (dot(inc, inc) == 0.0f) return false;
+    if (dot(inc, inc) == 0.0f) return LightS{};
     V3 incn = normalize(inc);
     pdf = dot(inc, inc) / fabsf(dot(sn, -incn));
-    if (isinf(pdf) || isnan(pdf)) return false;
+    if (isinf(pdf) || isnan(pdf)) return LightS{};
   } else if (lt.shape == kShapeSphere) {
     if (dot(ref, ref) <= 1.0f) {
       float ct = 1.0f - 2.0f * u, st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct)), s, c;
@@ -1156,9 +1160,9 @@ DFC_LIGHT_FN bool area_light_sample(const float* tri_attr, const DLight& lt, V3 
       sp = {st * c, st * s, ct};
       sn = normalize(sp);
       V3 inc = sp - ref;
-      if (dot(inc, inc) == 0.0f) return false;
+      if (dot(inc, inc) == 0.0f) return LightS{};
       pdf = dot(inc, inc) / fabsf(dot(sn, -normalize(inc)));
-      if (isinf(pdf) || isnan(pdf)) return false;
+      if (isinf(pdf) || isnan(pdf)) return LightS{};
     } else {
       float dist = len(ref), dr = 1.0f / dist;
       V3 dc = (-ref) * dr;
@@ -1174,19 +1178,19 @@ DFC_LIGHT_FN bool area_light_sample(const float* tri_attr, const DLight& lt, V3 
       sp = sd; sn = normalize(sd); pdf = 1.0f / (2.0f * kPi * (1.0f - ctm));
     }
   } else {
-    return false;  // Shape3F.sample default: no sample for other shapes
+    return LightS{};  // Shape3F.sample default: no sample for other shapes
   }
   V3 pw = xf_point(lt.o2w, sp);
   V3 nw = normalize(xf_vec_t(lt.w2o, sn));
   V3 wi = normalize(pw - p);
-  if (pdf > 0.0f && (lt.two_sided || dot(nw, -wi) > 0.0f)) { *o = LightS{ld3(lt.radiance), pw, wi, pdf}; return true; }
-  return false;
+  if (pdf > 0.0f && (lt.two_sided || dot(nw, -wi) > 0.0f)) return LightS{ld3(lt.radiance), pw, wi, pdf};
+  return LightS{};
 }
 
 // PerezLight and ImageLight (scene/light/ImageLight.java:207) sampleRadianceIncoming;
 // q is the light's record in the sky pool, gw and sw the surface's geometric and
 // shading normals.
-DFC_LIGHT_FN bool sky_light_sample(const float* q, int type, V3 p, V3 gw, V3 sw, float u, float v, float sun_pick, LightS* o) {
+DFC_LIGHT_FN LightS sky_light_sample(const float* q, int type, V3 p, V3 gw, V3 sw, float u, float v, float sun_pick) {
   if (type == kLightPerez) {
     const float* dist = q + 48;
     V3 sunW = ld3(q + 38), sunO = ld3(q + 35);
@@ -1196,43 +1200,41 @@ DFC_LIGHT_FN bool sky_light_sample(const float* q, int type, V3 p, V3 gw, V3 sw,
         float phi = atan2f(sunO.y, sunO.x);
         if (phi < 0.0f) phi += 2.0f * kPi;
         float pdf = d2_pdf(dist, phi * (1.0f / (2.0f * kPi)), acosf(clampf(sunO.z, -1.0f, 1.0f)) * (1.0f / kPi)) / (2.0f * kPi * kPi * st);
-        if (pdf != 0.0f) { *o = LightS{ld3(q + 32), p + sunW * (2.0f * q[45]), sunW, pdf}; return true; }
+        if (pdf != 0.0f) return LightS{ld3(q + 32), p + sunW * (2.0f * q[45]), sunW, pdf};
       }
     }
     float ru, rv;
     d2_remap(dist, u, v, &ru, &rv);
     float pr = d2_pdf(dist, ru, rv);
-    if (pr == 0.0f) return false;
+    if (pr == 0.0f) return LightS{};
     float sth, cth, sph, cph;
     sincosf(rv * kPi, &sth, &cth);
     sincosf(ru * 2.0f * kPi, &sph, &cph);
     V3 dobj = {sth * cph, sth * sph, cth};
     V3 dw = normalize(xf_vec(q, dobj));
     float st = sint(dobj);
-    if (st == 0.0f) return false;
-    *o = LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
-    return true;
+    if (st == 0.0f) return LightS{};
+    return LightS{sat0(perez_sky(q, dobj)), p + dw * (2.0f * q[45]), dw, pr / (2.0f * kPi * kPi * st)};
   }
   float ru, rv;
   d2_remap(q + 40, u, v, &ru, &rv);
   const float pr = d2_pdf(q + 40, ru, rv);
-  if (pr == 0.0f) return false;
+  if (pr == 0.0f) return LightS{};
   float sth, cth, sph, cph;
   sincosf(rv * kPi, &sth, &cth);
   sincosf(ru * 2.0f * kPi, &sph, &cph);
   const V3 dobj = {sth * cph, sth * sph, cth};
   const V3 dw = normalize(xf_vec(q, dobj));
   const float st = sint(dobj);
-  if (st == 0.0f) return false;
-  *o = LightS{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
-  return true;
+  if (st == 0.0f) return LightS{};
+  return LightS{image_sky(q, dobj), p + dw * (2.0f * q[35]), dw, pr / (2.0f * kPi * kPi * st)};
 }
 
 // Light.sampleRadianceIncoming for each supported light type.
 DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf, float u, float v, float sun_pick, LightS* o) {
   const V3 p = sf.p;
   switch (lt.type) {
-    case kLightDiffuseArea: return area_light_sample(S.tri_attr, lt, p, u, v, o);
+    case kLightDiffuseArea: *o = area_light_sample(S.tri_attr, lt, p, u, v); return o->pdf > 0.0f;
     case kLightPoint: {
       V3 pos = ld3(lt.pos);
       V3 d = pos - p;
@@ -1257,7 +1259,7 @@ DFC_D bool light_sample(const SceneView& S, const DLight& lt, const Surface& sf,
       return true;
     }
     case kLightPerez:
-    case kLightImage: return sky_light_sample(S.perez + lt.perez, lt.type, p, sf.g.w, sf.s.w, u, v, sun_pick, o);
+    case kLightImage: *o = sky_light_sample(S.perez + lt.perez, lt.type, p, sf.g.w, sf.s.w, u, v, sun_pick); return o->pdf > 0.0f;
   }
   return false;
 }
