@@ -333,6 +333,11 @@ int enqueue_pass(dfc_renderer* r) {
       so.keys = r->d_sort_keys.as<unsigned char>();
       so.bins = r->d_sort_bins.as<unsigned>() + (size_t)s * 2 * kSortBins;
       so.sorted = r->d_sorted.as<unsigned>();
+      // path-ordered ray lists pay for their extra launch only on large passes; small ones stay launch-bound
+      a.ray_mask = r->paths >= kOrderedRayListMinPaths ? r->d_ray_mask.as<unsigned char>() : nullptr;
+      // the next work list also in path order (the material sort below keeps that order within
+      // each warp's run, so neighbouring lanes read neighbouring paths' state)
+      a.ordered_work = a.ray_mask != nullptr;
       ev = stage_begin(r, DFC_KERNEL_SORT_COUNT);
       k_sort_count<<<shade_grid, 256, 0, r->stream>>>(so);
       stage_end(r, ev);
@@ -340,8 +345,6 @@ int enqueue_pass(dfc_renderer* r) {
       k_sort_scatter<<<sort_grid, 256, 0, r->stream>>>(so);
       stage_end(r, ev);
       a.work_list = so.sorted;
-      // path-ordered ray lists pay for their extra launch only on large passes; small ones stay launch-bound
-      a.ray_mask = r->paths >= kOrderedRayListMinPaths ? r->d_ray_mask.as<unsigned char>() : nullptr;
       // the two-lobe kernel shades the matte ... plastic hits, misses and light-ray-only paths; the general
       // kernel the other materials, when the scene has any
       ShadeArgs simple = a;
@@ -365,7 +368,7 @@ int enqueue_pass(dfc_renderer* r) {
       if (a.ray_mask && s < steps - 1) {  // the next step's ray list, in path order
         ev = stage_begin(r, DFC_KERNEL_RAY_LIST);
         k_ray_list_ordered<<<(r->paths + kRayListBlock - 1) / kRayListBlock, kRayListBlock, 0, r->stream>>>(
-            a.ray_mask, r->paths, a.next_ray_list, a.next_ray_count);
+            a.ray_mask, r->paths, a.next_ray_list, a.next_ray_count, a.ordered_work ? a.next_work_list : nullptr, a.next_work_count);
         stage_end(r, ev);
         r->launches += 1;
       }

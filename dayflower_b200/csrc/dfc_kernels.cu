@@ -50,16 +50,20 @@ __global__ void k_raygen(RaygenArgs a) {
 }
 
 // One block per kRayListBlock consecutive paths: each thread counts its
-// path's rays, a block scan places them, one atomic reserves the block's run.
-// Within a run the rays are in path (pixel) order, so the traversal's warps
-// fetch neighbouring pixels' rays together.
+// path's rays (and, with a work list, whether the path is shaded again), a
+// block scan places them, one atomic per list reserves the block's run.
+// Within a run the entries are in path (pixel) order, so the traversal's
+// warps fetch neighbouring pixels' rays together and the shading kernel reads
+// neighbouring paths' state.
 __global__ void __launch_bounds__(kRayListBlock) k_ray_list_ordered(const unsigned char* ray_mask, unsigned paths, unsigned* ray_list,
-                                                                     unsigned* ray_count) {
+                                                                     unsigned* ray_count, unsigned* work_list, unsigned* work_count) {
+  static_assert(kRayListBlock * 3 < 65536, "ray and work counts are packed in 16-bit fields");
   __shared__ unsigned warp_sum[kRayListBlock / 32];
-  __shared__ unsigned block_base;
+  __shared__ unsigned block_base, work_base;
   const unsigned p = blockIdx.x * kRayListBlock + threadIdx.x;
   const unsigned m = p < paths ? (unsigned)ray_mask[p] : 0u;
-  const unsigned c = __popc(m & 7u);
+  const unsigned keep = work_list != nullptr && (m & kMaskKeep) ? 1u : 0u;
+  const unsigned c = __popc(m & 7u) | (keep << 16);  // rays, work entries (packed)
   const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   unsigned incl = c;  // inclusive warp scan
   for (int o = 1; o < 32; o <<= 1) {
@@ -71,13 +75,17 @@ __global__ void __launch_bounds__(kRayListBlock) k_ray_list_ordered(const unsign
   if (threadIdx.x == 0) {
     unsigned acc = 0;
     for (int w = 0; w < kRayListBlock / 32; ++w) { const unsigned t = warp_sum[w]; warp_sum[w] = acc; acc += t; }
-    block_base = acc ? atomicAdd(ray_count, acc) : 0u;
+    const unsigned rays = acc & 0xffffu, works = acc >> 16;
+    block_base = rays ? atomicAdd(ray_count, rays) : 0u;
+    work_base = works ? atomicAdd(work_count, works) : 0u;
   }
   __syncthreads();
-  unsigned at = block_base + warp_sum[warp] + incl - c;
+  const unsigned excl = warp_sum[warp] + incl - c;
+  unsigned at = block_base + (excl & 0xffffu);
   if (m & 1u) ray_list[at++] = p << 3;
   if (m & 2u) ray_list[at++] = (p << 3) | ((m & 8u) ? 4u : 0u) | 1u;
   if (m & 4u) ray_list[at] = (p << 3) | 2u;
+  if (keep) work_list[work_base + (excl >> 16)] = p;
 }
 
 // ---- material sort of the shade work list -----------------------------------

@@ -125,8 +125,11 @@ struct ShadeArgs {
   unsigned* next_ray_count;
   // When set (per-job renderer), shading records each path's new rays here
   // (bit 0 extension, 1 shadow, 2 MIS, 3 shadow is any-hit) instead of
-  // appending them, and k_ray_list_ordered builds the next ray list in path order.
+  // appending them, and k_ray_list_ordered builds the next ray list in path
+  // order.  With ordered_work set, bit 4 (kMaskKeep) marks a path that is
+  // shaded again and the next work list is built in path order the same way.
   unsigned char* ray_mask;
+  int ordered_work;
   float4* beta;
   float4* radiance;
   uint4* meta;
@@ -238,7 +241,9 @@ __global__ void k_shade_primary(ShadeArgs a, int algorithm);
 // The next step's ray list from ShadeArgs::ray_mask, paths in index order
 // within each block of kRayListBlock paths.
 constexpr int kRayListBlock = 256;
-__global__ void k_ray_list_ordered(const unsigned char* ray_mask, unsigned paths, unsigned* ray_list, unsigned* ray_count);
+constexpr unsigned kMaskKeep = 16u;
+__global__ void k_ray_list_ordered(const unsigned char* ray_mask, unsigned paths, unsigned* ray_list, unsigned* ray_count,
+                                   unsigned* work_list, unsigned* work_count);
 __global__ void k_trace_ao(AoArgs a);
 // RAY_TRACING (scene/Scene.java:786 doRadianceRayTracer): one thread per camera
 // sample walks the sample's specular reflection/transmission tree depth first.

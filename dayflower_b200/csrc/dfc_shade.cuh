@@ -138,7 +138,8 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
     const unsigned i = base + threadIdx.x;
     bool spawn_ext = false, spawn_shadow = false, spawn_mis = false, keep = false, shadow_any = false, retire = false;
     unsigned p = 0, job = 0;
-    if (i < n) {
+    const bool valid = i < n;
+    if (valid) {
       p = a.work_list[i];
       const DJob* J = nullptr;
       if constexpr (kMulti) { job = a.slot_job[p]; J = a.jobs + job; }
@@ -351,7 +352,9 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
     // appends (all lanes of the warp take part)
     if (!kMulti && a.ray_mask) {
       // rays listed later in path order (k_ray_list_ordered): pixel-coherent traversal batches
-      if (i < n) a.ray_mask[p] = (unsigned char)((spawn_ext ? 1u : 0u) | (spawn_shadow ? 2u : 0u) | (spawn_mis ? 4u : 0u) | (shadow_any ? 8u : 0u));
+      if (valid)
+        a.ray_mask[p] = (unsigned char)((spawn_ext ? 1u : 0u) | (spawn_shadow ? 2u : 0u) | (spawn_mis ? 4u : 0u) | (shadow_any ? 8u : 0u) |
+                                        (keep && a.ordered_work ? kMaskKeep : 0u));
     } else {
       const unsigned r0 = warp_append(a.next_ray_count, spawn_ext);
       if (spawn_ext) a.next_ray_list[r0] = p << 3;
@@ -360,8 +363,10 @@ __device__ __forceinline__ void shade_path(const ShadeArgs& a) {
       const unsigned r2 = warp_append(a.next_ray_count, spawn_mis);
       if (spawn_mis) a.next_ray_list[r2] = (p << 3) | 2u;
     }
-    const unsigned w = warp_append(a.next_work_count, keep);
-    if (keep) a.next_work_list[w] = p;
+    if (kMulti || !a.ordered_work) {
+      const unsigned w = warp_append(a.next_work_count, keep);
+      if (keep) a.next_work_list[w] = p;
+    }
     if constexpr (kMulti) {
       // retired slots back on the free stack; per-job retire counts, one atomic per job in the warp
       const unsigned f = warp_append(a.free_top, retire);
