@@ -1232,9 +1232,11 @@ extern "C" int dfc_engine_autotune(dfc_engine* e, const dfc_job_desc* jobs, int 
     c = best;
     c.shade_threads = 128;
     consider(c);
-    c = best;
-    c.shade_blocks_per_sm = 16;
-    consider(c);
+    for (int sb : {16, 64}) {  // more shading blocks than fit at once let the block scheduler balance the SMs
+      c = best;
+      c.shade_blocks_per_sm = sb;
+      consider(c);
+    }
   }
   if (best_v <= 0.0) return efail(e, DFC_E_CUDA, "autotune: no candidate ran: " + e->err);
   int rc = dfc_engine_configure(e, &best);
