@@ -521,13 +521,25 @@ def main():
         q.setMaximumBounce(CONFIG["max_bounce"])
         q.setMinimumBounceRussianRoulette(CONFIG["min_rr"])
 
+        parts = {"set_scene_s": 0.0, "setup_s": 0.0, "render_s": 0.0, "read_image_s": 0.0}
+
         def e2e_step():
+            t = [time.perf_counter()]
             q.setScene(compiled)
+            t.append(time.perf_counter())
             q.setup()
+            t.append(time.perf_counter())
             q.render(args.spp)
-            return q.getImage()
+            t.append(time.perf_counter())
+            im = q.getImage()
+            t.append(time.perf_counter())
+            for k, a_, b_ in zip(parts, t, t[1:]):
+                parts[k] += b_ - a_
+            return im
 
         e2e_step()  # warm-up
+        for k in parts:
+            parts[k] = 0.0
         if world > 1:
             dist.barrier()
         e_steps = 2
@@ -535,10 +547,12 @@ def main():
         for _ in range(e_steps):
             img = e2e_step()
         dt = time.perf_counter() - t0
+        commit_ms = q.commitMillis()
         e2e_value, _ = replica_throughput(paths_per_step * e_steps, dt, world, "cuda")
         q.dispose()
         e2e = {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(img.nbytes), "steps": e_steps,
+               "per_step_s": {k: v / e_steps for k, v in parts.items()}, "last_commit_ms": commit_ms,
                "note": "per step: setScene from host arrays (upload + acceleration build) + setup + render(%d) + RGBA8 read-back" % args.spp}
 
     if rank == 0:
