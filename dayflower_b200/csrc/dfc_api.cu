@@ -474,14 +474,17 @@ int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t c
   DFC_LOCK(r);
   if (!name) return fail(r, DFC_E_INVALID_ARG, "name == null");
   if (count < 0 || (count > 0 && !data)) return fail(r, DFC_E_INVALID_ARG, "data == null or negative count");
-  if (type == DFC_F32) {
-    const float* f = static_cast<const float*>(data);
-    r->staged.f32[name].assign(f, f + count);
-  } else if (type == DFC_I32) {
-    const int32_t* q = static_cast<const int32_t*>(data);
-    r->staged.i32[name].assign(q, q + count);
-  } else {
-    return fail(r, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
+  if (type != DFC_F32 && type != DFC_I32) return fail(r, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
+  try {  // the staging arrays are page-locked host memory (PinnedAllocator)
+    if (type == DFC_F32) {
+      const float* f = static_cast<const float*>(data);
+      r->staged.f32[name].assign(f, f + count);
+    } else {
+      const int32_t* q = static_cast<const int32_t*>(data);
+      r->staged.i32[name].assign(q, q + count);
+    }
+  } catch (const std::bad_alloc&) {
+    return fail(r, DFC_E_OOM, std::string("no page-locked host memory to stage ") + name);
   }
   return DFC_OK;
 }

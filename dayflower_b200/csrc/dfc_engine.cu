@@ -840,14 +840,17 @@ int dfc_engine_scene_put(dfc_engine* e, const char* name, const void* data, int6
   std::lock_guard<std::mutex> c(e->commit_mu);
   if (!name) return efail(e, DFC_E_INVALID_ARG, "name == null");
   if (count < 0 || (count > 0 && !data)) return efail(e, DFC_E_INVALID_ARG, "data == null or negative count");
-  if (type == DFC_F32) {
-    const float* f = static_cast<const float*>(data);
-    e->staged.f32[name].assign(f, f + count);
-  } else if (type == DFC_I32) {
-    const int32_t* q = static_cast<const int32_t*>(data);
-    e->staged.i32[name].assign(q, q + count);
-  } else {
-    return efail(e, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
+  if (type != DFC_F32 && type != DFC_I32) return efail(e, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
+  try {  // the staging arrays are page-locked host memory (PinnedAllocator)
+    if (type == DFC_F32) {
+      const float* f = static_cast<const float*>(data);
+      e->staged.f32[name].assign(f, f + count);
+    } else {
+      const int32_t* q = static_cast<const int32_t*>(data);
+      e->staged.i32[name].assign(q, q + count);
+    }
+  } catch (const std::bad_alloc&) {
+    return efail(e, DFC_E_OOM, std::string("no page-locked host memory to stage ") + name);
   }
   return DFC_OK;
 }

@@ -52,9 +52,9 @@ struct Fail {
   std::string msg;
 };
 
-template <typename T>
-const std::vector<T>& get(const std::map<std::string, std::vector<T>>& m, const char* name) {
-  static const std::vector<T> empty;
+template <typename V>
+const V& get(const std::map<std::string, V>& m, const char* name) {
+  static const V empty;
   auto it = m.find(name);
   return it == m.end() ? empty : it->second;
 }
@@ -70,10 +70,10 @@ struct Decoder {
 
   Decoder(const Staged& s, int l, HostScene& h, bool dev) : st(s), layout(l), hs(h), device_blas(dev) {}
 
-  const std::vector<float>& F(const char* n) { return get(st.f32, n); }
-  const std::vector<int32_t>& I(const char* n) { return get(st.i32, n); }
+  const StagedF& F(const char* n) { return get(st.f32, n); }
+  const StagedI& I(const char* n) { return get(st.i32, n); }
 
-  void texref(const std::vector<int32_t>& arr, int base, int slot, int* ida, int* offa, int* idb, int* offb) {
+  void texref(const StagedI& arr, int base, int slot, int* ida, int* offa, int* idb, int* offb) {
     if (layout == 2) {
       size_t k = (size_t)base + (size_t)slot * 4;
       if (k + 4 > arr.size()) throw Fail{DFC_E_INVALID_ARG, "material record out of range"};
@@ -85,7 +85,7 @@ struct Decoder {
       *ida = v & 0xFF; *offa = (v >> 8) & 0xFF; *idb = (v >> 16) & 0xFF; *offb = (v >> 24) & 0xFF;
     }
   }
-  int plain(const std::vector<int32_t>& arr, int base, int slot) {
+  int plain(const StagedI& arr, int base, int slot) {
     size_t k = (size_t)base + (size_t)slot * (layout == 2 ? 4 : 1);
     if (k >= arr.size()) throw Fail{DFC_E_INVALID_ARG, "material record out of range"};
     return arr[k];
@@ -420,13 +420,13 @@ struct Decoder {
 
   // Checks a packed Distribution2F (sampler/Distribution2F.java toArray) so that
   // every offset and count the device follows stays inside the array.
-  void validate_distribution1(const std::vector<float>& A, size_t off) {
+  void validate_distribution1(const StagedF& A, size_t off) {
     if (off + 4 > A.size()) throw Fail{DFC_E_INVALID_ARG, "distribution out of range"};
     const float len = A[off], cdf = A[off + 1], cnt = A[off + 2];
     if (!(cnt >= 1.0f && cdf == cnt + 1.0f && len == 4.0f + cdf + cnt) || off + (size_t)len > A.size())
       throw Fail{DFC_E_INVALID_ARG, "malformed Distribution1F"};
   }
-  void validate_distribution2(const std::vector<float>& A, size_t base) {
+  void validate_distribution2(const StagedF& A, size_t base) {
     if (base + 3 > A.size()) throw Fail{DFC_E_INVALID_ARG, "distribution out of range"};
     const float tab = A[base + 1];  // offset table length = 1 + conditionals
     if (!(tab >= 2.0f && tab < 1.0e6f) || base + 2 + (size_t)tab > A.size()) throw Fail{DFC_E_INVALID_ARG, "malformed Distribution2F"};
@@ -521,7 +521,7 @@ struct Decoder {
     if (X.size() < (size_t)np * 32) throw Fail{DFC_E_INVALID_ARG, "primitiveMatrix44FArray is shorter than 32 floats per primitive"};
     if (C.size() < 19) throw Fail{DFC_E_INVALID_ARG, "cameraArray needs 19 floats"};
     std::memcpy(hs.camera, C.data(), sizeof hs.camera);
-    hs.rects = R;
+    hs.rects.assign(R.begin(), R.end());
     // the record-sized shapes share one float pool on the device
     for (RecordArray& ra : record_arrays) {
       ra.base = hs.shapes.size();
@@ -529,7 +529,7 @@ struct Decoder {
       hs.shapes.insert(hs.shapes.end(), A.begin(), A.end());
     }
     if (hs.shapes.empty()) hs.shapes.assign(4, 0.0f);
-    hs.perez = F("lightPerezLightArray");  // the sky pool: Perez records, then image light records
+    hs.perez.assign(F("lightPerezLightArray").begin(), F("lightPerezLightArray").end());  // the sky pool: Perez records, then image light records
     {
       const auto& img = F("lightImageLightArray");
       hs.perez.insert(hs.perez.end(), img.begin(), img.end());

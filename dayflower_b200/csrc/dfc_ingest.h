@@ -1,8 +1,11 @@
 // Host-side scene ingest: reference compiled arrays -> device records.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -11,10 +14,33 @@
 
 namespace dfc {
 
+// Page-locked host memory for the staging arrays: the scene upload then
+// copies straight from them by DMA instead of through the driver's pageable
+// bounce buffers, whose speed depends on the host's memory traffic.
+template <typename T>
+struct PinnedAllocator {
+  using value_type = T;
+  PinnedAllocator() = default;
+  template <typename U>
+  PinnedAllocator(const PinnedAllocator<U>&) {}
+  T* allocate(size_t n) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, n * sizeof(T), cudaHostAllocPortable) != cudaSuccess) throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) { cudaFreeHost(p); }
+  template <typename U>
+  bool operator==(const PinnedAllocator<U>&) const { return true; }
+  template <typename U>
+  bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+using StagedF = std::vector<float, PinnedAllocator<float>>;
+using StagedI = std::vector<int32_t, PinnedAllocator<int32_t>>;
+
 // Arrays staged by dfc_scene_put, by reference field name.
 struct Staged {
-  std::map<std::string, std::vector<float>> f32;
-  std::map<std::string, std::vector<int32_t>> i32;
+  std::map<std::string, StagedF> f32;
+  std::map<std::string, StagedI> i32;
   // Empties every array but keeps its allocation, so that staging the next
   // scene of a similar size copies into memory that is already mapped.
   void recycle() {

@@ -33,7 +33,7 @@ typedef enum dfc_status {
   DFC_OK = 0,
   DFC_E_INVALID_ARG = 1,   /* NullPointerException / IllegalArgumentException */
   DFC_E_UNSUPPORTED = 2,   /* unknown or unimplemented shape, material, texture or light id */
-  DFC_E_OOM = 3,           /* device allocation failed */
+  DFC_E_OOM = 3,           /* device (or page-locked host staging) allocation failed */
   DFC_E_CUDA = 4,          /* any other CUDA runtime error */
   DFC_E_TIMEOUT = 5,       /* a device-side iteration bound ran out (traversal stack overflow etc.) */
   DFC_E_STOPPED = 6,       /* dfc_render_shutdown() ended the render early */
@@ -79,7 +79,9 @@ const char* dfc_last_error(const dfc_renderer* r);
 /* setScene(scene) part 1: one Aparapi put() of a CompiledScene array,
  * renderer/gpu/AbstractSceneKernel.java:1777-1852.  `name` is the kernel field
  * the reference uploads (e.g. "primitiveArray", "shape3FTriangle3FArray");
- * `type` is DFC_F32 or DFC_I32; `count` elements are copied. */
+ * `type` is DFC_F32 or DFC_I32; `count` elements are copied into page-locked
+ * host memory that the handle keeps for the next commits (the upload then runs
+ * by DMA); DFC_E_OOM if that memory cannot be had. */
 int dfc_scene_put(dfc_renderer* r, const char* name, const void* data, int64_t count, int type);
 
 /* setScene(scene) part 2: decodes the staged arrays, builds the acceleration
