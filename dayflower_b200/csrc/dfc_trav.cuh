@@ -360,6 +360,13 @@ DFC_D bool node_step(const SceneView& S, Trav& T, int* stack, unsigned* overflow
     if (n > 3) stack[(T.sp++) * kTraceBlock] = (int)e3;
     if (n > 2) stack[(T.sp++) * kTraceBlock] = (int)e2;
     if (n > 1) stack[(T.sp++) * kTraceBlock] = (int)e1;
+    // the nearest child, when it is a leaf, becomes this lane's pending leaf at
+    // once (it would be the next entry popped), saving the node step that pops it
+    if ((e0 & kTagMask) == kTagLeaf && lf_cnt == 0) {
+      lf_first = (int)((e0 & ~kTagMask) >> 2);
+      lf_cnt = (int)(e0 & 3u) + 1;
+      return false;
+    }
     stack[(T.sp++) * kTraceBlock] = (int)e0;
     return false;
   }
