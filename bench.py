@@ -53,8 +53,8 @@ TRACE_RECORD_BYTES = 52
 # from an ncu capture of one whole 1-spp pass of this workload (the small case
 # of the same scene, camera and rays); the bench scales them by the rays each
 # launch traced and divides by the launch times it measures with CUDA events.
-TRACE_WARP_INST_PER_RAY = 607.2
-TRACE_DRAM_BYTES_PER_RAY = 135.5
+TRACE_WARP_INST_PER_RAY = 600.4
+TRACE_DRAM_BYTES_PER_RAY = 135.1
 TRACE_PROFILE = "profiles/k_trace_terrain_spheres_1080p_1spp.md"
 ISSUE_SLOTS_PER_SM_CYCLE = 4
 # Algorithmic bytes per item of the queue stages (fixed record sizes):
