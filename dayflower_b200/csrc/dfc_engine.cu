@@ -180,7 +180,9 @@ int kernel_variant(const dfc_engine* e) {
 dfc_engine_config resolved(const dfc_engine* e, dfc_engine_config c) {
   if (c.capacity <= 0) c.capacity = kDefaultCapacity;
   if (c.trace_blocks_per_sm <= 0 || c.trace_blocks_per_sm > e->max_trace_blocks) c.trace_blocks_per_sm = e->max_trace_blocks;
-  if (c.shade_blocks_per_sm <= 0) c.shade_blocks_per_sm = 8;
+  // shading: more blocks than fit at once (4096 path slots per SM at the default capacity), so that
+  // the block scheduler balances SMs over the material-sorted work list
+  if (c.shade_blocks_per_sm <= 0) c.shade_blocks_per_sm = 32;
   if (c.shade_threads != 128) c.shade_threads = 256;
   if (c.iterations_per_launch <= 0) c.iterations_per_launch = 4;
   c.iterations_per_launch += c.iterations_per_launch & 1;  // even: the graph ends on the parity it started with
@@ -288,11 +290,13 @@ void enqueue_iteration(dfc_engine* e, int b, int variant) {
   iteration_args(e, b, &ba, &ta, &so, &sa);
   const dfc_engine_config& c = e->active;
   const int shade_grid = e->sm_count * c.shade_blocks_per_sm;
+  // the sort's kernels end each block with global atomics per key: they keep at most 8 blocks per SM
+  const int sort_grid = e->sm_count * std::min(c.shade_blocks_per_sm, 8);
   k_batch_plan<<<1, 32, 0, e->stream>>>(ba);
   k_batch_regen<<<e->sm_count * 4, 256, 0, e->stream>>>(ba);
   (variant >= 1 ? k_trace_batch_records : k_trace_batch)<<<e->sm_count * c.trace_blocks_per_sm, kTraceThreads, 0, e->stream>>>(ta);
-  k_sort_count_batch<<<shade_grid, 256, 0, e->stream>>>(so);
-  k_sort_scatter<<<shade_grid, 256, 0, e->stream>>>(so);
+  k_sort_count_batch<<<sort_grid, 256, 0, e->stream>>>(so);
+  k_sort_scatter<<<sort_grid, 256, 0, e->stream>>>(so);
   // the two-lobe kernel over the matte ... plastic hits, misses and light-ray-only paths, the general one over the rest
   ShadeArgs simple = sa;
   simple.range_bins = so.bins;

@@ -353,7 +353,7 @@ enum { DFC_SCHEDULE_ROUND_ROBIN = 0, DFC_SCHEDULE_FIFO = 1, DFC_SCHEDULE_SHORTES
 typedef struct dfc_engine_config {
   int64_t capacity;              /* path slots of the wavefront (0: default 2^20) */
   int32_t trace_blocks_per_sm;   /* resident blocks per SM of the traversal kernel (0: occupancy maximum) */
-  int32_t shade_blocks_per_sm;   /* blocks per SM of the sort and shade kernels (0: 8) */
+  int32_t shade_blocks_per_sm;   /* blocks per SM of the shade kernels (0: 32); the sort's kernels use at most 8 */
   int32_t shade_threads;         /* threads per shade block: 128 or 256 (0: 256) */
   int32_t iterations_per_launch; /* bounce iterations per CUDA-graph launch, even (0: 4) */
   int32_t policy;                /* DFC_SCHEDULE_* */
