@@ -847,11 +847,9 @@ int dfc_engine_scene_put(dfc_engine* e, const char* name, const void* data, int6
   if (type != DFC_F32 && type != DFC_I32) return efail(e, DFC_E_INVALID_ARG, "type must be DFC_F32 or DFC_I32");
   try {  // the staging arrays are page-locked host memory (PinnedAllocator)
     if (type == DFC_F32) {
-      const float* f = static_cast<const float*>(data);
-      e->staged.f32[name].assign(f, f + count);
+      stage_copy(e->staged.f32[name], static_cast<const float*>(data), (size_t)count);
     } else {
-      const int32_t* q = static_cast<const int32_t*>(data);
-      e->staged.i32[name].assign(q, q + count);
+      stage_copy(e->staged.i32[name], static_cast<const int32_t*>(data), (size_t)count);
     }
   } catch (const std::bad_alloc&) {
     return efail(e, DFC_E_OOM, std::string("no page-locked host memory to stage ") + name);

@@ -47,6 +47,13 @@ void parallel_for(size_t n, F&& f) {
   for (auto& w : ws) w.join();
 }
 
+template <typename V, typename T>
+void stage_copy_into(V& dst, const T* src, size_t count) {
+  dst.resize(count);
+  T* out = dst.data();
+  parallel_for(count, [&](size_t a, size_t b) { std::memcpy(out + a, src + a, (b - a) * sizeof(T)); });
+}
+
 struct Fail {
   int code;
   std::string msg;
@@ -754,6 +761,9 @@ struct Decoder {
 };
 
 }  // namespace
+
+void stage_copy(StagedF& dst, const float* src, size_t count) { stage_copy_into(dst, src, count); }
+void stage_copy(StagedI& dst, const int32_t* src, size_t count) { stage_copy_into(dst, src, count); }
 
 int ingest_scene(Staged& st, int layout, HostScene* out, std::string* err, bool device_blas) {
   try {

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <map>
 #include <new>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -29,6 +30,12 @@ struct PinnedAllocator {
     return static_cast<T*>(p);
   }
   void deallocate(T* p, size_t) { cudaFreeHost(p); }
+  // resize() default-initialises (no zero fill): every staged element is
+  // written by stage_copy right after
+  template <typename U>
+  void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
   template <typename U>
   bool operator==(const PinnedAllocator<U>&) const { return true; }
   template <typename U>
@@ -36,6 +43,12 @@ struct PinnedAllocator {
 };
 using StagedF = std::vector<float, PinnedAllocator<float>>;
 using StagedI = std::vector<int32_t, PinnedAllocator<int32_t>>;
+
+// Copies `count` elements into a staging array (capacity kept between
+// commits), on the host's threads when the array is large.  Throws
+// std::bad_alloc when no page-locked memory can be had.
+void stage_copy(StagedF& dst, const float* src, size_t count);
+void stage_copy(StagedI& dst, const int32_t* src, size_t count);
 
 // Arrays staged by dfc_scene_put, by reference field name.
 struct Staged {
