@@ -191,7 +191,9 @@ int dfc_set_film_filter(dfc_renderer* r, int filter);
  * host binned-SAH builder, 1 (default) the device builder (Morton-ordered
  * radix tree collapsed to 4-wide nodes, built from the uploaded triangle
  * records; about 9x faster to commit a 2M-triangle mesh, about 3% slower to
- * trace).  The
+ * trace; its temporaries come from a per-device memory pool that keeps up to
+ * 1 GiB of device memory reserved between commits, for the life of the
+ * process).  The
  * reference builds its mesh hierarchies on the host (BVHNode3Fs.create,
  * geometry/boundingvolume/hierarchy/BVHNode3Fs.java:63-237); both produce the
  * same node format and the same hits. */
